@@ -1,0 +1,445 @@
+#!/usr/bin/env python
+"""Benchmark of the ISAAC rendering hot path on B200.
+
+Workload (default): the precision scene -- four float32 512^3 spectral-field
+sources (seeds 6-9, slopes -5/3, -2, -3, -11/3), rendered at 1920x1080 with
+trilinear sampling, step 0.5 cells, the default (combined, pre-classified)
+renderer.  One step = one ``doVisualization`` frame: merge of the sources into
+the combined RGBA8 texture, then clear + shading + volume ray-cast.
+
+Metric: frames/s (whole job over all GPUs; replicas, so weak scaling) with
+Gsamples/s beside it, where a sample is one iteration of the reference's
+ray-march loop (lib/isaac/isaac_volume_kernel.hpp:69-82), counted by the
+kernel itself and checked against the CPU oracle in the parity tests.
+
+``--impl reference`` times the reference's CPU path instead.  The reference
+cannot be built here (alpaka, Boost, glm, IceT and MPI are absent), so its
+stand-in is the CPU restatement in oracle/ run with all host threads on a
+bounded sample of the same frame (the full merge plus a band of image rows).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="isaac_b200", choices=["isaac_b200", "reference"])
+    ap.add_argument("--size", type=int, default=512, help="edge of each cubic source volume")
+    ap.add_argument("--sources", type=int, default=4)
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--renderer", default="combined", choices=["combined", "per_source"])
+    ap.add_argument("--dtype", default="f32", choices=["f32", "bf16", "f16"], help="per-source renderer bricks")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-rows", type=int, default=0, help="image rows of the CPU sample (0 = auto)")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL,
+                text=True,
+            )
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_scene(args, device):
+    import torch
+
+    from isaac_b200 import scenes
+
+    n = args.size
+    seeds = (6, 7, 8, 9, 10, 11, 12, 13)[: args.sources]
+    slopes = (-5.0 / 3.0, -2.0, -3.0, -11.0 / 3.0, -5.0 / 3.0, -2.0, -3.0, -11.0 / 3.0)[: args.sources]
+    fields = scenes.precision_scene(n, seeds=seeds, slopes=slopes, device=device)
+    tfs = [scenes.transfer_4point(0.7 * i) for i in range(args.sources)]
+    P, MV = scenes.camera(args.width, args.height, seed=3, distance=2.5)
+    torch.cuda.synchronize() if device != "cpu" else None
+    return fields, tfs, P, MV
+
+
+def make_viz(args, fields, tfs, P, MV):
+    from isaac_b200 import IsaacVisualization, VolumeSource
+
+    n = args.size
+    vols = [VolumeSource(f"field{i}", f, feature_dim=1, persistent=True) for i, f in enumerate(fields)]
+    viz = IsaacVisualization("bench", (args.width, args.height), (n, n, n), (n, n, n), (1, 1, 1), (0, 0, 0), vols)
+    for i, tf in enumerate(tfs):
+        viz.setTransferPoints(i, tf)
+    viz.setInterpolation(True)
+    viz.setStep(0.5)
+    viz.setCamera(P, MV)
+    if args.renderer == "per_source":
+        viz.setRenderOptimization(False)
+        dt = {"f32": 0, "bf16": 1, "f16": 2}[args.dtype]
+        for i in range(len(fields)):
+            viz.setStorage(i, dt)
+    return viz
+
+
+def oracle_for(args, host_fields, tfs, P, MV):
+    from oracle import oracle as O
+
+    n = args.size
+    k = len(host_fields)
+    o = O.Oracle((args.width, args.height), (n, n, n), (n, n, n), (1, 1, 1), (0, 0, 0), (1, 1, 1), [1] * k, [1] * k, k)
+    for i, f in enumerate(host_fields):
+        o.set_source(i, f)
+        o.set_transfer(i, tfs[i])
+    o.set_interpolation(True)
+    o.set_step(0.5)
+    o.set_camera(P, MV)
+    if args.renderer == "per_source":
+        o.set_optimized(False)
+    return o
+
+
+def cpu_sample(args, o, rows_hint=0):
+    """Time the oracle on the full merge plus a band of rows through the image centre;
+    returns (frame seconds extrapolated, samples/s, rows, merge s, band s, samples)."""
+    from oracle import oracle as O
+
+    threads = O.num_threads()
+    rows = rows_hint or max(8, 2 * threads)
+    rows = min(rows, args.height)
+    r0 = args.height // 2 - rows // 2
+    t0 = time.perf_counter()
+    o.update()
+    t1 = time.perf_counter()
+    o.render(rows=(r0, r0 + rows))
+    t2 = time.perf_counter()
+    samples = o.samples()[0]
+    merge_s, band_s = t1 - t0, t2 - t1
+    frame_s = merge_s + band_s * args.height / rows
+    return frame_s, samples / max(band_s, 1e-9), rows, merge_s, band_s, samples, threads
+
+
+def run_reference(args):
+    """CPU stand-in for the reference's own CPU backend (see module docstring)."""
+    import numpy as np
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    fields, tfs, P, MV = build_scene(args, dev)
+    host = [f.cpu().numpy() for f in fields]
+    del fields
+    o = oracle_for(args, host, tfs, P, MV)
+    frame_times, sps = [], []
+    rows = args.cpu_rows
+    info = None
+    for i in range(args.warmup + args.steps):
+        info = cpu_sample(args, o, rows)
+        if i >= args.warmup:
+            frame_times.append(info[0])
+            sps.append(info[1])
+    frame_s = sorted(frame_times)[len(frame_times) // 2]
+    fps = 1.0 / frame_s
+    cores = info[6]
+    sample = f"full merge of {args.sources}x{args.size}^3 + {info[2]} of {args.height} rows per step, extrapolated to a frame"
+    line = {
+        "metric": metric_name(args),
+        "value": fps,
+        "unit": "frames/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": frame_s * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "impl": "reference",
+        "config": config_of(args),
+        "gsamples_per_s": sorted(sps)[len(sps) // 2] / 1e9,
+        "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CPU backend not buildable here (alpaka/Boost/glm/IceT/MPI absent); oracle/ CPU restatement timed instead",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def metric_name(args):
+    return f"fps @{args.width}x{args.height}, {args.sources}x{args.size}^3 f32 sources, plain GPU ray-caster"
+
+
+def config_of(args):
+    return {
+        "workload": f"precision scene: {args.sources} x {args.size}^3 float32 spectral sources, "
+        f"{args.width}x{args.height}, trilinear, step 0.5, {args.renderer} renderer"
+        + (f" ({args.dtype} bricks)" if args.renderer == "per_source" else ""),
+        "sources": args.sources,
+        "volume": args.size,
+        "framebuffer": [args.width, args.height],
+        "renderer": args.renderer,
+        "parallelism": "replicas",
+        "l2": "inputs larger than L2 (sources and textures are > 126 MB)",
+    }
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    fields, tfs, P, MV = build_scene(args, "cuda")
+    viz = make_viz(args, fields, tfs, P, MV)
+
+    # samples of one frame, counted by the kernels (untimed)
+    viz.setCounting(True)
+    viz.update()
+    viz.render()
+    samples, _ = viz.counters()
+    viz.setCounting(False)
+
+    for _ in range(args.warmup):
+        viz.update()
+        viz.render()
+    torch.cuda.synchronize()
+
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.3)
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        viz.update()
+        viz.render()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clk.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    upd_l, ren_l = viz.launchCounts()
+    launches = args.steps * (upd_l + ren_l)
+    fps = world * 1000.0 / ms
+
+    # per-kernel device time with events on the launch stream
+    viz.setTiming(True)
+    acc = {}
+    nt = max(3, min(args.steps, 10))
+    for _ in range(nt):
+        viz.update()
+        viz.render()
+        for k, v in viz.timings().items():
+            acc[k] = acc.get(k, 0.0) + v / nt
+    viz.setTiming(False)
+    vol_ms = acc.get("shade_volume", 0.0)
+    peak, peak_kind = measured_peaks()
+    bytes_per_sample = 32 if args.renderer == "combined" else {"f32": 4, "bf16": 2, "f16": 2}[args.dtype] * 8 * args.sources
+    achieved = samples * bytes_per_sample / (vol_ms * 1e-3) / 1e9 if vol_ms > 0 else None
+    traffic = None
+    prof = ROOT / "profiles" / "traffic.json"
+    if prof.exists():
+        try:
+            traffic = json.loads(prof.read_text()).get(f"{args.renderer}_{args.size}_{args.width}x{args.height}")
+        except Exception:
+            traffic = None
+    roofline = {
+        "bound": "hbm",
+        "kernel": "k_shade_volume (shading + volume ray-march)",
+        "achieved": achieved,
+        "peak": peak,
+        "peak_kind": peak_kind,
+        "unit": "GB/s",
+        "frac": (achieved / peak) if achieved else None,
+        "traffic": traffic,
+        "algorithmic_bytes_per_sample": bytes_per_sample,
+        "samples_per_launch": samples,
+        "kernel_ms": vol_ms,
+    }
+
+    # end to end through the public API: pinned host sources -> device, frame -> pinned host
+    e2e = None
+    if not args.no_e2e:
+        host_src = [f.cpu().pin_memory() for f in fields]
+        frame_host = torch.empty((args.height, args.width, 4), dtype=torch.uint8).pin_memory()
+        out = frame_host.numpy()
+        h2d = sum(h.numel() * h.element_size() for h in host_src)
+        d2h = frame_host.numel()
+
+        def e2e_step():
+            for h, d in zip(host_src, fields):
+                d.copy_(h, non_blocking=True)
+            viz.doVisualization(out=out)
+
+        for _ in range(2):
+            e2e_step()
+        ne = max(3, min(args.steps, 8))
+        barrier()
+        torch.cuda.synchronize()
+        t0 = e0.__class__(enable_timing=True)
+        t1 = e0.__class__(enable_timing=True)
+        t0.record(stream)
+        for _ in range(ne):
+            e2e_step()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e2e_ms = max_over_ranks(t0.elapsed_time(t1) / ne)
+        e2e = {"value": world * 1000.0 / e2e_ms, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": e2e_ms}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            host = [f.cpu().numpy() for f in fields]
+            o = oracle_for(args, host, tfs, P, MV)
+            frame_s, sps, rows, merge_s, band_s, cs, threads = cpu_sample(args, o, args.cpu_rows)
+            cpu = {
+                "value": 1.0 / frame_s,
+                "unit": "frames/s",
+                "cores": threads,
+                "kind": "port",
+                "sample": f"full merge ({merge_s:.2f} s) + {rows} of {args.height} rows ({band_s:.2f} s), extrapolated to a frame",
+                "gsamples_per_s": sps / 1e9,
+            }
+            del o
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "frames/s", "cores": None, "kind": "port", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": metric_name(args),
+            "value": fps,
+            "unit": "frames/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32" if args.renderer == "combined" else args.dtype,
+            "data": "synthetic (seeded spectral fields)",
+            "config": config_of(args),
+            "gsamples_per_s": samples * fps / 1e9,
+            "samples_per_frame": samples,
+            "phases_ms": acc,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clocks,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    viz.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

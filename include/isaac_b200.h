@@ -1,0 +1,218 @@
+/* isaac_b200.h -- C ABI of the B200-native ISAAC in-situ rendering hot path.
+ *
+ * One context renders one local volume (plus optional particle sources) into
+ * an RGBA8 framebuffer on one GPU.  All device work is enqueued on the
+ * caller's CUDA stream (passed as `void*` = cudaStream_t, NULL = legacy
+ * default stream) and is asynchronous unless an entry point says otherwise.
+ * Every entry point returns an isaacb_status; a failing call leaves a message
+ * in isaacb_last_error().  No call aborts, traps or exits.
+ *
+ * The reference is a header-only C++ template library; its per-frame entry
+ * is IsaacVisualization::doVisualization (lib/isaac.hpp:1298-2104) with the
+ * draw callback drawCallBack (lib/isaac.hpp:2140-2543).  Each function below
+ * names the reference interface it replaces.
+ *
+ * Source indices are "combined" indices as in the reference
+ * (lib/isaac.hpp:720-731): volume sources first, then particle sources.
+ * Field sources (advected vector fields, lib/isaac/isaac_common_kernel.hpp:500-550)
+ * are not part of this library.
+ */
+#ifndef ISAAC_B200_H
+#define ISAAC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ISAACB_MAX_SOURCES 16 /* ISAAC_MAX_SOURCES, lib/isaac/isaac_defines.hpp:36-38 */
+#define ISAACB_MAX_FUNCTORS 3 /* ISAAC_MAX_FUNCTORS, lib/isaac/isaac_defines.hpp:27-29 */
+#define ISAACB_MAX_CLIPPING 16 /* ISAAC_MAX_CLIPPING, lib/isaac/isaac_defines.hpp:44-46 */
+
+typedef enum isaacb_status
+{
+    ISAACB_OK = 0,
+    ISAACB_INVALID_ARG = 1,
+    ISAACB_PARSE_ERROR = 2, /* functor chain had an error code; the parsed prefix is applied */
+    ISAACB_CUDA_ERROR = 3,
+    ISAACB_TIMEOUT = 4,
+    ISAACB_OOM = 5,
+    ISAACB_NOT_READY = 6 /* a required input (source pointer, camera) was never set */
+} isaacb_status;
+
+typedef enum isaacb_dtype
+{
+    ISAACB_F32 = 0,
+    ISAACB_BF16 = 1,
+    ISAACB_F16 = 2
+} isaacb_dtype;
+
+typedef enum isaacb_renderer
+{
+    /* pre-classified RGBA8 volume + iso textures, the reference default
+     * (ISAAC_RENDERER_OPTIMIZED, lib/ISAACConfig.cmake:50-53) */
+    ISAACB_RENDERER_COMBINED = 0,
+    /* per-source sampling, functor chain and transfer function at every sample
+     * (ISAAC_RENDERER_LEGACY, lib/isaac/isaac_volume_kernel.hpp:91-632) */
+    ISAACB_RENDERER_PER_SOURCE = 1
+} isaacb_renderer;
+
+/* Geometry and source layout.  Mirrors the IsaacVisualization constructor
+ * arguments (lib/isaac.hpp:565-583) minus the alpaka/stream/server arguments. */
+typedef struct isaacb_desc
+{
+    uint32_t framebuffer[2]; /* width, height */
+    uint32_t global_size[3];
+    uint32_t local_size[3];
+    uint32_t local_particle_size[3];
+    int32_t position[3];
+    float scale[3];
+    uint32_t transfer_size; /* T_transferSize, 1024 in the reference example */
+    uint32_t n_volume_sources;
+    uint32_t n_particle_sources;
+    uint32_t feature_dim[ISAACB_MAX_SOURCES]; /* 1..4 */
+    uint32_t persistent[ISAACB_MAX_SOURCES]; /* T_Source::persistent */
+    uint32_t guard_size[ISAACB_MAX_SOURCES]; /* T_Source::guardSize; must be 0 */
+} isaacb_desc;
+
+typedef struct isaacb_ctx isaacb_ctx;
+
+/* Constructor + init (lib/isaac.hpp:565-945): allocates textures, transfer
+ * tables and G-buffer; sets the reference defaults (step 0.5, weight 2,
+ * chain "idem", hue-ramp transfer functions, dither mode 1, render mode 0,
+ * AO off with weight 0.5, nearest filtering). */
+isaacb_status isaacb_create(const isaacb_desc* desc, isaacb_ctx** out);
+/* Destructor (lib/isaac.hpp ~IsaacVisualization). */
+isaacb_status isaacb_destroy(isaacb_ctx* ctx);
+/* Last error message of this context (or of the last failed create if ctx is NULL). */
+const char* isaacb_last_error(const isaacb_ctx* ctx);
+
+/* Volume source memory: `dev` points to (local+2*guard)^3 voxels, x fastest,
+ * feature_dim floats per voxel -- what the reference reads through
+ * T_Source::operator[] (example/example.cpp:66-71).  The pointer is borrowed. */
+isaacb_status isaacb_set_source(isaacb_ctx* ctx, uint32_t src, const float* dev);
+
+/* Particle source as a cell list -- what the reference reads through
+ * T_ParticleSource::getIterator(cell) (example/example.cpp:148-228):
+ * cell_offsets[ncells+1] (cell = x + y*PX + z*PX*PY), positions relative to the
+ * cell in [0,1)^3 (3 floats), feature_dim attribute floats, per-particle radius
+ * (or NULL to use const_radius).  All device pointers, borrowed. */
+isaacb_status isaacb_set_particles(
+    isaacb_ctx* ctx,
+    uint32_t src,
+    const uint32_t* cell_offsets,
+    const float* positions,
+    const float* attributes,
+    const float* radii,
+    float const_radius);
+
+/* Functor chain (lib/isaac.hpp:1079-1241): same grammar ("op(p0,..)|op|op"),
+ * pool order idem, add, mul, length, pow, sum, and error codes
+ * (1 too many functors, -1 missing ')', 2 more than 4 parameters,
+ * -2 bad number or unknown functor).  As in the reference the parsed prefix
+ * is applied even when error_code != 0; the call then returns PARSE_ERROR. */
+isaacb_status isaacb_set_functions(isaacb_ctx* ctx, uint32_t src, const char* chain, int32_t* error_code);
+/* Pure host parser of one chain string (no context, no GPU). */
+isaacb_status isaacb_parse_chain(
+    const char* chain,
+    int32_t bytecode[ISAACB_MAX_FUNCTORS],
+    float params[4 * ISAACB_MAX_FUNCTORS],
+    int32_t* error_code);
+
+/* Transfer function control points (lib/isaac.hpp:1591-1612) and table
+ * rebuild (updateTransfer, lib/isaac.hpp:1244-1266).  keys ascending or not;
+ * a repeated key keeps its first value. */
+isaacb_status isaacb_set_transfer(
+    isaacb_ctx* ctx,
+    uint32_t src,
+    uint32_t n_points,
+    const uint32_t* keys,
+    const float* rgba);
+/* Host copy of a source's transfer table (transfer_size x float4). */
+isaacb_status isaacb_get_transfer(isaacb_ctx* ctx, uint32_t src, float* lut_rgba);
+
+/* Steering setters: "weight" (lib/isaac.hpp:1700-1706), "iso threshold"
+ * (:1684-1690), "step" (:1626-1635, raised to 0.01), "interpolation"
+ * (:1613-1618), "render optimization" (:1619-1625), "ao" (:1768-1778),
+ * "render mode" (:1780-1786), "dither mode" (:1788-1795; modes 0, 1, 2). */
+isaacb_status isaacb_set_weight(isaacb_ctx* ctx, uint32_t src, float weight);
+isaacb_status isaacb_set_iso_threshold(isaacb_ctx* ctx, uint32_t src, float iso);
+isaacb_status isaacb_set_step(isaacb_ctx* ctx, float step);
+isaacb_status isaacb_set_interpolation(isaacb_ctx* ctx, int32_t enabled);
+isaacb_status isaacb_set_renderer(isaacb_ctx* ctx, int32_t renderer);
+isaacb_status isaacb_set_ao(isaacb_ctx* ctx, int32_t enabled, float weight, int32_t filter);
+isaacb_status isaacb_set_render_mode(isaacb_ctx* ctx, int32_t mode);
+isaacb_status isaacb_set_dither_mode(isaacb_ctx* ctx, int32_t mode);
+/* Storage type of the per-source renderer's bricks (no reference counterpart;
+ * FP32 is the reference behaviour). */
+isaacb_status isaacb_set_storage(isaacb_ctx* ctx, uint32_t src, int32_t dtype);
+/* Background colour as handed to the draw callback (lib/isaac.hpp:2245-2249
+ * swizzles it to (a,b,g,r) with alpha 0 for the G-buffer clear). */
+isaacb_status isaacb_set_background(isaacb_ctx* ctx, const float rgba[4]);
+
+/* Clipping planes: addClipping / editClipping / removeClipping
+ * (lib/isaac.hpp:956-1015).  INVALID_ARG where the reference returns false. */
+isaacb_status isaacb_add_clipping(isaacb_ctx* ctx, const float position[3], const float normal[3]);
+isaacb_status isaacb_edit_clipping(isaacb_ctx* ctx, uint32_t nr, const float position[3], const float normal[3]);
+isaacb_status isaacb_remove_clipping(isaacb_ctx* ctx, uint32_t nr);
+
+/* Camera: projection and modelview matrices, column major (the doubles IceT
+ * passes to drawCallBack, lib/isaac.hpp:2140-2178).  The inverse of P*MV is
+ * formed in FP32 exactly as the reference does. */
+isaacb_status isaacb_set_camera(isaacb_ctx* ctx, const double projection[16], const double modelview[16]);
+
+/* Buffer update of doVisualization (lib/isaac.hpp:1805-1947): per-source
+ * textures of non-persistent sources and the merge into the combined RGBA8
+ * volume and iso textures.  Asynchronous on `stream`. */
+isaacb_status isaacb_update(isaacb_ctx* ctx, void* stream);
+
+/* drawCallBack (lib/isaac.hpp:2140-2543): clear, particles, iso, SSAO,
+ * shading, volume.  The frame stays in the context's device framebuffer;
+ * if rgba_dev is not NULL it is also copied there.  Asynchronous. */
+isaacb_status isaacb_render(isaacb_ctx* ctx, void* stream, uint8_t* rgba_dev);
+
+/* One whole doVisualization frame with a host result: update, render and the
+ * device-to-host framebuffer copy (lib/isaac.hpp:2532-2542) into rgba_host
+ * (W*H*4 bytes, row 0 = bottom).  Synchronous on `stream`. */
+isaacb_status isaacb_frame(isaacb_ctx* ctx, void* stream, uint8_t* rgba_host);
+
+/* Device pointer of the context's RGBA8 framebuffer. */
+isaacb_status isaacb_framebuffer(isaacb_ctx* ctx, uint8_t** rgba_dev);
+
+/* Min/max of every source after its functor chain ("minmax" request,
+ * lib/isaac.hpp:1951-2006 with MinMaxKernel/MinMaxParticleKernel,
+ * lib/isaac/isaac_min_max_kernel.hpp:22-97).  Results are bit-identical to
+ * the reference's column scan.  mn/mx are host arrays of n_sources floats.
+ * Synchronous on `stream`. */
+isaacb_status isaacb_minmax(isaacb_ctx* ctx, void* stream, float* mn, float* mx);
+
+/* Diagnostics used by the parity tests.  Synchronous on `stream`. */
+/* G-buffer readback: depth (W*H), normal (W*H*3), ao (W*H); any may be NULL. */
+isaacb_status isaacb_get_gbuffer(isaacb_ctx* ctx, void* stream, float* depth, float* normal, float* ao);
+/* Combined textures in reference layout (local size, x fastest, RGBA8); either may be NULL. */
+isaacb_status isaacb_get_combined(isaacb_ctx* ctx, void* stream, uint8_t* volume, uint8_t* iso);
+/* Enable per-frame counting of executed ray-march iterations (the reference's
+ * loop trips, including those empty-space skipping jumps over). */
+isaacb_status isaacb_set_counting(isaacb_ctx* ctx, int32_t enabled);
+/* Counters of the last rendered frame.  Synchronous on `stream`. */
+isaacb_status isaacb_get_counters(isaacb_ctx* ctx, void* stream, uint64_t* volume_samples, uint64_t* iso_samples);
+/* Per-kernel timing with CUDA events recorded on the launch stream around
+ * every kernel of isaacb_update / isaacb_render (off by default).
+ * isaacb_get_timing returns, for the last update+render, the milliseconds of
+ * ISAACB_TIMING_SLOTS phases in this order: merge (or per-source bricks),
+ * clear+particles, iso, ssao, shade+volume; a phase that did not run is 0.
+ * Synchronous on `stream`. */
+#define ISAACB_TIMING_SLOTS 5
+isaacb_status isaacb_set_timing(isaacb_ctx* ctx, int32_t enabled);
+isaacb_status isaacb_get_timing(isaacb_ctx* ctx, void* stream, float ms[ISAACB_TIMING_SLOTS]);
+
+/* Number of kernels the last isaacb_update / isaacb_render enqueued. */
+isaacb_status isaacb_get_launch_count(isaacb_ctx* ctx, uint32_t* update_launches, uint32_t* render_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ISAAC_B200_H */

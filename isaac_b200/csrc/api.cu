@@ -1,0 +1,1156 @@
+// Host side of the C ABI declared in include/isaac_b200.h: context state,
+// the functor-chain parser, transfer tables, camera set-up and the launch
+// sequence of a frame.  The reference keeps this state in
+// IsaacVisualization (lib/isaac.hpp:58-3036).
+#include "../../include/isaac_b200.h"
+#include "isaacb_internal.h"
+
+#include <algorithm>
+#include <cctype>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+using namespace isaacb;
+
+namespace
+{
+    const char* kFunctorNames[6] = {"idem", "add", "mul", "length", "pow", "sum"};
+    thread_local std::string g_createError;
+
+    // Per-source body of IsaacVisualization::updateFunctions (lib/isaac.hpp:1084-1186).
+    int parse_chain(const std::string& text, int32_t* bytecode, float* params)
+    {
+        int errorCode = 0;
+        std::string source = text;
+        size_t pos = 0;
+        bool again = true;
+        int elem = 0;
+        for(int i = 0; i < 4 * kMaxFunctors; ++i)
+            params[i] = 0.0f;
+        while(again && ((pos = source.find('|')) != std::string::npos || ((again = false) == false)))
+        {
+            if(elem >= kMaxFunctors)
+            {
+                errorCode = 1;
+                break;
+            }
+            std::string token = source.substr(0, pos);
+            source.erase(0, pos + 1);
+            token.erase(
+                std::remove_if(token.begin(), token.end(), [](unsigned char c) { return std::isspace(c) != 0; }),
+                token.end());
+            const size_t open = token.find('(');
+            float* p = params + 4 * elem;
+            if(open != std::string::npos)
+            {
+                const size_t close = token.find(')');
+                if(close == std::string::npos)
+                {
+                    errorCode = -1;
+                    break;
+                }
+                if(close - open == 1)
+                {
+                    p[0] = p[1] = p[2] = p[3] = 0.0f;
+                }
+                else
+                {
+                    std::string args = token.substr(open + 1, close - open - 1);
+                    size_t cpos = 0;
+                    bool more = true;
+                    int n = 0;
+                    while(more && ((cpos = args.find(',')) != std::string::npos || ((more = false) == false)))
+                    {
+                        if(n >= 4)
+                        {
+                            errorCode = 2;
+                            break;
+                        }
+                        const std::string one = args.substr(0, cpos);
+                        args.erase(0, cpos + 1);
+                        try
+                        {
+                            p[n] = std::stof(one);
+                        }
+                        catch(const std::invalid_argument&)
+                        {
+                            errorCode = -2;
+                            n++;
+                            break;
+                        }
+                        catch(const std::out_of_range&)
+                        {
+                            errorCode = -2;
+                            n++;
+                            break;
+                        }
+                        n++;
+                    }
+                    for(; n < 4; n++)
+                        p[n] = p[n - 1];
+                }
+                token = token.substr(0, open);
+            }
+            else
+            {
+                p[0] = p[1] = p[2] = p[3] = 0.0f;
+            }
+            int found = -1;
+            for(int f = 0; f < 6 && found < 0; ++f)
+                if(token == kFunctorNames[f])
+                    found = f;
+            if(found < 0)
+            {
+                errorCode = -2;
+                break;
+            }
+            bytecode[elem] = found;
+            elem++;
+        }
+        for(; elem < kMaxFunctors; elem++)
+        {
+            bytecode[elem] = 0;
+            float* p = params + 4 * elem;
+            p[0] = p[1] = p[2] = p[3] = 0.0f;
+        }
+        return errorCode;
+    }
+
+    // getHSVA (lib/isaac/isaac_helper.hpp:221-264)
+    void hsva(float h, float s, float v, float a, float* out)
+    {
+        const int hi = int(std::floor(double(h) / (M_PI / 3)));
+        const float f = float(double(h) / (M_PI / 3) - double(float(hi)));
+        const float p = v * (1.0f - s);
+        const float q = v * (1.0f - s * f);
+        const float t = v * (1.0f - s * (1.0f - f));
+        float r = 0, g = 0, b = 0;
+        switch(hi)
+        {
+        case 0:
+        case 6:
+            r = v, g = t, b = p;
+            break;
+        case 1:
+            r = q, g = v, b = p;
+            break;
+        case 2:
+            r = p, g = v, b = t;
+            break;
+        case 3:
+            r = p, g = q, b = v;
+            break;
+        case 4:
+            r = t, g = p, b = v;
+            break;
+        case 5:
+            r = v, g = p, b = q;
+            break;
+        default:
+            break;
+        }
+        out[0] = r;
+        out[1] = g;
+        out[2] = b;
+        out[3] = a;
+    }
+
+    // glm::inverse of a float mat4 (compute_inverse<4,4>, cofactor expansion), column major m[c*4+r]
+    void inverse4(const float* in, float* out)
+    {
+        auto m = [&](int c, int r) { return in[c * 4 + r]; };
+        const float c00 = m(2, 2) * m(3, 3) - m(3, 2) * m(2, 3);
+        const float c02 = m(1, 2) * m(3, 3) - m(3, 2) * m(1, 3);
+        const float c03 = m(1, 2) * m(2, 3) - m(2, 2) * m(1, 3);
+        const float c04 = m(2, 1) * m(3, 3) - m(3, 1) * m(2, 3);
+        const float c06 = m(1, 1) * m(3, 3) - m(3, 1) * m(1, 3);
+        const float c07 = m(1, 1) * m(2, 3) - m(2, 1) * m(1, 3);
+        const float c08 = m(2, 1) * m(3, 2) - m(3, 1) * m(2, 2);
+        const float c10 = m(1, 1) * m(3, 2) - m(3, 1) * m(1, 2);
+        const float c11 = m(1, 1) * m(2, 2) - m(2, 1) * m(1, 2);
+        const float c12 = m(2, 0) * m(3, 3) - m(3, 0) * m(2, 3);
+        const float c14 = m(1, 0) * m(3, 3) - m(3, 0) * m(1, 3);
+        const float c15 = m(1, 0) * m(2, 3) - m(2, 0) * m(1, 3);
+        const float c16 = m(2, 0) * m(3, 2) - m(3, 0) * m(2, 2);
+        const float c18 = m(1, 0) * m(3, 2) - m(3, 0) * m(1, 2);
+        const float c19 = m(1, 0) * m(2, 2) - m(2, 0) * m(1, 2);
+        const float c20 = m(2, 0) * m(3, 1) - m(3, 0) * m(2, 1);
+        const float c22 = m(1, 0) * m(3, 1) - m(3, 0) * m(1, 1);
+        const float c23 = m(1, 0) * m(2, 1) - m(2, 0) * m(1, 1);
+        const float f0[4] = {c00, c00, c02, c03}, f1[4] = {c04, c04, c06, c07}, f2[4] = {c08, c08, c10, c11};
+        const float f3[4] = {c12, c12, c14, c15}, f4[4] = {c16, c16, c18, c19}, f5[4] = {c20, c20, c22, c23};
+        const float v0[4] = {m(1, 0), m(0, 0), m(0, 0), m(0, 0)};
+        const float v1[4] = {m(1, 1), m(0, 1), m(0, 1), m(0, 1)};
+        const float v2[4] = {m(1, 2), m(0, 2), m(0, 2), m(0, 2)};
+        const float v3[4] = {m(1, 3), m(0, 3), m(0, 3), m(0, 3)};
+        float I[16];
+        const float sa[4] = {1, -1, 1, -1}, sb[4] = {-1, 1, -1, 1};
+        for(int i = 0; i < 4; ++i)
+        {
+            const float i0 = v1[i] * f0[i] - v2[i] * f1[i] + v3[i] * f2[i];
+            const float i1 = v0[i] * f0[i] - v2[i] * f3[i] + v3[i] * f4[i];
+            const float i2 = v0[i] * f1[i] - v1[i] * f3[i] + v3[i] * f5[i];
+            const float i3 = v0[i] * f2[i] - v1[i] * f4[i] + v2[i] * f5[i];
+            I[0 * 4 + i] = i0 * sa[i];
+            I[1 * 4 + i] = i1 * sb[i];
+            I[2 * 4 + i] = i2 * sa[i];
+            I[3 * 4 + i] = i3 * sb[i];
+        }
+        const float d0 = m(0, 0) * I[0 * 4 + 0], d1 = m(0, 1) * I[1 * 4 + 0], d2 = m(0, 2) * I[2 * 4 + 0],
+                    d3 = m(0, 3) * I[3 * 4 + 0];
+        const float det = (d0 + d1) + (d2 + d3);
+        const float inv = 1.0f / det;
+        for(int i = 0; i < 16; ++i)
+            out[i] = I[i] * inv;
+    }
+
+    // glm mat4 * mat4: column j = ((A0*B[j][0] + A1*B[j][1]) + A2*B[j][2]) + A3*B[j][3]
+    void mul4(const float* A, const float* B, float* R)
+    {
+        for(int c = 0; c < 4; ++c)
+            for(int r = 0; r < 4; ++r)
+            {
+                float s = A[0 * 4 + r] * B[c * 4 + 0];
+                s = s + A[1 * 4 + r] * B[c * 4 + 1];
+                s = s + A[2 * 4 + r] * B[c * 4 + 2];
+                s = s + A[3 * 4 + r] * B[c * 4 + 3];
+                R[c * 4 + r] = s;
+            }
+    }
+} // namespace
+
+struct isaacb_ctx
+{
+    isaacb_desc desc{};
+    Geom g{};
+    int nVol = 0, nPart = 0, nTotal = 0;
+    int ts = 1024;
+    // steering state
+    std::string functions[kMaxSources];
+    Chain chain[kMaxSources]{};
+    int32_t errorCode[kMaxSources]{};
+    std::vector<float> lutHost; // nTotal*ts*4
+    bool lutDirty = true;
+    float weight[kMaxSources]{};
+    float iso[kMaxSources]{};
+    int storage[kMaxSources]{};
+    float step = 0.5f;
+    int interpolation = 0;
+    int renderer = ISAACB_RENDERER_COMBINED;
+    int clipCount = 0;
+    float clipPos[kMaxClip][3]{};
+    float clipNrm[kMaxClip][3]{};
+    int aoEnabled = 0;
+    float aoWeight = 0.5f;
+    int aoFilter = 0;
+    int renderMode = 0;
+    int ditherMode = 1;
+    float bg[4] = {0, 0, 0, 0};
+    double proj[16]{}, mv[16]{};
+    bool cameraSet = false;
+    const float* src[kMaxSources]{};
+    ParticleSrc part[kMaxSources]{};
+    bool partSet[kMaxSources]{};
+    bool counting = false;
+    bool isoWritten = false;
+    // device buffers
+    float4* lutDev = nullptr;
+    float* lutPinned = nullptr;
+    cudaEvent_t lutEvent = nullptr;
+    uint4* volQ = nullptr;
+    uint32_t* isoAQ = nullptr;
+    uint32_t* isoLin = nullptr;
+    uint8_t* volFlag = nullptr;
+    uint8_t* isoFlag = nullptr;
+    void* srcBricks[kMaxSources]{};
+    size_t srcBrickBytes[kMaxSources]{};
+    uchar4* color = nullptr;
+    float* depth = nullptr;
+    float* normal = nullptr;
+    float* ao = nullptr;
+    unsigned long long* counters = nullptr;
+    float* mmPartial = nullptr;
+    float* mmResult = nullptr;
+    unsigned long long* mmKeys = nullptr;
+    uint32_t updateLaunches = 0, renderLaunches = 0;
+    bool timing = false;
+    cudaEvent_t ev[2 * ISAACB_TIMING_SLOTS]{};
+    bool evUsed[ISAACB_TIMING_SLOTS]{};
+    std::string lastError;
+};
+
+namespace
+{
+    isaacb_status fail(isaacb_ctx* c, isaacb_status st, const std::string& msg)
+    {
+        if(c)
+            c->lastError = msg;
+        else
+            g_createError = msg;
+        return st;
+    }
+
+    isaacb_status cuda_fail(isaacb_ctx* c, cudaError_t e, const char* what)
+    {
+        const bool oom = e == cudaErrorMemoryAllocation;
+        std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+        return fail(c, oom ? ISAACB_OOM : ISAACB_CUDA_ERROR, m);
+    }
+
+#define ISAACB_CUDA(c, call, what)                                                                                    \
+    do                                                                                                                \
+    {                                                                                                                 \
+        cudaError_t e_ = (call);                                                                                      \
+        if(e_ != cudaSuccess)                                                                                         \
+            return cuda_fail((c), e_, (what));                                                                        \
+    } while(0)
+
+    bool valid_src(const isaacb_ctx* c, uint32_t s)
+    {
+        return c && s < uint32_t(c->nTotal);
+    }
+
+    // updateTransfer (lib/isaac.hpp:1244-1266) over a description whose repeated
+    // keys keep their first value; entries outside [first key, last key) keep
+    // their previous values.
+    void build_transfer(isaacb_ctx* c, uint32_t s, uint32_t n, const uint32_t* keys, const float* rgba)
+    {
+        std::map<uint32_t, const float*> desc;
+        for(uint32_t i = 0; i < n; ++i)
+            desc.insert({keys[i], rgba + 4 * i});
+        if(desc.empty())
+            return;
+        float* lut = c->lutHost.data() + size_t(s) * c->ts * 4;
+        auto next = desc.begin();
+        auto before = next;
+        for(next++; next != desc.end(); next++)
+        {
+            const uint32_t width = next->first - before->first;
+            for(size_t j = 0; j < size_t(width) && size_t(j + before->first) < size_t(c->ts); j++)
+            {
+                const float wj = float(width - j), jj = float(j), wf = float(width);
+                for(int k = 0; k < 4; ++k)
+                    lut[(before->first + j) * 4 + k] = (before->second[k] * wj + next->second[k] * jj) / wf;
+            }
+            before = next;
+        }
+        c->lutDirty = true;
+    }
+
+    isaacb_status upload_lut(isaacb_ctx* c, cudaStream_t st)
+    {
+        if(!c->lutDirty)
+            return ISAACB_OK;
+        // the pinned staging buffer may still feed a previous asynchronous copy
+        ISAACB_CUDA(c, cudaEventSynchronize(c->lutEvent), "transfer table staging wait");
+        std::memcpy(c->lutPinned, c->lutHost.data(), c->lutHost.size() * sizeof(float));
+        ISAACB_CUDA(
+            c,
+            cudaMemcpyAsync(c->lutDev, c->lutPinned, c->lutHost.size() * sizeof(float), cudaMemcpyHostToDevice, st),
+            "transfer table upload");
+        ISAACB_CUDA(c, cudaEventRecord(c->lutEvent, st), "transfer table event");
+        c->lutDirty = false;
+        return ISAACB_OK;
+    }
+
+    size_t brick_count(const Geom& g)
+    {
+        return size_t(g.nb[0]) * g.nb[1] * g.nb[2];
+    }
+
+    void fill_view(const isaacb_ctx* c, View& v)
+    {
+        float P[16], MV[16], PM[16];
+        for(int i = 0; i < 16; ++i)
+        {
+            P[i] = float(c->proj[i]);
+            MV[i] = float(c->mv[i]);
+        }
+        mul4(P, MV, PM);
+        inverse4(PM, v.inv);
+        v.W = int32_t(c->desc.framebuffer[0]);
+        v.H = int32_t(c->desc.framebuffer[1]);
+        v.scale = make_float3(c->desc.scale[0], c->desc.scale[1], c->desc.scale[2]);
+        v.clipCount = c->clipCount;
+        for(int i = 0; i < kMaxClip; ++i)
+            for(int k = 0; k < 3; ++k)
+            {
+                v.clipPos[i][k] = c->clipPos[i][k];
+                v.clipNrm[i][k] = c->clipNrm[i][k];
+            }
+    }
+
+    // events around one phase (slot) when timing is on
+    struct PhaseTimer
+    {
+        isaacb_ctx* c;
+        int slot;
+        cudaStream_t st;
+        PhaseTimer(isaacb_ctx* c_, int s_, cudaStream_t st_) : c(c_), slot(s_), st(st_)
+        {
+            if(c->timing)
+            {
+                cudaEventRecord(c->ev[2 * slot], st);
+                c->evUsed[slot] = true;
+            }
+        }
+        ~PhaseTimer()
+        {
+            if(c->timing)
+                cudaEventRecord(c->ev[2 * slot + 1], st);
+        }
+    };
+
+    bool any_iso_active(const isaacb_ctx* c)
+    {
+        for(int s = 0; s < c->nVol; ++s)
+            if(c->iso[s] > 0.0f)
+                return true;
+        return false;
+    }
+} // namespace
+
+extern "C"
+{
+    const char* isaacb_last_error(const isaacb_ctx* ctx)
+    {
+        return ctx ? ctx->lastError.c_str() : g_createError.c_str();
+    }
+
+    isaacb_status isaacb_parse_chain(const char* chain, int32_t* bytecode, float* params, int32_t* error_code)
+    {
+        if(!chain || !bytecode || !params)
+            return fail(nullptr, ISAACB_INVALID_ARG, "isaacb_parse_chain: null argument");
+        const int e = parse_chain(std::string(chain), bytecode, params);
+        if(error_code)
+            *error_code = e;
+        return e == 0 ? ISAACB_OK : ISAACB_PARSE_ERROR;
+    }
+
+    isaacb_status isaacb_create(const isaacb_desc* d, isaacb_ctx** out)
+    {
+        if(!d || !out)
+            return fail(nullptr, ISAACB_INVALID_ARG, "isaacb_create: null argument");
+        *out = nullptr;
+        const uint32_t nTotal = d->n_volume_sources + d->n_particle_sources;
+        if(nTotal == 0 || nTotal > uint32_t(kMaxSources))
+            return fail(nullptr, ISAACB_INVALID_ARG, "isaacb_create: 1..16 sources required");
+        if(d->framebuffer[0] == 0 || d->framebuffer[1] == 0 || d->framebuffer[0] > 16384 || d->framebuffer[1] > 16384)
+            return fail(nullptr, ISAACB_INVALID_ARG, "isaacb_create: framebuffer must be 1..16384 per side");
+        for(int i = 0; i < 3; ++i)
+        {
+            if(d->local_size[i] == 0 || d->local_size[i] > 8192 || d->global_size[i] == 0 || d->global_size[i] > 1u << 20)
+                return fail(nullptr, ISAACB_INVALID_ARG, "isaacb_create: local/global size out of range");
+            if(d->n_particle_sources && (d->local_particle_size[i] == 0 || d->local_particle_size[i] > 8192))
+                return fail(nullptr, ISAACB_INVALID_ARG, "isaacb_create: particle grid out of range");
+            if(!(d->scale[i] > 0.0f) || !std::isfinite(d->scale[i]))
+                return fail(nullptr, ISAACB_INVALID_ARG, "isaacb_create: scale must be positive");
+        }
+        if(d->transfer_size < 2 || d->transfer_size > (1u << 16))
+            return fail(nullptr, ISAACB_INVALID_ARG, "isaacb_create: transfer_size must be 2..65536");
+        for(uint32_t s = 0; s < nTotal; ++s)
+        {
+            if(d->feature_dim[s] < 1 || d->feature_dim[s] > 4)
+                return fail(nullptr, ISAACB_INVALID_ARG, "isaacb_create: feature_dim must be 1..4");
+            if(d->guard_size[s] != 0)
+                return fail(nullptr, ISAACB_INVALID_ARG, "isaacb_create: guard_size must be 0");
+        }
+        isaacb_ctx* c = new isaacb_ctx;
+        c->desc = *d;
+        c->nVol = int(d->n_volume_sources);
+        c->nPart = int(d->n_particle_sources);
+        c->nTotal = int(nTotal);
+        c->ts = int(d->transfer_size);
+        Geom& g = c->g;
+        for(int i = 0; i < 3; ++i)
+        {
+            g.gs[i] = int32_t(d->global_size[i]);
+            g.ls[i] = int32_t(d->local_size[i]);
+            g.lps[i] = int32_t(d->local_particle_size[i]);
+            g.pos[i] = d->position[i];
+            // isaac_float3(size) * scale stored into integer vectors (lib/isaac.hpp:659-661)
+            g.gss[i] = int32_t(int64_t(float(d->global_size[i]) * d->scale[i]));
+            g.lss[i] = int32_t(int64_t(float(d->local_size[i]) * d->scale[i]));
+            g.posS[i] = int32_t(float(d->position[i]) * d->scale[i]);
+            g.nb[i] = bricks_per_axis(g.ls[i]);
+        }
+        g.maxGss = std::max(g.gss[0], std::max(g.gss[1], g.gss[2]));
+        // reference defaults (lib/isaac.hpp:720-793)
+        c->lutHost.assign(size_t(c->nTotal) * c->ts * 4, 0.0f);
+        for(int s = 0; s < c->nTotal; ++s)
+        {
+            c->weight[s] = 2.0f;
+            c->iso[s] = 0.0f;
+            c->functions[s] = "idem";
+            c->errorCode[s] = parse_chain(c->functions[s], c->chain[s].op, c->chain[s].p);
+            const float hue = float(double(float(2 * s)) * M_PI / double(float(c->nTotal)));
+            float c0[4], c1[4];
+            hsva(hue, 1, 1, s < c->nVol ? 0.0f : 1.0f, c0);
+            hsva(hue, 1, 1, 1.0f, c1);
+            const uint32_t keys[2] = {0u, uint32_t(c->ts)};
+            float rgba[8];
+            std::memcpy(rgba, c0, 16);
+            std::memcpy(rgba + 4, c1, 16);
+            build_transfer(c, uint32_t(s), 2, keys, rgba);
+        }
+        const size_t npix = size_t(d->framebuffer[0]) * d->framebuffer[1];
+        const size_t nbr = brick_count(g);
+        cudaError_t e = cudaSuccess;
+        auto alloc = [&](void** p, size_t bytes) {
+            if(e == cudaSuccess)
+                e = cudaMalloc(p, bytes);
+        };
+        alloc((void**) &c->lutDev, c->lutHost.size() * sizeof(float));
+        if(e == cudaSuccess)
+            e = cudaMallocHost((void**) &c->lutPinned, c->lutHost.size() * sizeof(float));
+        if(e == cudaSuccess)
+            e = cudaEventCreateWithFlags(&c->lutEvent, cudaEventDisableTiming);
+        alloc((void**) &c->volQ, nbr * kSlotsPerBrick * sizeof(uint4));
+        alloc((void**) &c->isoAQ, nbr * kSlotsPerBrick * sizeof(uint32_t));
+        alloc((void**) &c->isoLin, size_t(g.ls[0]) * g.ls[1] * g.ls[2] * sizeof(uint32_t));
+        alloc((void**) &c->volFlag, nbr);
+        alloc((void**) &c->isoFlag, nbr);
+        alloc((void**) &c->color, npix * sizeof(uchar4));
+        alloc((void**) &c->depth, npix * sizeof(float));
+        alloc((void**) &c->normal, npix * 3 * sizeof(float));
+        alloc((void**) &c->ao, npix * sizeof(float));
+        alloc((void**) &c->counters, 2 * sizeof(unsigned long long));
+        alloc((void**) &c->mmPartial, 2 * 148 * 8 * sizeof(float));
+        alloc((void**) &c->mmResult, 2 * sizeof(float));
+        alloc((void**) &c->mmKeys, 2 * sizeof(unsigned long long));
+        if(e == cudaSuccess)
+            e = cudaMemset(c->isoLin, 0, size_t(g.ls[0]) * g.ls[1] * g.ls[2] * sizeof(uint32_t));
+        if(e == cudaSuccess)
+            e = cudaMemset(c->isoFlag, 0, nbr);
+        if(e == cudaSuccess)
+            e = cudaMemset(c->color, 0, npix * sizeof(uchar4));
+        if(e != cudaSuccess)
+        {
+            const bool oom = e == cudaErrorMemoryAllocation;
+            std::string m = std::string("isaacb_create: ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+            isaacb_destroy(c);
+            return fail(nullptr, oom ? ISAACB_OOM : ISAACB_CUDA_ERROR, m);
+        }
+        *out = c;
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_destroy(isaacb_ctx* c)
+    {
+        if(!c)
+            return ISAACB_OK;
+        cudaFree(c->lutDev);
+        if(c->lutPinned)
+            cudaFreeHost(c->lutPinned);
+        if(c->lutEvent)
+            cudaEventDestroy(c->lutEvent);
+        cudaFree(c->volQ);
+        cudaFree(c->isoAQ);
+        cudaFree(c->isoLin);
+        cudaFree(c->volFlag);
+        cudaFree(c->isoFlag);
+        for(int s = 0; s < kMaxSources; ++s)
+            cudaFree(c->srcBricks[s]);
+        cudaFree(c->color);
+        cudaFree(c->depth);
+        cudaFree(c->normal);
+        cudaFree(c->ao);
+        cudaFree(c->counters);
+        cudaFree(c->mmPartial);
+        cudaFree(c->mmResult);
+        cudaFree(c->mmKeys);
+        for(auto& e : c->ev)
+            if(e)
+                cudaEventDestroy(e);
+        delete c;
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_set_source(isaacb_ctx* c, uint32_t s, const float* dev)
+    {
+        if(!valid_src(c, s) || int(s) >= c->nVol)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_source: not a volume source index");
+        c->src[s] = dev;
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_set_particles(
+        isaacb_ctx* c,
+        uint32_t s,
+        const uint32_t* offsets,
+        const float* positions,
+        const float* attributes,
+        const float* radii,
+        float constRadius)
+    {
+        if(!valid_src(c, s) || int(s) < c->nVol)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_particles: not a particle source index");
+        if(!offsets || !positions || !attributes)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_particles: null device pointer");
+        ParticleSrc& P = c->part[s - c->nVol];
+        P.offsets = offsets;
+        P.pos = positions;
+        P.attr = attributes;
+        P.radius = radii;
+        P.constRadius = constRadius;
+        c->partSet[s - c->nVol] = true;
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_set_functions(isaacb_ctx* c, uint32_t s, const char* chain, int32_t* error_code)
+    {
+        if(!valid_src(c, s) || !chain)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_functions: bad source or null chain");
+        c->functions[s] = chain;
+        c->errorCode[s] = parse_chain(c->functions[s], c->chain[s].op, c->chain[s].p);
+        if(error_code)
+            *error_code = c->errorCode[s];
+        if(c->errorCode[s] != 0)
+            return fail(c, ISAACB_PARSE_ERROR, "isaacb_set_functions: error code " + std::to_string(c->errorCode[s]));
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_set_transfer(isaacb_ctx* c, uint32_t s, uint32_t n, const uint32_t* keys, const float* rgba)
+    {
+        if(!valid_src(c, s) || (n && (!keys || !rgba)))
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_transfer: bad arguments");
+        build_transfer(c, s, n, keys, rgba);
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_get_transfer(isaacb_ctx* c, uint32_t s, float* lut)
+    {
+        if(!valid_src(c, s) || !lut)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_get_transfer: bad arguments");
+        std::memcpy(lut, c->lutHost.data() + size_t(s) * c->ts * 4, size_t(c->ts) * 4 * sizeof(float));
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_set_weight(isaacb_ctx* c, uint32_t s, float w)
+    {
+        if(!valid_src(c, s))
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_weight: bad source");
+        c->weight[s] = w;
+        return ISAACB_OK;
+    }
+    isaacb_status isaacb_set_iso_threshold(isaacb_ctx* c, uint32_t s, float v)
+    {
+        if(!valid_src(c, s))
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_iso_threshold: bad source");
+        c->iso[s] = v;
+        return ISAACB_OK;
+    }
+    isaacb_status isaacb_set_step(isaacb_ctx* c, float v)
+    {
+        if(!c || !(v == v))
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_step: bad step");
+        c->step = v < 0.01f ? 0.01f : v;
+        return ISAACB_OK;
+    }
+    isaacb_status isaacb_set_interpolation(isaacb_ctx* c, int32_t v)
+    {
+        if(!c)
+            return ISAACB_INVALID_ARG;
+        c->interpolation = v != 0;
+        return ISAACB_OK;
+    }
+    isaacb_status isaacb_set_renderer(isaacb_ctx* c, int32_t r)
+    {
+        if(!c || (r != ISAACB_RENDERER_COMBINED && r != ISAACB_RENDERER_PER_SOURCE))
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_renderer: unknown renderer");
+        c->renderer = r;
+        return ISAACB_OK;
+    }
+    isaacb_status isaacb_set_storage(isaacb_ctx* c, uint32_t s, int32_t dt)
+    {
+        if(!valid_src(c, s) || int(s) >= c->nVol || dt < 0 || dt > 2)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_storage: bad source or dtype");
+        c->storage[s] = dt;
+        return ISAACB_OK;
+    }
+    isaacb_status isaacb_set_ao(isaacb_ctx* c, int32_t enabled, float weight, int32_t filter)
+    {
+        if(!c)
+            return ISAACB_INVALID_ARG;
+        c->aoEnabled = enabled != 0;
+        c->aoWeight = weight;
+        c->aoFilter = filter != 0;
+        return ISAACB_OK;
+    }
+    isaacb_status isaacb_set_render_mode(isaacb_ctx* c, int32_t m)
+    {
+        if(!c)
+            return ISAACB_INVALID_ARG;
+        c->renderMode = m;
+        return ISAACB_OK;
+    }
+    isaacb_status isaacb_set_dither_mode(isaacb_ctx* c, int32_t m)
+    {
+        if(!c || m < 0 || m > 2)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_dither_mode: modes 0, 1 and 2 are supported");
+        c->ditherMode = m;
+        return ISAACB_OK;
+    }
+    isaacb_status isaacb_set_background(isaacb_ctx* c, const float* rgba)
+    {
+        if(!c || !rgba)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_background: null argument");
+        std::memcpy(c->bg, rgba, sizeof(c->bg));
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_edit_clipping(isaacb_ctx* c, uint32_t nr, const float* pos, const float* n)
+    {
+        if(!c || !pos || !n || nr >= uint32_t(kMaxClip))
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_edit_clipping: bad plane index or null argument");
+        // editClipping (lib/isaac.hpp:956-985): the normal is scaled and normalised
+        float ns[3] = {n[0] * c->desc.scale[0], n[1] * c->desc.scale[1], n[2] * c->desc.scale[2]};
+        const float t0 = ns[0] * ns[0], t1 = ns[1] * ns[1], t2 = ns[2] * ns[2];
+        const float l = std::sqrt((t0 + t1) + t2);
+        if(l == 0.0f)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_edit_clipping: zero normal");
+        for(int k = 0; k < 3; ++k)
+        {
+            c->clipPos[nr][k] = pos[k];
+            c->clipNrm[nr][k] = ns[k] / l;
+        }
+        return ISAACB_OK;
+    }
+    isaacb_status isaacb_add_clipping(isaacb_ctx* c, const float* pos, const float* n)
+    {
+        if(!c)
+            return ISAACB_INVALID_ARG;
+        isaacb_status st = isaacb_edit_clipping(c, uint32_t(c->clipCount), pos, n);
+        if(st == ISAACB_OK)
+            c->clipCount++;
+        return st;
+    }
+    isaacb_status isaacb_remove_clipping(isaacb_ctx* c, uint32_t nr)
+    {
+        if(!c || nr >= uint32_t(c->clipCount))
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_remove_clipping: no such plane");
+        c->clipCount--;
+        for(int i = int(nr); i < c->clipCount; ++i)
+            for(int k = 0; k < 3; ++k)
+            {
+                c->clipPos[i][k] = c->clipPos[i + 1][k];
+                c->clipNrm[i][k] = c->clipNrm[i + 1][k];
+            }
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_set_camera(isaacb_ctx* c, const double* proj, const double* mv)
+    {
+        if(!c || !proj || !mv)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_camera: null argument");
+        std::memcpy(c->proj, proj, sizeof(c->proj));
+        std::memcpy(c->mv, mv, sizeof(c->mv));
+        c->cameraSet = true;
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_set_counting(isaacb_ctx* c, int32_t on)
+    {
+        if(!c)
+            return ISAACB_INVALID_ARG;
+        c->counting = on != 0;
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_update(isaacb_ctx* c, void* stream)
+    {
+        if(!c)
+            return ISAACB_INVALID_ARG;
+        cudaStream_t st = (cudaStream_t) stream;
+        for(int s = 0; s < c->nVol; ++s)
+            if(!c->src[s] && (c->weight[s] != 0.0f || c->iso[s] != 0.0f))
+                return fail(c, ISAACB_NOT_READY, "isaacb_update: source " + std::to_string(s) + " has no memory");
+        isaacb_status r = upload_lut(c, st);
+        if(r != ISAACB_OK)
+            return r;
+        c->updateLaunches = 0;
+        if(c->renderer == ISAACB_RENDERER_COMBINED)
+        {
+            MergeParams p{};
+            p.g = c->g;
+            p.nVol = c->nVol;
+            p.ts = c->ts;
+            p.ditherMode = c->ditherMode;
+            p.writeIso = any_iso_active(c) ? 1 : 0;
+            p.lut = c->lutDev;
+            p.totalWeight = 0.0f;
+            for(int s = 0; s < c->nVol; ++s)
+            {
+                p.src[s] = c->src[s];
+                p.fdim[s] = int32_t(c->desc.feature_dim[s]);
+                p.chain[s] = c->chain[s];
+                p.weight[s] = c->weight[s];
+                p.iso[s] = c->iso[s];
+                p.totalWeight += c->weight[s];
+            }
+            p.volQ = c->volQ;
+            p.isoAQ = c->isoAQ;
+            p.isoLin = c->isoLin;
+            p.volFlag = c->volFlag;
+            p.isoFlag = c->isoFlag;
+            {
+                for(int k = 0; k < ISAACB_TIMING_SLOTS; ++k)
+                    c->evUsed[k] = false;
+                PhaseTimer t(c, 0, st);
+                launch_merge(p, st);
+            }
+            c->updateLaunches++;
+            if(!p.writeIso && c->isoWritten)
+            {
+                // the reference's iso texture is all zero when no source has an iso threshold
+                ISAACB_CUDA(
+                    c,
+                    cudaMemsetAsync(c->isoLin, 0, size_t(c->g.ls[0]) * c->g.ls[1] * c->g.ls[2] * 4, st),
+                    "iso clear");
+                ISAACB_CUDA(c, cudaMemsetAsync(c->isoFlag, 0, brick_count(c->g), st), "iso flag clear");
+            }
+            c->isoWritten = p.writeIso != 0;
+        }
+        else
+        {
+            for(int k = 0; k < ISAACB_TIMING_SLOTS; ++k)
+                c->evUsed[k] = false;
+            if(c->timing)
+            {
+                cudaEventRecord(c->ev[0], st);
+                c->evUsed[0] = true;
+            }
+            for(int s = 0; s < c->nVol; ++s)
+            {
+                const bool enabled = c->weight[s] != 0.0f || c->iso[s] != 0.0f;
+                if(!enabled)
+                    continue;
+                const int fdim = int(c->desc.feature_dim[s]);
+                const int ncomp = c->desc.persistent[s] ? fdim : 1;
+                const size_t esz = c->storage[s] == 0 ? 4 : 2;
+                const size_t bytes = brick_count(c->g) * kSlotsPerBrick * 4 * ncomp * esz;
+                if(c->srcBrickBytes[s] != bytes)
+                {
+                    cudaFree(c->srcBricks[s]);
+                    c->srcBricks[s] = nullptr;
+                    c->srcBrickBytes[s] = 0;
+                    ISAACB_CUDA(c, cudaMalloc(&c->srcBricks[s], bytes), "per-source brick allocation");
+                    c->srcBrickBytes[s] = bytes;
+                }
+                SourceBrickParams p{};
+                p.g = c->g;
+                p.src = c->src[s];
+                p.fdim = fdim;
+                p.ncomp = ncomp;
+                p.applyChain = c->desc.persistent[s] ? 0 : 1;
+                p.dtype = c->storage[s];
+                p.chain = c->chain[s];
+                p.out = c->srcBricks[s];
+                launch_source_bricks(p, st);
+                c->updateLaunches++;
+            }
+            if(c->timing)
+                cudaEventRecord(c->ev[1], st);
+        }
+        ISAACB_CUDA(c, cudaGetLastError(), "isaacb_update launch");
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_render(isaacb_ctx* c, void* stream, uint8_t* rgba_dev)
+    {
+        if(!c)
+            return ISAACB_INVALID_ARG;
+        if(!c->cameraSet)
+            return fail(c, ISAACB_NOT_READY, "isaacb_render: camera not set");
+        for(int s = 0; s < c->nPart; ++s)
+            if(!c->partSet[s] && c->weight[c->nVol + s] != 0.0f)
+                return fail(c, ISAACB_NOT_READY, "isaacb_render: particle source without memory");
+        cudaStream_t st = (cudaStream_t) stream;
+        isaacb_status r = upload_lut(c, st);
+        if(r != ISAACB_OK)
+            return r;
+        FrameParams p{};
+        fill_view(c, p.v);
+        p.g = c->g;
+        p.ts = c->ts;
+        p.interpolation = c->interpolation;
+        p.step = c->step;
+        p.bg = make_float4(c->bg[0], c->bg[1], c->bg[2], c->bg[3]);
+        p.bgSwizzled = make_float4(c->bg[3], c->bg[2], c->bg[1], 0.0f);
+        p.renderMode = c->renderMode;
+        p.aoWeight = c->aoWeight;
+        p.aoFilter = c->aoFilter;
+        p.totalWeightAll = 0.0f;
+        for(int s = 0; s < c->nTotal; ++s)
+            p.totalWeightAll += c->weight[s];
+        p.lut = c->lutDev;
+        p.volQ = c->volQ;
+        p.isoAQ = c->isoAQ;
+        p.isoLin = c->isoLin;
+        p.volFlag = c->volFlag;
+        p.isoFlag = c->isoFlag;
+        p.nVol = c->nVol;
+        p.nPart = c->nPart;
+        p.pscale = make_float3(
+            float(c->g.lss[0]) / float(c->g.lps[0] ? c->g.lps[0] : 1),
+            float(c->g.lss[1]) / float(c->g.lps[1] ? c->g.lps[1] : 1),
+            float(c->g.lss[2]) / float(c->g.lps[2] ? c->g.lps[2] : 1));
+        for(int s = 0; s < c->nPart; ++s)
+        {
+            ParticleSrc P = c->part[s];
+            const int cs = c->nVol + s;
+            P.fdim = int32_t(c->desc.feature_dim[cs]);
+            P.weight = c->weight[cs];
+            P.lutBase = cs * c->ts;
+            P.chain = c->chain[cs];
+            p.part[s] = P;
+        }
+        for(int s = 0; s < c->nVol; ++s)
+        {
+            PerSourceSrc& S = p.ps[s];
+            S.bricks = c->srcBricks[s];
+            S.dtype = c->storage[s];
+            S.persistent = int32_t(c->desc.persistent[s]);
+            S.fdim = int32_t(c->desc.feature_dim[s]);
+            S.ncomp = S.persistent ? S.fdim : 1;
+            S.weight = c->weight[s];
+            S.iso = c->iso[s];
+            S.chain = c->chain[s];
+            if(c->renderer == ISAACB_RENDERER_PER_SOURCE && (S.weight != 0.0f || S.iso != 0.0f) && !S.bricks)
+                return fail(c, ISAACB_NOT_READY, "isaacb_render: per-source bricks missing; call isaacb_update");
+        }
+        p.color = c->color;
+        p.depth = c->depth;
+        p.normal = c->normal;
+        p.ao = c->ao;
+        p.counters = nullptr;
+        if(c->counting)
+        {
+            ISAACB_CUDA(c, cudaMemsetAsync(c->counters, 0, 2 * sizeof(unsigned long long), st), "counter reset");
+            p.counters = c->counters;
+        }
+        c->renderLaunches = 0;
+        for(int k = 1; k < ISAACB_TIMING_SLOTS; ++k)
+            c->evUsed[k] = false;
+        {
+            PhaseTimer t(c, 1, st);
+            launch_clear_particles(p, st);
+        }
+        c->renderLaunches++;
+        if(c->renderer == ISAACB_RENDERER_COMBINED)
+        {
+            if(any_iso_active(c))
+            {
+                PhaseTimer t(c, 2, st);
+                launch_iso(p, st);
+                c->renderLaunches++;
+            }
+        }
+        else
+        {
+            PhaseTimer t(c, 2, st);
+            launch_iso_per_source(p, st);
+            c->renderLaunches++;
+        }
+        if(c->aoEnabled && c->aoWeight > 0.0f)
+        {
+            PhaseTimer t(c, 3, st);
+            launch_ssao(p, st);
+            c->renderLaunches++;
+        }
+        {
+            PhaseTimer t(c, 4, st);
+            if(c->renderer == ISAACB_RENDERER_COMBINED)
+                launch_shade_volume(p, p.totalWeightAll > 0.0f, st);
+            else
+                launch_shade_volume_per_source(p, st);
+        }
+        c->renderLaunches++;
+        ISAACB_CUDA(c, cudaGetLastError(), "isaacb_render launch");
+        if(rgba_dev)
+        {
+            const size_t bytes = size_t(c->desc.framebuffer[0]) * c->desc.framebuffer[1] * 4;
+            ISAACB_CUDA(c, cudaMemcpyAsync(rgba_dev, c->color, bytes, cudaMemcpyDeviceToDevice, st), "frame copy");
+        }
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_frame(isaacb_ctx* c, void* stream, uint8_t* rgba_host)
+    {
+        if(!c || !rgba_host)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_frame: null argument");
+        isaacb_status r = isaacb_update(c, stream);
+        if(r != ISAACB_OK)
+            return r;
+        r = isaacb_render(c, stream, nullptr);
+        if(r != ISAACB_OK)
+            return r;
+        cudaStream_t st = (cudaStream_t) stream;
+        const size_t bytes = size_t(c->desc.framebuffer[0]) * c->desc.framebuffer[1] * 4;
+        ISAACB_CUDA(c, cudaMemcpyAsync(rgba_host, c->color, bytes, cudaMemcpyDeviceToHost, st), "frame readback");
+        ISAACB_CUDA(c, cudaStreamSynchronize(st), "isaacb_frame");
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_framebuffer(isaacb_ctx* c, uint8_t** rgba_dev)
+    {
+        if(!c || !rgba_dev)
+            return ISAACB_INVALID_ARG;
+        *rgba_dev = reinterpret_cast<uint8_t*>(c->color);
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_minmax(isaacb_ctx* c, void* stream, float* mn, float* mx)
+    {
+        if(!c || !mn || !mx)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_minmax: null argument");
+        cudaStream_t st = (cudaStream_t) stream;
+        for(int s = 0; s < c->nTotal; ++s)
+        {
+            MinMaxParams p{};
+            p.g = c->g;
+            p.chain = c->chain[s];
+            p.fdim = int32_t(c->desc.feature_dim[s]);
+            p.partial = c->mmPartial;
+            p.keys = c->mmKeys;
+            if(s < c->nVol)
+            {
+                if(!c->src[s])
+                    return fail(c, ISAACB_NOT_READY, "isaacb_minmax: source without memory");
+                p.src = c->src[s];
+                p.particle = 0;
+            }
+            else
+            {
+                const ParticleSrc& P = c->part[s - c->nVol];
+                if(!c->partSet[s - c->nVol])
+                    return fail(c, ISAACB_NOT_READY, "isaacb_minmax: particle source without memory");
+                p.offsets = P.offsets;
+                p.attr = P.attr;
+                p.particle = 1;
+            }
+            launch_minmax(p, minmax_blocks(p), c->mmResult, st);
+            float res[2];
+            ISAACB_CUDA(c, cudaMemcpyAsync(res, c->mmResult, sizeof(res), cudaMemcpyDeviceToHost, st), "minmax read");
+            ISAACB_CUDA(c, cudaStreamSynchronize(st), "minmax");
+            if(res[0] == 0.0f || res[1] == 0.0f)
+            {
+                // +0 and -0 compare equal: the reference keeps the first in its scan order
+                const unsigned long long init[2] = {ULLONG_MAX, ULLONG_MAX};
+                ISAACB_CUDA(c, cudaMemcpyAsync(c->mmKeys, init, sizeof(init), cudaMemcpyHostToDevice, st), "keys");
+                launch_minmax_zero_keys(p, st);
+                unsigned long long keys[2];
+                ISAACB_CUDA(c, cudaMemcpyAsync(keys, c->mmKeys, sizeof(keys), cudaMemcpyDeviceToHost, st), "keys");
+                ISAACB_CUDA(c, cudaStreamSynchronize(st), "minmax zero order");
+                const float firstZero = keys[1] < keys[0] ? -0.0f : 0.0f;
+                if(res[0] == 0.0f)
+                    res[0] = firstZero;
+                if(res[1] == 0.0f)
+                    res[1] = firstZero;
+            }
+            mn[s] = res[0];
+            mx[s] = res[1];
+        }
+        ISAACB_CUDA(c, cudaGetLastError(), "isaacb_minmax");
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_get_gbuffer(isaacb_ctx* c, void* stream, float* depth, float* normal, float* ao)
+    {
+        if(!c)
+            return ISAACB_INVALID_ARG;
+        cudaStream_t st = (cudaStream_t) stream;
+        const size_t npix = size_t(c->desc.framebuffer[0]) * c->desc.framebuffer[1];
+        if(depth)
+            ISAACB_CUDA(c, cudaMemcpyAsync(depth, c->depth, npix * 4, cudaMemcpyDeviceToHost, st), "depth");
+        if(normal)
+            ISAACB_CUDA(c, cudaMemcpyAsync(normal, c->normal, npix * 12, cudaMemcpyDeviceToHost, st), "normal");
+        if(ao)
+            ISAACB_CUDA(c, cudaMemcpyAsync(ao, c->ao, npix * 4, cudaMemcpyDeviceToHost, st), "ao");
+        ISAACB_CUDA(c, cudaStreamSynchronize(st), "gbuffer");
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_get_combined(isaacb_ctx* c, void* stream, uint8_t* volume, uint8_t* iso)
+    {
+        if(!c)
+            return ISAACB_INVALID_ARG;
+        cudaStream_t st = (cudaStream_t) stream;
+        const size_t n = size_t(c->g.ls[0]) * c->g.ls[1] * c->g.ls[2];
+        if(volume)
+        {
+            uint32_t* tmp = nullptr;
+            ISAACB_CUDA(c, cudaMalloc(&tmp, n * 4), "unbrick buffer");
+            launch_unbrick(c->g, c->volQ, tmp, st);
+            cudaError_t e = cudaMemcpyAsync(volume, tmp, n * 4, cudaMemcpyDeviceToHost, st);
+            if(e == cudaSuccess)
+                e = cudaStreamSynchronize(st);
+            cudaFree(tmp);
+            if(e != cudaSuccess)
+                return cuda_fail(c, e, "combined volume readback");
+        }
+        if(iso)
+        {
+            ISAACB_CUDA(c, cudaMemcpyAsync(iso, c->isoLin, n * 4, cudaMemcpyDeviceToHost, st), "iso readback");
+            ISAACB_CUDA(c, cudaStreamSynchronize(st), "iso readback");
+        }
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_get_counters(isaacb_ctx* c, void* stream, uint64_t* vol, uint64_t* iso)
+    {
+        if(!c)
+            return ISAACB_INVALID_ARG;
+        unsigned long long h[2] = {0, 0};
+        cudaStream_t st = (cudaStream_t) stream;
+        ISAACB_CUDA(c, cudaMemcpyAsync(h, c->counters, sizeof(h), cudaMemcpyDeviceToHost, st), "counters");
+        ISAACB_CUDA(c, cudaStreamSynchronize(st), "counters");
+        if(vol)
+            *vol = h[0];
+        if(iso)
+            *iso = h[1];
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_set_timing(isaacb_ctx* c, int32_t on)
+    {
+        if(!c)
+            return ISAACB_INVALID_ARG;
+        if(on && !c->ev[0])
+            for(auto& e : c->ev)
+                ISAACB_CUDA(c, cudaEventCreate(&e), "timing events");
+        c->timing = on != 0;
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_get_timing(isaacb_ctx* c, void* stream, float* ms)
+    {
+        if(!c || !ms)
+            return ISAACB_INVALID_ARG;
+        ISAACB_CUDA(c, cudaStreamSynchronize((cudaStream_t) stream), "timing sync");
+        for(int k = 0; k < ISAACB_TIMING_SLOTS; ++k)
+        {
+            ms[k] = 0.0f;
+            if(c->timing && c->evUsed[k])
+                ISAACB_CUDA(c, cudaEventElapsedTime(&ms[k], c->ev[2 * k], c->ev[2 * k + 1]), "timing read");
+        }
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_get_launch_count(isaacb_ctx* c, uint32_t* upd, uint32_t* ren)
+    {
+        if(!c)
+            return ISAACB_INVALID_ARG;
+        if(upd)
+            *upd = c->updateLaunches;
+        if(ren)
+            *ren = c->renderLaunches;
+        return ISAACB_OK;
+    }
+}

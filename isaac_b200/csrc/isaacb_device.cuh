@@ -1,0 +1,545 @@
+// Device-side building blocks of the B200 ISAAC hot path: parameter structs,
+// glm-semantics float helpers, the functor-chain interpreter, ray setup and
+// the brick samplers.
+//
+// Exactness: every translation unit that includes this header is compiled with
+// --fmad=false, so plain float expressions round exactly like the reference's
+// CPU backend (no fused multiply-add).  Where a kernel trades that exactness
+// for speed it calls fmaf() explicitly and says so.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace isaacb
+{
+    constexpr int kMaxSources = 16;
+    constexpr int kMaxFunctors = 3;
+    constexpr int kMaxClip = 16;
+    // Quad-packed apron brick: 8x8 (x,y) slots x 9 z-planes.  Slot (lx,ly,lz) of
+    // brick (bx,by,bz) holds the four texels (x0,y0),(x0+1,y0),(x0,y0+1),(x0+1,y0+1)
+    // of plane z, with x0 = 8bx-1+lx, y0 = 8by-1+ly, z = 8bz-1+lz, each clamped to
+    // the volume.  A trilinear footprint whose base texel is (x0,y0,z0) is the two
+    // slots (lx,ly,lz) and (lx,ly,lz+1) of one brick.
+    constexpr int kSlotsPerBrick = 576;
+    constexpr int kApron = 9;
+
+    enum Op : int32_t
+    {
+        OP_IDEM = 0,
+        OP_ADD = 1,
+        OP_MUL = 2,
+        OP_LENGTH = 3,
+        OP_POW = 4,
+        OP_SUM = 5
+    };
+
+    struct Chain
+    {
+        int32_t op[kMaxFunctors];
+        float p[4 * kMaxFunctors];
+    };
+
+    // SimulationSizeStruct (lib/isaac/isaac_types.hpp:119-131) with the integer
+    // values the reference stores in size_t / int vectors.
+    struct Geom
+    {
+        int32_t gs[3], ls[3], lps[3], pos[3], gss[3], lss[3], posS[3];
+        int32_t maxGss;
+        int32_t nb[3]; // bricks per axis = (ls >> 3) + 1
+    };
+
+    __host__ __device__ inline int32_t bricks_per_axis(int32_t l)
+    {
+        return (l >> 3) + 1;
+    }
+
+    // ------------------------------------------------------------- glm semantics
+    __device__ __forceinline__ float gmin(float a, float b)
+    {
+        return (b < a) ? b : a;
+    }
+    __device__ __forceinline__ float gmax(float a, float b)
+    {
+        return (a < b) ? b : a;
+    }
+    __device__ __forceinline__ float gclamp(float x, float lo, float hi)
+    {
+        return gmin(gmax(x, lo), hi);
+    }
+    __device__ __forceinline__ float gsign(float x)
+    {
+        return float((0.0f < x) ? 1 : 0) - float((x < 0.0f) ? 1 : 0);
+    }
+    __device__ __forceinline__ float gfract(float x)
+    {
+        return x - floorf(x);
+    }
+    __device__ __forceinline__ int iclamp(int x, int lo, int hi)
+    {
+        return min(max(x, lo), hi);
+    }
+    // float -> int conversion of the GPU (saturating, NaN -> 0)
+    __device__ __forceinline__ int f2i(float x)
+    {
+        return __float2int_rz(x);
+    }
+
+    __device__ __forceinline__ float3 f3(float x, float y, float z)
+    {
+        return make_float3(x, y, z);
+    }
+    __device__ __forceinline__ float3 add3(float3 a, float3 b)
+    {
+        return f3(a.x + b.x, a.y + b.y, a.z + b.z);
+    }
+    __device__ __forceinline__ float3 sub3(float3 a, float3 b)
+    {
+        return f3(a.x - b.x, a.y - b.y, a.z - b.z);
+    }
+    __device__ __forceinline__ float3 mul3(float3 a, float3 b)
+    {
+        return f3(a.x * b.x, a.y * b.y, a.z * b.z);
+    }
+    __device__ __forceinline__ float3 muls3(float3 a, float s)
+    {
+        return f3(a.x * s, a.y * s, a.z * s);
+    }
+    __device__ __forceinline__ float3 smul3(float s, float3 a)
+    {
+        return f3(s * a.x, s * a.y, s * a.z);
+    }
+    __device__ __forceinline__ float3 div3(float3 a, float3 b)
+    {
+        return f3(a.x / b.x, a.y / b.y, a.z / b.z);
+    }
+    __device__ __forceinline__ float3 divs3(float3 a, float s)
+    {
+        return f3(a.x / s, a.y / s, a.z / s);
+    }
+    __device__ __forceinline__ float3 neg3(float3 a)
+    {
+        return f3(-a.x, -a.y, -a.z);
+    }
+    __device__ __forceinline__ float dot3(float3 a, float3 b)
+    {
+        float tx = a.x * b.x, ty = a.y * b.y, tz = a.z * b.z;
+        return (tx + ty) + tz;
+    }
+    __device__ __forceinline__ float length3(float3 a)
+    {
+        return sqrtf(dot3(a, a));
+    }
+    __device__ __forceinline__ float3 normalize3(float3 a)
+    {
+        float inv = 1.0f / sqrtf(dot3(a, a));
+        return muls3(a, inv);
+    }
+    __device__ __forceinline__ float comp(float3 v, int i)
+    {
+        return i == 0 ? v.x : (i == 1 ? v.y : v.z);
+    }
+
+    // transformColor (lib/isaac/isaac_helper.hpp:71-79)
+    __device__ __forceinline__ uint32_t byte_of(float v)
+    {
+        return (uint32_t) min(max(f2i(gclamp(v, 0.0f, 1.0f) * 255.0f), 0), 255);
+    }
+    __device__ __forceinline__ uchar4 to_byte4(float4 c)
+    {
+        return make_uchar4(byte_of(c.x), byte_of(c.y), byte_of(c.z), byte_of(c.w));
+    }
+    __device__ __forceinline__ float4 from_byte4(uchar4 b)
+    {
+        return make_float4(float(b.x) / 255.0f, float(b.y) / 255.0f, float(b.z) / 255.0f, float(b.w) / 255.0f);
+    }
+
+    // ------------------------------------------------------------- functor chain
+    // generateFunctorChain (lib/isaac/isaac_functor_chain.hpp:95-108) as a
+    // register interpreter over the bytecode the host parser produced; the
+    // reference dispatches the same chain through a device function-pointer table.
+    __device__ __forceinline__ float dotN(const float (&v)[4], int n)
+    {
+        if(n == 1)
+            return v[0] * v[0];
+        if(n == 2)
+        {
+            float a = v[0] * v[0], b = v[1] * v[1];
+            return a + b;
+        }
+        if(n == 3)
+        {
+            float a = v[0] * v[0], b = v[1] * v[1], c = v[2] * v[2];
+            return (a + b) + c;
+        }
+        float a = v[0] * v[0], b = v[1] * v[1], c = v[2] * v[2], d = v[3] * v[3];
+        return (a + b) + (c + d);
+    }
+
+    __device__ __forceinline__ float apply_chain(float (&v)[4], int dim, const Chain& ch)
+    {
+        int n = dim;
+#pragma unroll
+        for(int k = 0; k < kMaxFunctors; ++k)
+        {
+            const int op = ch.op[k];
+            if(op == OP_ADD)
+            {
+#pragma unroll
+                for(int i = 0; i < 4; ++i)
+                    if(i < n)
+                        v[i] = v[i] + ch.p[4 * k + i];
+            }
+            else if(op == OP_MUL)
+            {
+#pragma unroll
+                for(int i = 0; i < 4; ++i)
+                    if(i < n)
+                        v[i] = v[i] * ch.p[4 * k + i];
+            }
+            else if(op == OP_LENGTH)
+            {
+                v[0] = sqrtf(dotN(v, n));
+                n = 1;
+            }
+            else if(op == OP_POW)
+            {
+#pragma unroll
+                for(int i = 0; i < 4; ++i)
+                    if(i < n)
+                        v[i] = powf(v[i], ch.p[4 * k + i]);
+            }
+            else if(op == OP_SUM)
+            {
+                float r = 0.0f;
+#pragma unroll
+                for(int i = 0; i < 4; ++i)
+                    if(i < n)
+                        r += v[i];
+                v[0] = r;
+                n = 1;
+            }
+        }
+        return v[0];
+    }
+
+    // transfer-function index round(v*TS) clamped to [0,TS-1], NaN -> 0
+    // (lib/isaac/isaac_common_kernel.hpp:589-591)
+    __device__ __forceinline__ int lut_index(float v, int ts)
+    {
+        float c = gclamp(roundf(v * float(ts)), 0.0f, float(ts - 1));
+        return f2i(c);
+    }
+
+    // ------------------------------------------------------------- ray setup
+    struct Ray
+    {
+        float3 dir, start;
+        float startDepth, endDepth;
+        bool isClipped;
+        float3 clippingNormal;
+    };
+
+    struct View
+    {
+        float inv[16]; // inverse(P*MV), column major
+        int32_t W, H;
+        float3 scale;
+        int32_t clipCount;
+        float clipPos[kMaxClip][3];
+        float clipNrm[kMaxClip][3];
+    };
+
+    // pixelToRay (lib/isaac/isaac_common_kernel.hpp:51-92)
+    __device__ __forceinline__ Ray pixel_to_ray(const View& v, const Geom& g, int px, int py)
+    {
+        float vx = float(px) / float(v.W) * 2.0f - 1.0f;
+        float vy = float(py) / float(v.H) * 2.0f - 1.0f;
+        float s4[4], e4[4];
+#pragma unroll
+        for(int i = 0; i < 4; ++i)
+        {
+            float m0 = v.inv[0 * 4 + i] * vx;
+            float m1 = v.inv[1 * 4 + i] * vy;
+            float a0 = m0 + m1;
+            float ms = v.inv[2 * 4 + i] * -1.0f;
+            float me = v.inv[2 * 4 + i] * 1.0f;
+            float m3 = v.inv[3 * 4 + i] * 1.0f;
+            s4[i] = a0 + (ms + m3);
+            e4[i] = a0 + (me + m3);
+        }
+        Ray r;
+        float3 start = f3(s4[0] / s4[3], s4[1] / s4[3], s4[2] / s4[3]);
+        float3 end = f3(e4[0] / e4[3], e4[1] / e4[3], e4[2] / e4[3]);
+        float maxSize = float(g.maxGss) * 0.5f;
+        start = muls3(start, maxSize);
+        end = muls3(end, maxSize);
+        r.start = start;
+        r.dir = normalize3(sub3(end, start));
+        r.isClipped = false;
+        r.clippingNormal = f3(0, 0, 0);
+        r.startDepth = r.endDepth = 0.0f;
+        return r;
+    }
+
+    // clipRay (lib/isaac/isaac_common_kernel.hpp:94-193)
+    __device__ __forceinline__ bool clip_ray(Ray& ray, const View& v, const Geom& g)
+    {
+        float off[3];
+#pragma unroll
+        for(int i = 0; i < 3; ++i)
+            off[i] = float(g.gss[i] / 2 - g.posS[i]);
+        ray.start = add3(ray.start, f3(off[0], off[1], off[2]));
+        float bbMin[3], bbMax[3];
+        float st[3] = {ray.start.x, ray.start.y, ray.start.z};
+        float dr[3] = {ray.dir.x, ray.dir.y, ray.dir.z};
+#pragma unroll
+        for(int i = 0; i < 3; ++i)
+        {
+            int mnl = max(0, -g.posS[i]);
+            int mxl = min(g.lss[i], g.gss[i] - g.posS[i]);
+            float a = (float(mnl) - st[i]) / dr[i];
+            float b = (float(mxl) - st[i]) / dr[i];
+            if(b < a)
+            {
+                float t = a;
+                a = b;
+                b = t;
+            }
+            bbMin[i] = a;
+            bbMax[i] = b;
+        }
+        ray.startDepth = gmax(bbMin[0], gmax(bbMin[1], bbMin[2]));
+        ray.endDepth = gmin(bbMax[0], gmin(bbMax[1], bbMax[2]));
+        float cn[3] = {0, 0, 0};
+#pragma unroll
+        for(int i = 0; i < 3; ++i)
+        {
+            float sign = gsign(dr[i]);
+            bool outerLow = g.pos[i] == 0 && (sign + 1.0f) != 0.0f;
+            bool outerHigh = g.pos[i] + g.ls[i] == g.gs[i] && (sign - 1.0f) != 0.0f;
+            if(bbMin[i] == ray.startDepth && (outerLow || outerHigh))
+            {
+                ray.isClipped = true;
+                cn[i] = sign;
+            }
+        }
+        ray.clippingNormal = f3(cn[0], cn[1], cn[2]);
+        for(int i = 0; i < v.clipCount; ++i)
+        {
+            float3 n = f3(v.clipNrm[i][0], v.clipNrm[i][1], v.clipNrm[i][2]);
+            float3 p = f3(
+                v.clipPos[i][0] * float(g.gss[0]) * 0.5f + off[0],
+                v.clipPos[i][1] * float(g.gss[1]) * 0.5f + off[1],
+                v.clipPos[i][2] * float(g.gss[2]) * 0.5f + off[2]);
+            float d = dot3(ray.dir, n);
+            float depth = (dot3(p, n) - dot3(ray.start, n)) / d;
+            if(d > 0.0f)
+            {
+                if(ray.endDepth < depth)
+                    return false;
+                if(ray.startDepth <= depth)
+                {
+                    ray.clippingNormal = n;
+                    ray.isClipped = true;
+                    ray.startDepth = depth;
+                }
+            }
+            else
+            {
+                if(ray.startDepth > depth)
+                    return false;
+                if(ray.endDepth > depth)
+                    ray.endDepth = depth;
+            }
+        }
+        ray.startDepth = gmax(ray.startDepth, 0.002f);
+        if(ray.startDepth > ray.endDepth || isinf(ray.startDepth) || isinf(ray.endDepth))
+            return false;
+        return true;
+    }
+
+    // ray-march preamble shared by the volume and iso kernels
+    // (lib/isaac/isaac_volume_kernel.hpp:56-65)
+    struct March
+    {
+        float stepU, factor;
+        int startSteps, endSteps;
+        float3 stepVec, startU;
+    };
+    __device__ __forceinline__ March march_setup(const Ray& ray, const Geom& g, float3 scale, float step)
+    {
+        March m;
+        float minSize = float(min(g.gs[0], min(g.gs[1], g.gs[2])));
+        m.stepU = step * (length3(ray.dir) / length3(div3(ray.dir, scale)));
+        m.factor = m.stepU / minSize * 2.0f;
+        m.startSteps = f2i(ceilf(ray.startDepth / m.stepU));
+        m.endSteps = f2i(floorf(ray.endDepth / m.stepU));
+        m.stepVec = div3(smul3(m.stepU, ray.dir), scale);
+        m.startU = div3(ray.start, scale);
+        return m;
+    }
+    __device__ __forceinline__ float3 march_pos(const March& m, int i)
+    {
+        return add3(m.startU, muls3(m.stepVec, float(i)));
+    }
+
+    // ------------------------------------------------------------- brick addressing
+    __device__ __forceinline__ size_t brick_slot(const Geom& g, int x0, int y0, int z0)
+    {
+        // x0 in [-1, L-1]: base texel of a trilinear footprint
+        int ax = x0 + 1, ay = y0 + 1, az = z0 + 1;
+        size_t brick = (size_t(az >> 3) * g.nb[1] + size_t(ay >> 3)) * g.nb[0] + size_t(ax >> 3);
+        return brick * kSlotsPerBrick + size_t((az & 7) * 64 + (ay & 7) * 8 + (ax & 7));
+    }
+
+    __device__ __forceinline__ float byte_f(uint32_t w, int c)
+    {
+        return float((w >> (8 * c)) & 0xffu);
+    }
+
+    // linear(o, a, b) = a*(1-o) + b*o (lib/isaac/isaac_helper.hpp:124-128)
+    __device__ __forceinline__ float lin(float o, float a, float b)
+    {
+        return a * (1.0f - o) + b * o;
+    }
+
+    // trilinear over the 8 texels of a footprint, z first then y then x
+    // (lib/isaac/isaac_helper.hpp:138-144).  q0 = plane z0, q1 = plane z0+1;
+    // each .x/.y/.z/.w = (x0,y0),(x0+1,y0),(x0,y0+1),(x0+1,y0+1).
+    __device__ __forceinline__ float tri_q(float fx, float fy, float fz, float d000, float d100, float d010, float d110,
+                                           float d001, float d101, float d011, float d111)
+    {
+        float A = lin(fy, lin(fz, d000, d001), lin(fz, d010, d011));
+        float B = lin(fy, lin(fz, d100, d101), lin(fz, d110, d111));
+        return lin(fx, A, B);
+    }
+
+    // Sampler<LINEAR|NEAREST, CLAMP, normalized> on the combined RGBA8 texture
+    // (lib/isaac/isaac_texture.hpp:140-259), exact arithmetic.
+    __device__ __forceinline__ float4 sample_rgba8(const uint4* __restrict__ q, const Geom& g, float3 pos, bool linear)
+    {
+        if(linear)
+        {
+            float cx = pos.x - 0.5f, cy = pos.y - 0.5f, cz = pos.z - 0.5f;
+            float flx = floorf(cx), fly = floorf(cy), flz = floorf(cz);
+            float fx = cx - flx, fy = cy - fly, fz = cz - flz;
+            int ix = iclamp(f2i(flx), -1, g.ls[0] - 1);
+            int iy = iclamp(f2i(fly), -1, g.ls[1] - 1);
+            int iz = iclamp(f2i(flz), -1, g.ls[2] - 1);
+            size_t s = brick_slot(g, ix, iy, iz);
+            uint4 a = __ldg(q + s);
+            uint4 b = __ldg(q + s + 64);
+            float r[4];
+#pragma unroll
+            for(int c = 0; c < 4; ++c)
+                r[c] = tri_q(
+                    fx,
+                    fy,
+                    fz,
+                    byte_f(a.x, c),
+                    byte_f(a.y, c),
+                    byte_f(a.z, c),
+                    byte_f(a.w, c),
+                    byte_f(b.x, c),
+                    byte_f(b.y, c),
+                    byte_f(b.z, c),
+                    byte_f(b.w, c));
+            return make_float4(r[0] / 255.0f, r[1] / 255.0f, r[2] / 255.0f, r[3] / 255.0f);
+        }
+        int ix = iclamp(f2i(pos.x), 0, g.ls[0] - 1);
+        int iy = iclamp(f2i(pos.y), 0, g.ls[1] - 1);
+        int iz = iclamp(f2i(pos.z), 0, g.ls[2] - 1);
+        uint32_t w = reinterpret_cast<const uint32_t*>(q)[brick_slot(g, ix, iy, iz) * 4];
+        return make_float4(byte_f(w, 0) / 255.0f, byte_f(w, 1) / 255.0f, byte_f(w, 2) / 255.0f, byte_f(w, 3) / 255.0f);
+    }
+
+    // alpha channel of the combined iso texture (alpha quads, 4 bytes per slot)
+    __device__ __forceinline__ float sample_alpha(const uint32_t* __restrict__ q, const Geom& g, float3 pos, bool linear)
+    {
+        if(linear)
+        {
+            float cx = pos.x - 0.5f, cy = pos.y - 0.5f, cz = pos.z - 0.5f;
+            float flx = floorf(cx), fly = floorf(cy), flz = floorf(cz);
+            float fx = cx - flx, fy = cy - fly, fz = cz - flz;
+            int ix = iclamp(f2i(flx), -1, g.ls[0] - 1);
+            int iy = iclamp(f2i(fly), -1, g.ls[1] - 1);
+            int iz = iclamp(f2i(flz), -1, g.ls[2] - 1);
+            size_t s = brick_slot(g, ix, iy, iz);
+            uint32_t a = __ldg(q + s);
+            uint32_t b = __ldg(q + s + 64);
+            float r = tri_q(
+                fx,
+                fy,
+                fz,
+                byte_f(a, 0),
+                byte_f(a, 1),
+                byte_f(a, 2),
+                byte_f(a, 3),
+                byte_f(b, 0),
+                byte_f(b, 1),
+                byte_f(b, 2),
+                byte_f(b, 3));
+            return r / 255.0f;
+        }
+        int ix = iclamp(f2i(pos.x), 0, g.ls[0] - 1);
+        int iy = iclamp(f2i(pos.y), 0, g.ls[1] - 1);
+        int iz = iclamp(f2i(pos.z), 0, g.ls[2] - 1);
+        uint32_t w = __ldg(q + brick_slot(g, ix, iy, iz));
+        return byte_f(w, 0) / 255.0f;
+    }
+
+    // full RGBA8 sample of a linear (x fastest) texture, exact arithmetic
+    __device__ __forceinline__ float4 sample_linear_rgba8(
+        const uint32_t* __restrict__ t,
+        const Geom& g,
+        float3 pos,
+        bool linear)
+    {
+        const int LX = g.ls[0], LY = g.ls[1], LZ = g.ls[2];
+        auto tex = [&](int x, int y, int z) -> uint32_t {
+            x = iclamp(x, 0, LX - 1);
+            y = iclamp(y, 0, LY - 1);
+            z = iclamp(z, 0, LZ - 1);
+            return __ldg(t + (size_t(z) * LY + y) * LX + x);
+        };
+        if(linear)
+        {
+            float cx = pos.x - 0.5f, cy = pos.y - 0.5f, cz = pos.z - 0.5f;
+            float flx = floorf(cx), fly = floorf(cy), flz = floorf(cz);
+            float fx = cx - flx, fy = cy - fly, fz = cz - flz;
+            int ix = f2i(flx), iy = f2i(fly), iz = f2i(flz);
+            uint32_t d000 = tex(ix, iy, iz), d100 = tex(ix + 1, iy, iz), d010 = tex(ix, iy + 1, iz),
+                     d110 = tex(ix + 1, iy + 1, iz);
+            uint32_t d001 = tex(ix, iy, iz + 1), d101 = tex(ix + 1, iy, iz + 1), d011 = tex(ix, iy + 1, iz + 1),
+                     d111 = tex(ix + 1, iy + 1, iz + 1);
+            float r[4];
+#pragma unroll
+            for(int c = 0; c < 4; ++c)
+                r[c] = tri_q(
+                    fx,
+                    fy,
+                    fz,
+                    byte_f(d000, c),
+                    byte_f(d100, c),
+                    byte_f(d010, c),
+                    byte_f(d110, c),
+                    byte_f(d001, c),
+                    byte_f(d101, c),
+                    byte_f(d011, c),
+                    byte_f(d111, c));
+            return make_float4(r[0] / 255.0f, r[1] / 255.0f, r[2] / 255.0f, r[3] / 255.0f);
+        }
+        uint32_t w = tex(f2i(pos.x), f2i(pos.y), f2i(pos.z));
+        return make_float4(byte_f(w, 0) / 255.0f, byte_f(w, 1) / 255.0f, byte_f(w, 2) / 255.0f, byte_f(w, 3) / 255.0f);
+    }
+
+    // pixel of a thread: a block of 256 threads covers 32x8 pixels and each warp an 8x4 tile
+    __device__ __forceinline__ void thread_pixel(int& px, int& py)
+    {
+        int t = threadIdx.x;
+        int w = t >> 5, l = t & 31;
+        px = blockIdx.x * 32 + (w & 3) * 8 + (l & 7);
+        py = blockIdx.y * 8 + (w >> 2) * 4 + (l >> 3);
+    }
+} // namespace isaacb

@@ -1,0 +1,138 @@
+// Internal launch interface between the C-ABI host code (api.cu) and the
+// kernel translation units.  Not installed; not part of the C ABI.
+#pragma once
+
+#include "isaacb_device.cuh"
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace isaacb
+{
+    // -------------------------------------------------------------- merge / update
+    struct MergeParams
+    {
+        Geom g;
+        int32_t nVol;
+        int32_t ts;
+        int32_t ditherMode;
+        int32_t writeIso;
+        const float* src[kMaxSources];
+        int32_t fdim[kMaxSources];
+        Chain chain[kMaxSources];
+        const float4* lut; // nTotal * ts, source s at s*ts
+        float weight[kMaxSources];
+        float iso[kMaxSources];
+        float totalWeight;
+        uint4* volQ; // combined volume, quad bricks
+        uint32_t* isoAQ; // combined iso alpha, quad bricks
+        uint32_t* isoLin; // combined iso RGBA8, linear
+        uint8_t* volFlag; // per brick: 1 if any texel (apron included) is non-zero
+        uint8_t* isoFlag; // per brick: max alpha byte (apron included)
+    };
+    void launch_merge(const MergeParams& p, cudaStream_t s);
+
+    // per-source renderer bricks: persistent sources keep their raw components,
+    // non-persistent sources their functor-chain value (UpdatePersistendTextureKernel)
+    struct SourceBrickParams
+    {
+        Geom g;
+        const float* src;
+        int32_t fdim; // components of the source
+        int32_t ncomp; // components stored (fdim or 1)
+        int32_t applyChain;
+        int32_t dtype; // 0 f32, 1 bf16, 2 f16
+        Chain chain;
+        void* out; // slots of ncomp*4 elements, component major
+    };
+    void launch_source_bricks(const SourceBrickParams& p, cudaStream_t s);
+
+    // quad bricks -> linear RGBA8 (diagnostics)
+    void launch_unbrick(const Geom& g, const uint4* volQ, uint32_t* out, cudaStream_t s);
+
+    // -------------------------------------------------------------- min / max
+    struct MinMaxParams
+    {
+        Geom g;
+        const float* src;
+        int32_t fdim;
+        Chain chain;
+        // particles
+        const uint32_t* offsets;
+        const float* attr;
+        int32_t particle;
+        float* partial; // 2 floats per block
+        unsigned long long* keys; // 4 keys: first +0 / -0 for min and max
+    };
+    int minmax_blocks(const MinMaxParams& p);
+    void launch_minmax(const MinMaxParams& p, int blocks, float* result, cudaStream_t s);
+    void launch_minmax_zero_keys(const MinMaxParams& p, cudaStream_t s);
+
+    // -------------------------------------------------------------- frame
+    struct ParticleSrc
+    {
+        const uint32_t* offsets;
+        const float* pos;
+        const float* attr;
+        const float* radius;
+        float constRadius;
+        int32_t fdim;
+        float weight;
+        int32_t lutBase;
+        Chain chain;
+    };
+
+    struct PerSourceSrc
+    {
+        const void* bricks;
+        int32_t dtype;
+        int32_t ncomp;
+        int32_t persistent;
+        int32_t fdim;
+        float weight;
+        float iso;
+        Chain chain;
+    };
+
+    struct FrameParams
+    {
+        View v;
+        Geom g;
+        int32_t ts;
+        int32_t interpolation;
+        float step;
+        float4 bgSwizzled; // (bg[3], bg[2], bg[1], 0)
+        float4 bg;
+        int32_t renderMode;
+        float aoWeight;
+        int32_t aoFilter;
+        float totalWeightAll;
+        const float4* lut;
+        // combined textures
+        const uint4* volQ;
+        const uint32_t* isoAQ;
+        const uint32_t* isoLin;
+        const uint8_t* volFlag;
+        const uint8_t* isoFlag;
+        // particles
+        int32_t nVol;
+        int32_t nPart;
+        float3 pscale;
+        ParticleSrc part[kMaxSources];
+        // per-source renderer
+        PerSourceSrc ps[kMaxSources];
+        // G-buffer
+        uchar4* color;
+        float* depth;
+        float* normal; // 3 floats per pixel
+        float* ao;
+        unsigned long long* counters; // [0] volume samples, [1] iso samples; null = off
+    };
+
+    void launch_clear_particles(const FrameParams& p, cudaStream_t s);
+    void launch_iso(const FrameParams& p, cudaStream_t s);
+    void launch_iso_per_source(const FrameParams& p, cudaStream_t s);
+    void launch_ssao(const FrameParams& p, cudaStream_t s);
+    void launch_shade_volume(const FrameParams& p, bool volume, cudaStream_t s);
+    void launch_shade_volume_per_source(const FrameParams& p, cudaStream_t s);
+} // namespace isaacb

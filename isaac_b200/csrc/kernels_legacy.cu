@@ -1,0 +1,300 @@
+// Frame kernels of the per-source renderer (the reference's legacy path,
+// ISAAC_RENDERER_LEGACY): every sample interpolates each source's own bricks,
+// applies its functor chain and transfer function and accumulates.
+//   getColorValue        lib/isaac/isaac_volume_kernel.hpp:101-168
+//   VolumeRenderKernel   lib/isaac/isaac_volume_kernel.hpp:302-432
+//   IsoStepRenderKernel  lib/isaac/isaac_iso_kernel.hpp:463-778
+//
+// Bricks hold FP32, BF16 or FP16 values; interpolation, chain, lookup and
+// compositing stay FP32.
+#include "isaacb_frame.cuh"
+
+#include <cfloat>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+namespace isaacb
+{
+    __device__ __forceinline__ float load_elem(const void* base, int dtype, size_t i)
+    {
+        if(dtype == 1)
+            return __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(base)[i]);
+        if(dtype == 2)
+            return __half2float(reinterpret_cast<const __half*>(base)[i]);
+        return __ldg(reinterpret_cast<const float*>(base) + i);
+    }
+
+    // one source's colour at pos (getColorValue)
+    __device__ float4 per_source_color(const FrameParams& p, int s, float3 pos, bool linear)
+    {
+        const PerSourceSrc& S = p.ps[s];
+        const Geom& g = p.g;
+        const int per = 4 * S.ncomp;
+        float v[4] = {0, 0, 0, 0};
+        float result;
+        if(linear)
+        {
+            const float cx = pos.x - 0.5f, cy = pos.y - 0.5f, cz = pos.z - 0.5f;
+            const float flx = floorf(cx), fly = floorf(cy), flz = floorf(cz);
+            const float fx = cx - flx, fy = cy - fly, fz = cz - flz;
+            int ix, iy, iz;
+            if(S.persistent)
+            {
+                // isaac_int(offsetPos) truncates; the mirror at the upper border equals a clamp
+                ix = f2i(cx);
+                iy = f2i(cy);
+                iz = f2i(cz);
+            }
+            else
+            {
+                ix = f2i(flx);
+                iy = f2i(fly);
+                iz = f2i(flz);
+            }
+            ix = iclamp(ix, -1, g.ls[0] - 1);
+            iy = iclamp(iy, -1, g.ls[1] - 1);
+            iz = iclamp(iz, -1, g.ls[2] - 1);
+            const size_t s0 = brick_slot(g, ix, iy, iz) * per;
+            const size_t s1 = s0 + size_t(64) * per;
+#pragma unroll
+            for(int c = 0; c < 4; ++c)
+            {
+                if(c < S.ncomp)
+                {
+                    v[c] = tri_q(
+                        fx,
+                        fy,
+                        fz,
+                        load_elem(S.bricks, S.dtype, s0 + 4 * c),
+                        load_elem(S.bricks, S.dtype, s0 + 4 * c + 1),
+                        load_elem(S.bricks, S.dtype, s0 + 4 * c + 2),
+                        load_elem(S.bricks, S.dtype, s0 + 4 * c + 3),
+                        load_elem(S.bricks, S.dtype, s1 + 4 * c),
+                        load_elem(S.bricks, S.dtype, s1 + 4 * c + 1),
+                        load_elem(S.bricks, S.dtype, s1 + 4 * c + 2),
+                        load_elem(S.bricks, S.dtype, s1 + 4 * c + 3));
+                }
+            }
+        }
+        else
+        {
+            const int ix = iclamp(f2i(pos.x), 0, g.ls[0] - 1);
+            const int iy = iclamp(f2i(pos.y), 0, g.ls[1] - 1);
+            const int iz = iclamp(f2i(pos.z), 0, g.ls[2] - 1);
+            const size_t s0 = brick_slot(g, ix, iy, iz) * per;
+#pragma unroll
+            for(int c = 0; c < 4; ++c)
+                if(c < S.ncomp)
+                    v[c] = load_elem(S.bricks, S.dtype, s0 + 4 * c);
+        }
+        if(S.persistent)
+            result = apply_chain(v, S.fdim, S.chain);
+        else
+            result = v[0];
+        return __ldg(p.lut + size_t(s) * p.ts + lut_index(result, p.ts));
+    }
+
+    // checkCoord (lib/isaac/isaac_volume_kernel.hpp:206-214) for guard 0
+    __device__ __forceinline__ float3 check_coord(const Geom& g, float3 c)
+    {
+        return f3(
+            gclamp(c.x, 0.0f, float(g.ls[0] - 1) - FLT_MIN),
+            gclamp(c.y, 0.0f, float(g.ls[1] - 1) - FLT_MIN),
+            gclamp(c.z, 0.0f, float(g.ls[2] - 1) - FLT_MIN));
+    }
+    __device__ __forceinline__ float4 accessor_value(const FrameParams& p, int s, float3 pos, bool linear)
+    {
+        if(p.ps[s].persistent)
+            pos = check_coord(p.g, pos);
+        return per_source_color(p, s, pos, linear);
+    }
+
+    // start/end step adjustment of the legacy kernels (lib/isaac/isaac_volume_kernel.hpp:362-376)
+    __device__ __forceinline__ bool inside_local(const Geom& g, float3 pos)
+    {
+        return !(pos.x < 0.0f || pos.y < 0.0f || pos.z < 0.0f || pos.x >= float(g.ls[0]) || pos.y >= float(g.ls[1])
+                 || pos.z >= float(g.ls[2]));
+    }
+    __device__ __forceinline__ void legacy_bounds(const Geom& g, March& m)
+    {
+        float3 pos = march_pos(m, m.startSteps);
+        while(!inside_local(g, pos) && m.startSteps <= m.endSteps)
+        {
+            m.startSteps++;
+            pos = march_pos(m, m.startSteps);
+        }
+        pos = march_pos(m, m.endSteps);
+        while(!inside_local(g, pos) && m.startSteps <= m.endSteps)
+        {
+            m.endSteps--;
+            pos = march_pos(m, m.endSteps);
+        }
+    }
+
+    __device__ __forceinline__ void count_warp(unsigned long long* ctr, unsigned long long n)
+    {
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+            n += __shfl_xor_sync(0xffffffffu, n, o);
+        if((threadIdx.x & 31) == 0 && n)
+            atomicAdd(ctr, n);
+    }
+
+    __global__ void __launch_bounds__(256) k_iso_per_source(const __grid_constant__ FrameParams p)
+    {
+        int px, py;
+        thread_pixel(px, py);
+        unsigned long long n = 0;
+        const bool linear = p.interpolation != 0;
+        bool any = false;
+        for(int s = 0; s < p.nVol; ++s)
+            any |= p.ps[s].iso != 0.0f;
+        if(any && px < p.v.W && py < p.v.H)
+        {
+            const size_t o = size_t(py) * p.v.W + px;
+            Ray ray = pixel_to_ray(p.v, p.g, px, py);
+            if(clip_ray(ray, p.v, p.g))
+            {
+                ray.endDepth = gmin(ray.endDepth, p.depth[o]);
+                if(!(ray.endDepth <= ray.startDepth))
+                {
+                    March m = march_setup(ray, p.g, p.v.scale, p.step);
+                    legacy_bounds(p.g, m);
+                    bool hit = false;
+                    float hitDepth = ray.endDepth;
+                    float4 hitColor = make_float4(0, 0, 0, 0);
+                    float3 hitNormal = f3(0, 0, 0);
+                    float oldValues[kMaxSources];
+                    for(int s = 0; s < kMaxSources; ++s)
+                        oldValues[s] = 0.0f;
+                    for(int i = m.startSteps; i <= m.endSteps && !hit; i++)
+                    {
+                        ++n;
+                        const float3 pos = march_pos(m, i);
+                        const bool first = ray.isClipped && i == m.startSteps;
+                        const float t = float(i) * m.stepU;
+                        for(int s = 0; s < p.nVol; ++s)
+                        {
+                            const float thr = p.ps[s].iso;
+                            if(thr == 0.0f)
+                                continue;
+                            const float value = accessor_value(p, s, pos, linear).w;
+                            const float prev = oldValues[s];
+                            oldValues[s] = value;
+                            if(value < thr)
+                                continue;
+                            float testDepth;
+                            if(first)
+                                testDepth = ray.startDepth;
+                            else
+                                testDepth = t + m.stepU * (thr - prev) / (value - prev);
+                            if(testDepth > hitDepth)
+                                continue;
+                            hitDepth = testDepth;
+                            hit = true;
+                            const float3 np = add3(ray.start, muls3(ray.dir, hitDepth));
+                            const float3 pu = div3(np, p.v.scale);
+                            hitColor = accessor_value(p, s, pu, linear);
+                            hitColor.w = 1.0f;
+                            float3 gr;
+                            gr.x = accessor_value(p, s, add3(pu, f3(1, 0, 0)), linear).w
+                                - accessor_value(p, s, sub3(pu, f3(1, 0, 0)), linear).w;
+                            gr.y = accessor_value(p, s, add3(pu, f3(0, 1, 0)), linear).w
+                                - accessor_value(p, s, sub3(pu, f3(0, 1, 0)), linear).w;
+                            gr.z = accessor_value(p, s, add3(pu, f3(0, 0, 1)), linear).w
+                                - accessor_value(p, s, sub3(pu, f3(0, 0, 1)), linear).w;
+                            float gl = length3(gr);
+                            if(first)
+                            {
+                                gr = ray.clippingNormal;
+                                gl = 1.0f;
+                            }
+                            hitNormal = divs3(neg3(gr), gl);
+                        }
+                    }
+                    if(hit)
+                    {
+                        p.color[o] = to_byte4(hitColor);
+                        p.normal[3 * o] = hitNormal.x;
+                        p.normal[3 * o + 1] = hitNormal.y;
+                        p.normal[3 * o + 2] = hitNormal.z;
+                        p.depth[o] = hitDepth;
+                    }
+                }
+            }
+        }
+        if(p.counters)
+            count_warp(p.counters + 1, n);
+    }
+
+    void launch_iso_per_source(const FrameParams& p, cudaStream_t s)
+    {
+        dim3 grid((p.v.W + 31) / 32, (p.v.H + 7) / 8);
+        k_iso_per_source<<<grid, 256, 0, s>>>(p);
+    }
+
+    __global__ void __launch_bounds__(256) k_shade_volume_per_source(const __grid_constant__ FrameParams p)
+    {
+        int px, py;
+        thread_pixel(px, py);
+        unsigned long long n = 0;
+        const bool linear = p.interpolation != 0;
+        if(px < p.v.W && py < p.v.H)
+        {
+            const size_t o = size_t(py) * p.v.W + px;
+            shade_pixel(p, px, py, o);
+            bool any = false;
+            for(int s = 0; s < p.nVol; ++s)
+                any |= p.ps[s].weight != 0.0f;
+            Ray ray = pixel_to_ray(p.v, p.g, px, py);
+            if(any && clip_ray(ray, p.v, p.g))
+            {
+                ray.endDepth = gmin(ray.endDepth, p.depth[o]);
+                if(!(ray.endDepth <= ray.startDepth))
+                {
+                    March m = march_setup(ray, p.g, p.v.scale, p.step);
+                    legacy_bounds(p.g, m);
+                    float4 value = make_float4(0, 0, 0, 0);
+                    float4 color = make_float4(0, 0, 0, 0);
+                    for(int i = m.startSteps; i <= m.endSteps; i++)
+                    {
+                        ++n;
+                        const float3 pos = march_pos(m, i);
+                        for(int s = 0; s < p.nVol; ++s)
+                        {
+                            const float w = p.ps[s].weight;
+                            if(w == 0.0f)
+                                continue;
+                            float4 c = per_source_color(p, s, pos, linear);
+                            c.w *= w;
+                            value.x += c.x * c.w;
+                            value.y += c.y * c.w;
+                            value.z += c.z * c.w;
+                            value.w += c.w;
+                        }
+                        const float oma = 1.0f - color.w;
+                        value = make_float4(value.x * m.factor, value.y * m.factor, value.z * m.factor, value.w * m.factor);
+                        color.x += oma * value.x;
+                        color.y += oma * value.y;
+                        color.z += oma * value.z;
+                        color.w += oma * value.w;
+                        if(color.w > 0.99f)
+                            break;
+                    }
+                    const float4 solid = from_byte4(p.color[o]);
+                    const float r = 1.0f - color.w;
+                    color = make_float4(color.x + r * solid.x, color.y + r * solid.y, color.z + r * solid.z, color.w + r * solid.w);
+                    p.color[o] = to_byte4(color);
+                }
+            }
+        }
+        if(p.counters)
+            count_warp(p.counters, n);
+    }
+
+    void launch_shade_volume_per_source(const FrameParams& p, cudaStream_t s)
+    {
+        dim3 grid((p.v.W + 31) / 32, (p.v.H + 7) / 8);
+        k_shade_volume_per_source<<<grid, 256, 0, s>>>(p);
+    }
+} // namespace isaacb

@@ -1,0 +1,260 @@
+// Buffer update kernels: the merge of all volume sources into the combined
+// RGBA8 volume / iso textures (MergeToCombinedTextureKernel,
+// lib/isaac/isaac_common_kernel.hpp:553-759) and the per-source bricks of the
+// per-source renderer (UpdatePersistendTextureKernel,
+// lib/isaac/isaac_common_kernel.hpp:432-451).
+//
+// One CTA builds one quad-packed apron brick.  It evaluates the 9^3 texels of
+// the brick (its 8^3 voxels plus the apron on the low side, clamped at the
+// volume border) once into shared memory, then writes the 576 slots as
+// coalesced 16-byte stores.  The per-brick flags feed empty-space skipping.
+#include "isaacb_internal.h"
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+namespace isaacb
+{
+    // 4x4x4 ordered dither masks (lib/isaac/isaac_dither_kernel.hpp:22-40)
+    __constant__ uint8_t c_dither1[64]
+        = {17, 46, 55, 1,  57, 7,  38, 31, 9,  52, 2,  54, 36, 26, 19, 44, 53, 20, 47, 22, 29, 60,
+           62, 12, 45, 14, 26, 33, 8,  39, 11, 63, 13, 56, 6,  50, 40, 32, 23, 48, 21, 42, 51, 5,
+           61, 3,  34, 27, 41, 10, 30, 37, 4,  35, 15, 59, 49, 24, 43, 18, 25, 64, 58, 16};
+    __constant__ uint8_t c_dither2[64]
+        = {13, 61, 45, 51, 59, 39, 16, 40, 10, 49, 2,  46, 36, 43, 15, 60, 26, 52, 23, 9,  32, 6,
+           31, 0,  54, 21, 58, 24, 17, 5,  28, 38, 56, 41, 11, 63, 14, 47, 37, 48, 42, 62, 12, 18,
+           3,  35, 50, 44, 19, 1,  20, 34, 29, 25, 57, 4,  22, 8,  33, 53, 30, 55, 27, 7};
+
+    // applyDither3D (lib/isaac/isaac_dither_kernel.hpp:7-329), modes 0, 1, 2
+    __device__ __forceinline__ uint32_t dither_rgba(int mode, int x, int y, int z, float4 c)
+    {
+        float v[4] = {c.x, c.y, c.z, c.w};
+        uint32_t out = 0;
+        if(mode == 0)
+        {
+#pragma unroll
+            for(int i = 0; i < 4; ++i)
+            {
+                int b = f2i(roundf(gclamp(v[i], 0.0f, 1.0f) * 255.0f));
+                out |= uint32_t(min(max(b, 0), 255)) << (8 * i);
+            }
+            return out;
+        }
+        const uint8_t* mask = (mode == 2) ? c_dither2 : c_dither1;
+        float d = float(mask[x % 4 + (y % 4) * 4 + (z % 4) * 16]) / 64.0f;
+#pragma unroll
+        for(int i = 0; i < 4; ++i)
+        {
+            float s = v[i] * 255.0f;
+            int ci = f2i(s);
+            ci += (gfract(s) > d) ? 1 : 0;
+            out |= uint32_t(min(max(ci, 0), 255)) << (8 * i);
+        }
+        return out;
+    }
+
+    __device__ __forceinline__ void read_voxel(const float* __restrict__ src, int fdim, size_t idx, float (&v)[4])
+    {
+        const float* p = src + idx * fdim;
+        v[0] = __ldg(p);
+        v[1] = fdim > 1 ? __ldg(p + 1) : 0.0f;
+        v[2] = fdim > 2 ? __ldg(p + 2) : 0.0f;
+        v[3] = fdim > 3 ? __ldg(p + 3) : 0.0f;
+    }
+
+    __global__ void __launch_bounds__(256) k_merge(const __grid_constant__ MergeParams p)
+    {
+        __shared__ uint32_t volS[kApron * kApron * kApron];
+        __shared__ uint32_t isoS[kApron * kApron * kApron];
+        __shared__ int isoMax;
+        const Geom& g = p.g;
+        const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
+        if(threadIdx.x == 0)
+            isoMax = 0;
+        __syncthreads();
+        int anyVol = 0;
+        int myIsoMax = 0;
+        for(int t = threadIdx.x; t < kApron * kApron * kApron; t += blockDim.x)
+        {
+            const int lx = t % kApron, ly = (t / kApron) % kApron, lz = t / (kApron * kApron);
+            const int x = iclamp(bx * 8 - 1 + lx, 0, g.ls[0] - 1);
+            const int y = iclamp(by * 8 - 1 + ly, 0, g.ls[1] - 1);
+            const int z = iclamp(bz * 8 - 1 + lz, 0, g.ls[2] - 1);
+            const size_t idx = (size_t(z) * g.ls[1] + y) * g.ls[0] + x;
+            float4 vc = make_float4(0, 0, 0, 0), ic = make_float4(0, 0, 0, 0);
+            for(int s = 0; s < p.nVol; ++s)
+            {
+                const float vw = p.weight[s];
+                const float it = p.iso[s];
+                if(!(vw + it > 0.0f))
+                    continue;
+                float v[4];
+                read_voxel(p.src[s], p.fdim[s], idx, v);
+                const float val = apply_chain(v, p.fdim[s], p.chain[s]);
+                const float4 c = __ldg(p.lut + size_t(s) * p.ts + lut_index(val, p.ts));
+                if(vw > 0.0f)
+                {
+                    float a = c.w * vw;
+                    vc.x += c.x * a;
+                    vc.y += c.y * a;
+                    vc.z += c.z * a;
+                    vc.w += a;
+                }
+                if(it > 0.0f)
+                {
+                    float a = c.w / it * 0.5f;
+                    if(ic.w < a)
+                        ic = make_float4(c.x, c.y, c.z, a);
+                }
+            }
+            vc = make_float4(vc.x / p.totalWeight, vc.y / p.totalWeight, vc.z / p.totalWeight, vc.w / p.totalWeight);
+            const uint32_t vb = dither_rgba(p.ditherMode, x, y, z, vc);
+            volS[t] = vb;
+            anyVol |= vb != 0u;
+            if(p.writeIso)
+            {
+                float iv[4] = {ic.x, ic.y, ic.z, ic.w};
+                uint32_t ib = 0;
+#pragma unroll
+                for(int i = 0; i < 4; ++i)
+                {
+                    int b = f2i(roundf(gclamp(iv[i], 0.0f, 1.0f) * 255.0f));
+                    ib |= uint32_t(min(max(b, 0), 255)) << (8 * i);
+                }
+                isoS[t] = ib;
+                myIsoMax = max(myIsoMax, int(ib >> 24));
+            }
+        }
+        if(p.writeIso)
+            atomicMax(&isoMax, myIsoMax);
+        anyVol = __syncthreads_or(anyVol);
+        const size_t brick = (size_t(bz) * g.nb[1] + by) * g.nb[0] + bx;
+        if(threadIdx.x == 0)
+        {
+            p.volFlag[brick] = anyVol ? 1 : 0;
+            if(p.writeIso)
+                p.isoFlag[brick] = uint8_t(isoMax);
+        }
+        for(int s = threadIdx.x; s < kSlotsPerBrick; s += blockDim.x)
+        {
+            const int lx = s & 7, ly = (s >> 3) & 7, lz = s >> 6;
+            const int t = (lz * kApron + ly) * kApron + lx;
+            uint4 q = make_uint4(volS[t], volS[t + 1], volS[t + kApron], volS[t + kApron + 1]);
+            p.volQ[brick * kSlotsPerBrick + s] = q;
+            if(p.writeIso)
+            {
+                uint32_t a = (isoS[t] >> 24) | ((isoS[t + 1] >> 24) << 8) | ((isoS[t + kApron] >> 24) << 16)
+                    | ((isoS[t + kApron + 1] >> 24) << 24);
+                p.isoAQ[brick * kSlotsPerBrick + s] = a;
+            }
+        }
+        if(p.writeIso)
+        {
+            // interior voxels 8b..8b+7 of this brick in the linear iso texture
+            for(int t = threadIdx.x; t < 512; t += blockDim.x)
+            {
+                const int lx = t & 7, ly = (t >> 3) & 7, lz = t >> 6;
+                const int x = bx * 8 + lx, y = by * 8 + ly, z = bz * 8 + lz;
+                if(x < g.ls[0] && y < g.ls[1] && z < g.ls[2])
+                    p.isoLin[(size_t(z) * g.ls[1] + y) * g.ls[0] + x]
+                        = isoS[((lz + 1) * kApron + (ly + 1)) * kApron + (lx + 1)];
+            }
+        }
+    }
+
+    void launch_merge(const MergeParams& p, cudaStream_t s)
+    {
+        dim3 grid(p.g.nb[0], p.g.nb[1], p.g.nb[2]);
+        k_merge<<<grid, 256, 0, s>>>(p);
+    }
+
+    // ---------------------------------------------------------------- per-source bricks
+    template<int DT>
+    __device__ __forceinline__ void store_elem(void* base, size_t i, float v)
+    {
+        if(DT == 0)
+            reinterpret_cast<float*>(base)[i] = v;
+        else if(DT == 1)
+            reinterpret_cast<__nv_bfloat16*>(base)[i] = __float2bfloat16_rn(v);
+        else
+            reinterpret_cast<__half*>(base)[i] = __float2half_rn(v);
+    }
+
+    template<int DT>
+    __global__ void __launch_bounds__(256) k_source_bricks(const __grid_constant__ SourceBrickParams p)
+    {
+        __shared__ float valS[4][kApron * kApron * kApron];
+        const Geom& g = p.g;
+        const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
+        for(int t = threadIdx.x; t < kApron * kApron * kApron; t += blockDim.x)
+        {
+            const int lx = t % kApron, ly = (t / kApron) % kApron, lz = t / (kApron * kApron);
+            const int x = iclamp(bx * 8 - 1 + lx, 0, g.ls[0] - 1);
+            const int y = iclamp(by * 8 - 1 + ly, 0, g.ls[1] - 1);
+            const int z = iclamp(bz * 8 - 1 + lz, 0, g.ls[2] - 1);
+            const size_t idx = (size_t(z) * g.ls[1] + y) * g.ls[0] + x;
+            float v[4];
+            const float* sp = p.src + idx * p.fdim;
+            v[0] = __ldg(sp);
+            v[1] = p.fdim > 1 ? __ldg(sp + 1) : 0.0f;
+            v[2] = p.fdim > 2 ? __ldg(sp + 2) : 0.0f;
+            v[3] = p.fdim > 3 ? __ldg(sp + 3) : 0.0f;
+            if(p.applyChain)
+            {
+                valS[0][t] = apply_chain(v, p.fdim, p.chain);
+            }
+            else
+            {
+#pragma unroll
+                for(int c = 0; c < 4; ++c)
+                    if(c < p.ncomp)
+                        valS[c][t] = v[c];
+            }
+        }
+        __syncthreads();
+        const size_t brick = (size_t(bz) * g.nb[1] + by) * g.nb[0] + bx;
+        const int per = 4 * p.ncomp;
+        for(int s = threadIdx.x; s < kSlotsPerBrick; s += blockDim.x)
+        {
+            const int lx = s & 7, ly = (s >> 3) & 7, lz = s >> 6;
+            const int t = (lz * kApron + ly) * kApron + lx;
+            const size_t base = (brick * kSlotsPerBrick + s) * per;
+            for(int c = 0; c < p.ncomp; ++c)
+            {
+                store_elem<DT>(p.out, base + 4 * c + 0, valS[c][t]);
+                store_elem<DT>(p.out, base + 4 * c + 1, valS[c][t + 1]);
+                store_elem<DT>(p.out, base + 4 * c + 2, valS[c][t + kApron]);
+                store_elem<DT>(p.out, base + 4 * c + 3, valS[c][t + kApron + 1]);
+            }
+        }
+    }
+
+    void launch_source_bricks(const SourceBrickParams& p, cudaStream_t s)
+    {
+        dim3 grid(p.g.nb[0], p.g.nb[1], p.g.nb[2]);
+        if(p.dtype == 1)
+            k_source_bricks<1><<<grid, 256, 0, s>>>(p);
+        else if(p.dtype == 2)
+            k_source_bricks<2><<<grid, 256, 0, s>>>(p);
+        else
+            k_source_bricks<0><<<grid, 256, 0, s>>>(p);
+    }
+
+    // ---------------------------------------------------------------- diagnostics
+    __global__ void k_unbrick(Geom g, const uint4* __restrict__ q, uint32_t* __restrict__ out)
+    {
+        const size_t n = size_t(g.ls[0]) * g.ls[1] * g.ls[2];
+        for(size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        {
+            const int x = int(i % g.ls[0]);
+            const int y = int((i / g.ls[0]) % g.ls[1]);
+            const int z = int(i / (size_t(g.ls[0]) * g.ls[1]));
+            out[i] = reinterpret_cast<const uint32_t*>(q)[brick_slot(g, x, y, z) * 4];
+        }
+    }
+
+    void launch_unbrick(const Geom& g, const uint4* volQ, uint32_t* out, cudaStream_t s)
+    {
+        k_unbrick<<<148 * 8, 256, 0, s>>>(g, volQ, out);
+    }
+} // namespace isaacb

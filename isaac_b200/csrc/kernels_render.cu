@@ -1,0 +1,337 @@
+// Frame kernels of the combined (pre-classified) renderer: drawCallBack
+// (lib/isaac.hpp:2140-2543).
+//
+//   k_clear_particles  ClearBufferKernel + ParticleRenderKernel
+//                      (lib/isaac/isaac_common_kernel.hpp:195-217,
+//                       lib/isaac/isaac_particle_kernel.hpp:32-260)
+//   k_iso              CombinedIsoRenderKernel (lib/isaac/isaac_iso_kernel.hpp:25-128)
+//   k_ssao             SSAOKernel (+ optional SSAOFilterKernel)
+//                      (lib/isaac/isaac_ssao_kernel.hpp:38-230)
+//   k_shade_volume     ShadingKernel + CombinedVolumeRenderKernel
+//                      (lib/isaac/isaac_common_kernel.hpp:220-320,
+//                       lib/isaac/isaac_volume_kernel.hpp:23-88)
+//
+// The reference launches these six passes with a blocking wait after each;
+// here the per-pixel passes that need no neighbour are fused, so a frame is
+// two launches (four with iso surfaces and SSAO).
+#include "isaacb_frame.cuh"
+
+#include <cfloat>
+
+namespace isaacb
+{
+    // ------------------------------------------------------------------ particles
+    __device__ void particle_pixel(const FrameParams& p, int px, int py)
+    {
+        bool any = false;
+        for(int s = 0; s < p.nPart; ++s)
+            any |= p.part[s].weight != 0.0f;
+        if(!any)
+            return;
+        Ray ray = pixel_to_ray(p.v, p.g, px, py);
+        if(!clip_ray(ray, p.v, p.g))
+            return;
+        const size_t o = pix(p, px, py);
+        ray.endDepth = gmin(ray.endDepth, p.depth[o]);
+        const float3 ps = p.pscale;
+        float4 pColor = make_float4(0, 0, 0, 0);
+        float depth = FLT_MAX;
+        bool hit = false;
+        int ds[3];
+        ds[0] = int(gsign(ray.dir.x));
+        ds[1] = int(gsign(ray.dir.y));
+        ds[2] = int(gsign(ray.dir.z));
+        const float3 cur = add3(ray.start, muls3(ray.dir, ray.startDepth));
+        uint32_t cell[3];
+        cell[0] = uint32_t(iclamp(f2i(cur.x / ps.x), 0, p.g.lps[0] - 1));
+        cell[1] = uint32_t(iclamp(f2i(cur.y / ps.y), 0, p.g.lps[1] - 1));
+        cell[2] = uint32_t(iclamp(f2i(cur.z / ps.z), 0, p.g.lps[2] - 1));
+        const float rayLength = ray.endDepth - ray.startDepth;
+        float tested = 0.0f;
+        float t[3], dT[3];
+        const float dr[3] = {ray.dir.x, ray.dir.y, ray.dir.z};
+        const float pc[3] = {ps.x, ps.y, ps.z};
+        const float cu[3] = {cur.x, cur.y, cur.z};
+#pragma unroll
+        for(int i = 0; i < 3; ++i)
+        {
+            t[i] = ((float(cell[i]) + float(max(ds[i], 0))) * pc[i] - cu[i]) / dr[i];
+            dT[i] = pc[i] / dr[i] * float(ds[i]);
+            if(dr[i] == 0.0f)
+                t[i] = FLT_MAX;
+        }
+        float3 pNormal = f3(0, 0, 0);
+        while(cell[0] < uint32_t(p.g.lps[0]) && cell[1] < uint32_t(p.g.lps[1]) && cell[2] < uint32_t(p.g.lps[2])
+              && !hit && tested <= rayLength)
+        {
+            const size_t ci = (size_t(cell[2]) * p.g.lps[1] + cell[1]) * p.g.lps[0] + cell[0];
+            const float3 cellf = f3(float(cell[0]), float(cell[1]), float(cell[2]));
+            for(int s = 0; s < p.nPart; ++s)
+            {
+                const ParticleSrc& P = p.part[s];
+                if(P.weight == 0.0f)
+                    continue;
+                const uint32_t k1 = __ldg(P.offsets + ci + 1);
+                for(uint32_t k = __ldg(P.offsets + ci); k < k1; ++k)
+                {
+                    const float3 pp
+                        = f3(__ldg(P.pos + 3 * size_t(k)), __ldg(P.pos + 3 * size_t(k) + 1), __ldg(P.pos + 3 * size_t(k) + 2));
+                    const float3 ppos = mul3(add3(pp, cellf), ps);
+                    const float3 L = sub3(ppos, cur);
+                    const float radius = (P.radius ? __ldg(P.radius + k) : P.constRadius) * P.weight;
+                    const float r2 = radius * radius;
+                    const float tca = dot3(L, ray.dir);
+                    const float d2 = dot3(L, L) - tca * tca;
+                    if(d2 <= r2)
+                    {
+                        const float thc = sqrtf(r2 - d2);
+                        const float t0 = tca - thc;
+                        const float t1 = tca + thc;
+                        if(t1 >= 0.0f && t0 < depth)
+                        {
+                            float a[4];
+                            const float* ap = P.attr + size_t(k) * P.fdim;
+                            a[0] = __ldg(ap);
+                            a[1] = P.fdim > 1 ? __ldg(ap + 1) : 0.0f;
+                            a[2] = P.fdim > 2 ? __ldg(ap + 2) : 0.0f;
+                            a[3] = P.fdim > 3 ? __ldg(ap + 3) : 0.0f;
+                            const float res = apply_chain(a, P.fdim, P.chain);
+                            const float4 value = __ldg(p.lut + P.lutBase + lut_index(res, p.ts));
+                            if(value.w >= 0.5f)
+                            {
+                                pColor = value;
+                                depth = t0;
+                                hit = true;
+                                pNormal = sub3(add3(cur, smul3(t0, ray.dir)), ppos);
+                                if(t0 < 0.0f && ray.isClipped)
+                                    pNormal = neg3(ray.clippingNormal);
+                            }
+                        }
+                    }
+                }
+            }
+            if(t[0] < t[1] && t[0] < t[2])
+            {
+                cell[0] += uint32_t(ds[0]);
+                tested = t[0];
+                t[0] += dT[0];
+            }
+            else if(t[1] < t[0] && t[1] < t[2])
+            {
+                cell[1] += uint32_t(ds[1]);
+                tested = t[1];
+                t[1] += dT[1];
+            }
+            else
+            {
+                cell[2] += uint32_t(ds[2]);
+                tested = t[2];
+                t[2] += dT[2];
+            }
+        }
+        if(!hit)
+            return;
+        pNormal = normalize3(pNormal);
+        pColor.w = 1.0f;
+        p.color[o] = to_byte4(pColor);
+        p.normal[3 * o] = pNormal.x;
+        p.normal[3 * o + 1] = pNormal.y;
+        p.normal[3 * o + 2] = pNormal.z;
+        p.depth[o] = depth + ray.startDepth;
+    }
+
+    __global__ void __launch_bounds__(256) k_clear_particles(const __grid_constant__ FrameParams p)
+    {
+        int px, py;
+        thread_pixel(px, py);
+        if(px >= p.v.W || py >= p.v.H)
+            return;
+        const size_t o = pix(p, px, py);
+        p.color[o] = to_byte4(p.bgSwizzled);
+        p.normal[3 * o] = 0.0f;
+        p.normal[3 * o + 1] = 0.0f;
+        p.normal[3 * o + 2] = 0.0f;
+        p.depth[o] = FLT_MAX;
+        p.ao[o] = 0.0f;
+        if(p.nPart > 0)
+            particle_pixel(p, px, py);
+    }
+
+    void launch_clear_particles(const FrameParams& p, cudaStream_t s)
+    {
+        dim3 grid((p.v.W + 31) / 32, (p.v.H + 7) / 8);
+        k_clear_particles<<<grid, 256, 0, s>>>(p);
+    }
+
+    // ------------------------------------------------------------------ iso
+    __global__ void __launch_bounds__(256) k_iso(const __grid_constant__ FrameParams p)
+    {
+        int px, py;
+        thread_pixel(px, py);
+        unsigned long long n = 0;
+        const bool linear = p.interpolation != 0;
+        if(px < p.v.W && py < p.v.H)
+        {
+            Ray ray = pixel_to_ray(p.v, p.g, px, py);
+            const size_t o = pix(p, px, py);
+            if(clip_ray(ray, p.v, p.g))
+            {
+                ray.endDepth = gmin(ray.endDepth, p.depth[o]);
+                if(!(ray.endDepth <= ray.startDepth))
+                {
+                    const March m = march_setup(ray, p.g, p.v.scale, p.step);
+                    bool hit = false;
+                    float depth = ray.endDepth;
+                    float4 hitColor = make_float4(0, 0, 0, 0);
+                    float3 hitNormal = f3(0, 0, 0);
+                    float oldValue = 0.0f;
+                    for(int i = m.startSteps; i <= m.endSteps && !hit; i++)
+                    {
+                        ++n;
+                        const float3 pos = march_pos(m, i);
+                        const bool first = ray.isClipped && i == m.startSteps;
+                        const float t = float(i) * m.stepU;
+                        const float value = sample_alpha(p.isoAQ, p.g, pos, linear);
+                        const float tmp = oldValue;
+                        oldValue = value;
+                        if(value < 0.5f)
+                            continue;
+                        if(first)
+                            depth = ray.startDepth;
+                        else
+                            depth = t + m.stepU * (0.5f - tmp) / (value - tmp);
+                        hit = true;
+                        const float3 np = add3(ray.start, muls3(ray.dir, depth));
+                        const float3 pu = div3(np, p.v.scale);
+                        hitColor = sample_linear_rgba8(p.isoLin, p.g, pu, linear);
+                        hitColor.w = 1.0f;
+                        float3 gr;
+                        gr.x = sample_linear_rgba8(p.isoLin, p.g, add3(pu, f3(1, 0, 0)), linear).w
+                            - sample_linear_rgba8(p.isoLin, p.g, sub3(pu, f3(1, 0, 0)), linear).w;
+                        gr.y = sample_linear_rgba8(p.isoLin, p.g, add3(pu, f3(0, 1, 0)), linear).w
+                            - sample_linear_rgba8(p.isoLin, p.g, sub3(pu, f3(0, 1, 0)), linear).w;
+                        gr.z = sample_linear_rgba8(p.isoLin, p.g, add3(pu, f3(0, 0, 1)), linear).w
+                            - sample_linear_rgba8(p.isoLin, p.g, sub3(pu, f3(0, 0, 1)), linear).w;
+                        float gl = length3(gr);
+                        if(first || gl == 0.0f)
+                        {
+                            gr = ray.clippingNormal;
+                            gl = 1.0f;
+                        }
+                        hitNormal = divs3(neg3(gr), gl);
+                    }
+                    if(hit)
+                    {
+                        p.color[o] = to_byte4(hitColor);
+                        p.normal[3 * o] = hitNormal.x;
+                        p.normal[3 * o + 1] = hitNormal.y;
+                        p.normal[3 * o + 2] = hitNormal.z;
+                        p.depth[o] = depth;
+                    }
+                }
+            }
+        }
+        if(p.counters)
+            count_samples(p.counters + 1, n);
+    }
+
+    void launch_iso(const FrameParams& p, cudaStream_t s)
+    {
+        dim3 grid((p.v.W + 31) / 32, (p.v.H + 7) / 8);
+        k_iso<<<grid, 256, 0, s>>>(p);
+    }
+
+    // ------------------------------------------------------------------ SSAO
+    __global__ void __launch_bounds__(256) k_ssao(const __grid_constant__ FrameParams p)
+    {
+        int px, py;
+        thread_pixel(px, py);
+        if(px >= p.v.W || py >= p.v.H)
+            return;
+        const size_t o = pix(p, px, py);
+        const float ref = p.depth[o];
+        float occ = 0.0f;
+        for(int i = -3; i <= 3; ++i)
+        {
+            const int x = iclamp(px + i * 10, 0, p.v.W - 1);
+            for(int j = -3; j <= 3; ++j)
+            {
+                const int y = iclamp(py + j * 10, 0, p.v.H - 1);
+                if(__ldg(p.depth + pix(p, x, y)) < ref)
+                    occ += 1.0f;
+            }
+        }
+        const float ao = gclamp(occ / 42.0f, 0.0f, 1.0f);
+        p.ao[o] = ao;
+        if(p.aoFilter)
+        {
+            const float4 c = from_byte4(p.color[o]);
+            const float w = p.aoWeight;
+            const float f = (1.0f - w) + w * (1.0f - ao);
+            p.color[o] = to_byte4(make_float4(f * c.x, f * c.y, f * c.z, c.w));
+        }
+    }
+
+    void launch_ssao(const FrameParams& p, cudaStream_t s)
+    {
+        dim3 grid((p.v.W + 31) / 32, (p.v.H + 7) / 8);
+        k_ssao<<<grid, 256, 0, s>>>(p);
+    }
+
+    template<bool VOLUME>
+    __global__ void __launch_bounds__(256) k_shade_volume(const __grid_constant__ FrameParams p)
+    {
+        int px, py;
+        thread_pixel(px, py);
+        unsigned long long n = 0;
+        if(px < p.v.W && py < p.v.H)
+        {
+            const size_t o = pix(p, px, py);
+            shade_pixel(p, px, py, o);
+            if(VOLUME)
+            {
+                Ray ray = pixel_to_ray(p.v, p.g, px, py);
+                if(clip_ray(ray, p.v, p.g))
+                {
+                    ray.endDepth = gmin(ray.endDepth, p.depth[o]);
+                    if(!(ray.endDepth <= ray.startDepth))
+                    {
+                        March m = march_setup(ray, p.g, p.v.scale, p.step);
+                        const float factor = m.factor * p.totalWeightAll;
+                        const bool linear = p.interpolation != 0;
+                        float4 color = make_float4(0, 0, 0, 0);
+                        for(int i = m.startSteps; i <= m.endSteps; i++)
+                        {
+                            ++n;
+                            const float3 pos = march_pos(m, i);
+                            float4 value = sample_rgba8(p.volQ, p.g, pos, linear);
+                            value = make_float4(value.x * factor, value.y * factor, value.z * factor, value.w * factor);
+                            const float w = 1.0f - color.w;
+                            color.x += w * value.x;
+                            color.y += w * value.y;
+                            color.z += w * value.z;
+                            color.w += w * value.w;
+                            if(color.w > 0.99f)
+                                break;
+                        }
+                        const float4 solid = from_byte4(p.color[o]);
+                        const float r = 1.0f - color.w;
+                        color = make_float4(color.x + r * solid.x, color.y + r * solid.y, color.z + r * solid.z, color.w + r * solid.w);
+                        p.color[o] = to_byte4(color);
+                    }
+                }
+            }
+        }
+        if(VOLUME && p.counters)
+            count_samples(p.counters, n);
+    }
+
+    void launch_shade_volume(const FrameParams& p, bool volume, cudaStream_t s)
+    {
+        dim3 grid((p.v.W + 31) / 32, (p.v.H + 7) / 8);
+        if(volume)
+            k_shade_volume<true><<<grid, 256, 0, s>>>(p);
+        else
+            k_shade_volume<false><<<grid, 256, 0, s>>>(p);
+    }
+} // namespace isaacb

@@ -1,0 +1,500 @@
+"""Host-side mirror of ISAAC's ``IsaacVisualization`` for the rendering hot path.
+
+The reference class (``lib/isaac.hpp:58-3036``) is a C++ template over source
+lists.  This Python class keeps its roles and names -- source objects with
+``featureDim``/``persistent``/``getName()``/``update()``, functor-chain strings,
+per-source transfer functions, weights, iso thresholds, clipping planes, the
+camera (projection, look-at, rotation, distance), ambient occlusion, render and
+dither modes -- and drives the sm_100a kernels through the C ABI
+(``include/isaac_b200.h``).  Steering messages use the reference's JSON keys
+(``lib/isaac.hpp:1345-1803``).  The IceT compositing, MPI and the streaming
+server are not part of this path.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+Z_NEAR = 0.002  # ISAAC_Z_NEAR, lib/isaac/isaac_defines.hpp:53
+Z_FAR = 100.0  # ISAAC_Z_FAR, lib/isaac/isaac_defines.hpp:54
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def perspective(fovy: float, aspect: float, znear: float, zfar: float) -> np.ndarray:
+    """glm::perspective (right handed, clip depth -1..1), column major 4x4 double."""
+    t = math.tan(fovy / 2.0)
+    m = np.zeros((4, 4), dtype=np.float64)  # m[col][row]
+    m[0][0] = 1.0 / (aspect * t)
+    m[1][1] = 1.0 / t
+    m[2][2] = -(zfar + znear) / (zfar - znear)
+    m[2][3] = -1.0
+    m[3][2] = -(2.0 * zfar * znear) / (zfar - znear)
+    return m
+
+
+def modelview(look_at=(0.0, 0.0, 0.0), rotation=None, distance=-4.5) -> np.ndarray:
+    """updateModelview (lib/isaac.hpp:2878-2889): distanceM * rotationM * translationM."""
+    rot = np.eye(3) if rotation is None else np.asarray(rotation, dtype=np.float64)
+    T = np.eye(4)
+    T[3, 0:3] = look_at  # column-major: translation in column 3
+    R = np.eye(4)
+    R[0:3, 0:3] = rot  # rot given column major [col][row]
+    D = np.eye(4)
+    D[3][2] = distance
+    # column-major product A*B == (B^T A^T)^T with row-major numpy; keep [col][row] storage
+    return _cm_mul(_cm_mul(D, R), T)
+
+
+def _cm_mul(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Product of two column-major [col][row] matrices, returned column-major."""
+    return (a.T @ b.T).T
+
+
+class DefaultController:
+    """isaac_controllers.hpp:23-43: perspective(45.0, w/h, Z_NEAR, Z_FAR), with 45.0 in radians as glm reads it."""
+
+    passCount = 1
+
+    @staticmethod
+    def updateProjection(framebuffer_size) -> np.ndarray:
+        w, h = framebuffer_size
+        return perspective(45.0, float(w) / float(h), Z_NEAR, Z_FAR)
+
+
+class VolumeSource:
+    """A volume source over device memory: ``data`` is a CUDA tensor of shape
+    (Z, Y, X, featureDim) or (Z, Y, X), float32, x fastest -- what the reference
+    reads through ``operator[]`` (example/example.cpp:36-143)."""
+
+    guardSize = 0
+
+    def __init__(self, name: str, data, feature_dim: int | None = None, persistent: bool = True):
+        self._name = name
+        self.data = data
+        self.featureDim = int(feature_dim if feature_dim is not None else (data.shape[-1] if data.dim() == 4 else 1))
+        self.persistent = bool(persistent)
+
+    def getName(self) -> str:
+        return self._name
+
+    def update(self, enabled: bool, pointer=None) -> None:
+        """Called before every buffer update, as the reference calls ``source.update``."""
+
+
+class ParticleSource:
+    """A particle source as a cell list (``getIterator`` of example/example.cpp:148-228):
+    ``offsets`` (ncells+1, uint32 as int32/int64 tensor), ``positions`` (N,3)
+    cell-relative in [0,1), ``attributes`` (N,featureDim), ``radii`` (N) or a constant."""
+
+    def __init__(self, name: str, offsets, positions, attributes, radii=None, radius: float = 0.5):
+        self._name = name
+        self.offsets = offsets
+        self.positions = positions
+        self.attributes = attributes
+        self.radii = radii
+        self.radius = float(radius)
+        self.featureDim = int(attributes.shape[1]) if attributes.dim() == 2 else 1
+
+    def getName(self) -> str:
+        return self._name
+
+    def update(self, enabled: bool, pointer=None) -> None:
+        pass
+
+
+def _fa(vals) -> C.Array:
+    vals = list(vals)
+    return (C.c_float * len(vals))(*vals)
+
+
+class IsaacVisualization:
+    """drop-in host object for the rendering path; see the module docstring."""
+
+    def __init__(
+        self,
+        name: str,
+        framebuffer_size: Sequence[int],
+        global_size: Sequence[int],
+        local_size: Sequence[int],
+        local_particle_size: Sequence[int],
+        position: Sequence[int],
+        volume_sources: Sequence[VolumeSource],
+        particle_sources: Sequence[ParticleSource] = (),
+        scale: Sequence[float] = (1.0, 1.0, 1.0),
+        transfer_size: int = 1024,
+        controller=DefaultController,
+    ):
+        self.lib = _lib.load()
+        self.name = name
+        self.framebufferSize = tuple(int(v) for v in framebuffer_size)
+        self.volumeSources = list(volume_sources)
+        self.particleSources = list(particle_sources)
+        self.scale = tuple(float(v) for v in scale)
+        self.transferSize = int(transfer_size)
+        n_vol, n_part = len(self.volumeSources), len(self.particleSources)
+        d = _lib.Desc()
+        d.framebuffer[:] = self.framebufferSize
+        d.global_size[:] = [int(v) for v in global_size]
+        d.local_size[:] = [int(v) for v in local_size]
+        d.local_particle_size[:] = [int(v) for v in local_particle_size]
+        d.position[:] = [int(v) for v in position]
+        d.scale[:] = self.scale
+        d.transfer_size = self.transferSize
+        d.n_volume_sources = n_vol
+        d.n_particle_sources = n_part
+        for i, s in enumerate(self.volumeSources + self.particleSources):
+            d.feature_dim[i] = s.featureDim
+            d.persistent[i] = int(getattr(s, "persistent", True))
+            d.guard_size[i] = int(getattr(s, "guardSize", 0))
+        self.desc = d
+        ctx = C.c_void_p()
+        check(self.lib.isaacb_create(C.byref(d), C.byref(ctx)), None)
+        self.ctx = ctx
+        self.combinedSourceListSize = n_vol + n_part
+        n = self.combinedSourceListSize
+        # steering state with the reference defaults (lib/isaac.hpp:565-945)
+        self.functions = ["idem"] * n
+        self.functionErrors = [0] * n
+        self.sourceWeight = [2.0] * n
+        self.sourceIsoThreshold = [0.0] * n
+        self.transferDescription: list[dict[int, tuple]] = [dict() for _ in range(n)]
+        self.step = 0.5
+        self.interpolation = False
+        self.renderOptimization = True
+        self.ambientOcclusion = {"isEnabled": False, "weight": 0.5}
+        self.renderMode = 0
+        self.ditherMode = 1
+        self.backgroundColor = [0.0, 0.0, 0.0, 0.0]
+        self.clipping: list[tuple] = []
+        self.controller = controller
+        self.projection = controller.updateProjection(self.framebufferSize)
+        self.lookAt = (0.0, 0.0, 0.0)
+        self.rotation = np.eye(3)
+        self.distance = -4.5
+        self.modelview = modelview(self.lookAt, self.rotation, self.distance)
+        self.kernelTime = 0.0
+        self.mergeTime = 0.0
+        self.copyTime = 0.0
+        self._frame = None
+        for i, s in enumerate(self.volumeSources):
+            check(self.lib.isaacb_set_source(ctx, i, C.c_void_p(s.data.data_ptr())), ctx)
+        for j, p in enumerate(self.particleSources):
+            self._set_particles(n_vol + j, p)
+        self._push_camera()
+
+    # ------------------------------------------------------------------ lifecycle
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.isaacb_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _set_particles(self, idx: int, p: ParticleSource):
+        radii = C.c_void_p(p.radii.data_ptr()) if p.radii is not None else None
+        check(
+            self.lib.isaacb_set_particles(
+                self.ctx,
+                idx,
+                C.c_void_p(p.offsets.data_ptr()),
+                C.c_void_p(p.positions.data_ptr()),
+                C.c_void_p(p.attributes.data_ptr()),
+                radii,
+                p.radius,
+            ),
+            self.ctx,
+        )
+
+    # ------------------------------------------------------------------ steering (reference setters)
+    def updateFunctions(self) -> list[int]:
+        """Parse ``self.functions`` (lib/isaac.hpp:1079-1241); returns the error codes."""
+        codes = []
+        for i, f in enumerate(self.functions):
+            err = C.c_int32(0)
+            st = self.lib.isaacb_set_functions(self.ctx, i, f.encode(), C.byref(err))
+            if st not in (_lib.OK, _lib.PARSE_ERROR):
+                check(st, self.ctx)
+            codes.append(int(err.value))
+        self.functionErrors = codes
+        return codes
+
+    def setTransferPoints(self, src: int, points: dict[int, Sequence[float]]):
+        """Replace the control points of one source ("transfer points", lib/isaac.hpp:1591-1612)."""
+        self.transferDescription[src] = {int(k): tuple(float(x) for x in v) for k, v in points.items()}
+        self.updateTransfer(src)
+
+    def updateTransfer(self, src: int | None = None):
+        """Rebuild transfer tables from the control points (lib/isaac.hpp:1244-1266)."""
+        srcs = range(self.combinedSourceListSize) if src is None else [src]
+        for i in srcs:
+            desc = self.transferDescription[i]
+            if not desc:
+                continue
+            keys = (C.c_uint32 * len(desc))(*desc.keys())
+            rgba = _fa([c for v in desc.values() for c in v])
+            check(self.lib.isaacb_set_transfer(self.ctx, i, len(desc), keys, rgba), self.ctx)
+
+    def getTransfer(self, src: int) -> np.ndarray:
+        out = np.zeros((self.transferSize, 4), dtype=np.float32)
+        check(self.lib.isaacb_get_transfer(self.ctx, src, out.ctypes.data_as(_lib._fp)), self.ctx)
+        return out
+
+    def setWeight(self, src: int, w: float):
+        self.sourceWeight[src] = float(w)
+        check(self.lib.isaacb_set_weight(self.ctx, src, float(w)), self.ctx)
+
+    def setIsoThreshold(self, src: int, v: float):
+        self.sourceIsoThreshold[src] = float(v)
+        check(self.lib.isaacb_set_iso_threshold(self.ctx, src, float(v)), self.ctx)
+
+    def setStep(self, step: float):
+        self.step = max(float(step), 0.01)
+        check(self.lib.isaacb_set_step(self.ctx, self.step), self.ctx)
+
+    def setInterpolation(self, on: bool):
+        self.interpolation = bool(on)
+        check(self.lib.isaacb_set_interpolation(self.ctx, int(on)), self.ctx)
+
+    def setRenderOptimization(self, on: bool):
+        self.renderOptimization = bool(on)
+        r = _lib.RENDERER_COMBINED if on else _lib.RENDERER_PER_SOURCE
+        check(self.lib.isaacb_set_renderer(self.ctx, r), self.ctx)
+
+    def setStorage(self, src: int, dtype: int):
+        check(self.lib.isaacb_set_storage(self.ctx, src, int(dtype)), self.ctx)
+
+    def setAmbientOcclusion(self, enabled: bool, weight: float = 0.5, filter: bool = False):
+        self.ambientOcclusion = {"isEnabled": bool(enabled), "weight": float(weight)}
+        check(self.lib.isaacb_set_ao(self.ctx, int(enabled), float(weight), int(filter)), self.ctx)
+
+    def setRenderMode(self, mode: int):
+        self.renderMode = int(mode)
+        check(self.lib.isaacb_set_render_mode(self.ctx, int(mode)), self.ctx)
+
+    def setDitherMode(self, mode: int):
+        self.ditherMode = int(mode)
+        check(self.lib.isaacb_set_dither_mode(self.ctx, int(mode)), self.ctx)
+
+    def setBackgroundColor(self, rgba: Sequence[float]):
+        self.backgroundColor = [float(v) for v in rgba]
+        check(self.lib.isaacb_set_background(self.ctx, _fa(self.backgroundColor)), self.ctx)
+
+    def editClipping(self, nr: int, px, py, pz, nx, ny, nz) -> bool:
+        st = self.lib.isaacb_edit_clipping(self.ctx, int(nr), _fa([px, py, pz]), _fa([nx, ny, nz]))
+        if st == _lib.OK and nr < len(self.clipping):
+            self.clipping[nr] = (px, py, pz, nx, ny, nz)
+        return st == _lib.OK
+
+    def addClipping(self, px, py, pz, nx, ny, nz) -> bool:
+        st = self.lib.isaacb_add_clipping(self.ctx, _fa([px, py, pz]), _fa([nx, ny, nz]))
+        if st == _lib.OK:
+            self.clipping.append((px, py, pz, nx, ny, nz))
+        return st == _lib.OK
+
+    def removeClipping(self, nr: int):
+        if 0 <= nr < len(self.clipping):
+            check(self.lib.isaacb_remove_clipping(self.ctx, int(nr)), self.ctx)
+            del self.clipping[nr]
+
+    # ------------------------------------------------------------------ camera
+    def setCamera(self, projection: np.ndarray, modelview_m: np.ndarray):
+        """Explicit projection and modelview, column-major [col][row] doubles."""
+        self.projection = np.asarray(projection, dtype=np.float64)
+        self.modelview = np.asarray(modelview_m, dtype=np.float64)
+        self._push_camera()
+
+    def updateModelview(self):
+        self.modelview = modelview(self.lookAt, self.rotation, self.distance)
+        self._push_camera()
+
+    def _push_camera(self):
+        p = np.ascontiguousarray(self.projection, dtype=np.float64).reshape(16)
+        m = np.ascontiguousarray(self.modelview, dtype=np.float64).reshape(16)
+        check(
+            self.lib.isaacb_set_camera(self.ctx, p.ctypes.data_as(_lib._dp), m.ctypes.data_as(_lib._dp)),
+            self.ctx,
+        )
+
+    # ------------------------------------------------------------------ JSON steering (reference keys)
+    def steer(self, message: dict):
+        """Apply a steering message with the reference's keys (lib/isaac.hpp:1560-1795)."""
+        if "projection" in message:
+            self.projection = np.asarray(message["projection"], dtype=np.float64).reshape(4, 4)
+            self._push_camera()
+        if "modelview" in message:
+            self.modelview = np.asarray(message["modelview"], dtype=np.float64).reshape(4, 4)
+            self._push_camera()
+        if "look at" in message:
+            self.lookAt = tuple(message["look at"])
+            self.updateModelview()
+        if "rotation" in message:
+            self.rotation = np.asarray(message["rotation"], dtype=np.float64).reshape(3, 3)
+            self.updateModelview()
+        if "distance" in message:
+            self.distance = float(message["distance"])
+            self.updateModelview()
+        if "transfer points" in message:
+            for i, pts in enumerate(message["transfer points"]):
+                self.setTransferPoints(i, {int(p["value"]): (p["r"], p["g"], p["b"], p["a"]) for p in pts})
+        if "interpolation" in message:
+            self.setInterpolation(bool(message["interpolation"]))
+        if "render optimization" in message:
+            self.setRenderOptimization(bool(message["render optimization"]))
+        if "step" in message:
+            self.setStep(float(message["step"]))
+        if "iso threshold" in message:
+            for i, v in enumerate(message["iso threshold"]):
+                self.setIsoThreshold(i, v)
+        if "functions" in message:
+            for i, f in enumerate(message["functions"]):
+                self.functions[i] = str(f)
+            self.updateFunctions()
+        if "weight" in message:
+            for i, v in enumerate(message["weight"]):
+                self.setWeight(i, v)
+        if "background color" in message and len(message["background color"]) == 3:
+            self.setBackgroundColor(list(message["background color"]) + [self.backgroundColor[3]])
+        if "clipping add" in message:
+            c = message["clipping add"]
+            self.addClipping(*c["position"], *c["normal"])
+        if "clipping remove" in message:
+            self.removeClipping(int(message["clipping remove"]))
+        if "clipping edit" in message:
+            c = message["clipping edit"]
+            self.editClipping(int(c["nr"]), *c["position"], *c["normal"])
+        if "ao" in message:
+            a = message["ao"]
+            self.setAmbientOcclusion(bool(a.get("isEnabled", False)), float(a.get("weight", 0.5)))
+        if "render mode" in message:
+            self.setRenderMode(int(message["render mode"]["mode"]))
+        if "dither mode" in message:
+            self.setDitherMode(int(message["dither mode"]["mode"]))
+
+    # ------------------------------------------------------------------ per frame
+    def _stream(self):
+        return C.c_void_p(_torch().cuda.current_stream().cuda_stream)
+
+    def doVisualization(self, pointer=None, redraw: bool = True, host: bool = True, out=None, timing: bool = False):
+        """One frame: the sources' ``update`` hooks, buffer update, draw and readback
+        (lib/isaac.hpp:1298-2104 with drawCallBack).
+
+        With ``host`` the frame comes back as an (H, W, 4) uint8 numpy array
+        (row 0 = bottom) through one synchronous ``isaacb_frame`` call; else it
+        is written to a (H, W, 4) uint8 CUDA tensor and the call stays
+        asynchronous.  ``timing`` records ``mergeTime`` / ``kernelTime`` (ms)
+        with CUDA events, like the reference's per-phase counters.
+        """
+        for i, s in enumerate(self.volumeSources):
+            s.update(self.sourceWeight[i] != 0 or self.sourceIsoThreshold[i] != 0, pointer)
+        for j, p in enumerate(self.particleSources):
+            p.update(self.sourceWeight[len(self.volumeSources) + j] != 0, pointer)
+        if not redraw:
+            return self._frame
+        w, h = self.framebufferSize
+        st = self._stream()
+        if host and not timing:
+            if out is None:
+                out = np.empty((h, w, 4), dtype=np.uint8)
+            check(self.lib.isaacb_frame(self.ctx, st, C.c_void_p(out.ctypes.data)), self.ctx)
+            self._frame = out
+            return out
+        torch = _torch()
+        dev = torch.empty((h, w, 4), dtype=torch.uint8, device="cuda") if (host or out is None) else out
+        if timing:
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record()
+        check(self.lib.isaacb_update(self.ctx, st), self.ctx)
+        if timing:
+            e1.record()
+        check(self.lib.isaacb_render(self.ctx, st, C.c_void_p(dev.data_ptr())), self.ctx)
+        if timing:
+            e2.record()
+            e2.synchronize()
+            self.mergeTime = e0.elapsed_time(e1)
+            self.kernelTime = e1.elapsed_time(e2)
+        result = dev.cpu().numpy() if host else dev
+        self._frame = result
+        return result
+
+    def update(self):
+        """Buffer update only (merge / per-source bricks), asynchronous."""
+        check(self.lib.isaacb_update(self.ctx, self._stream()), self.ctx)
+
+    def render(self, out=None):
+        """Draw only, asynchronous; optionally copies the frame into the CUDA tensor ``out``."""
+        ptr = C.c_void_p(out.data_ptr()) if out is not None else None
+        check(self.lib.isaacb_render(self.ctx, self._stream(), ptr), self.ctx)
+
+    def minMax(self) -> tuple[np.ndarray, np.ndarray]:
+        """"minmax" request (lib/isaac.hpp:1951-2006): per-source min and max after the functor chain."""
+        n = self.combinedSourceListSize
+        mn = np.zeros(n, dtype=np.float32)
+        mx = np.zeros(n, dtype=np.float32)
+        check(self.lib.isaacb_minmax(self.ctx, self._stream(), mn.ctypes.data_as(_lib._fp), mx.ctypes.data_as(_lib._fp)), self.ctx)
+        return mn, mx
+
+    # ------------------------------------------------------------------ diagnostics
+    def gbuffer(self):
+        w, h = self.framebufferSize
+        depth = np.zeros((h, w), dtype=np.float32)
+        normal = np.zeros((h, w, 3), dtype=np.float32)
+        ao = np.zeros((h, w), dtype=np.float32)
+        check(
+            self.lib.isaacb_get_gbuffer(
+                self.ctx, self._stream(), C.c_void_p(depth.ctypes.data), C.c_void_p(normal.ctypes.data), C.c_void_p(ao.ctypes.data)
+            ),
+            self.ctx,
+        )
+        return depth, normal, ao
+
+    def combinedTextures(self):
+        lx, ly, lz = (int(v) for v in self.desc.local_size)
+        vol = np.zeros((lz, ly, lx, 4), dtype=np.uint8)
+        iso = np.zeros((lz, ly, lx, 4), dtype=np.uint8)
+        check(
+            self.lib.isaacb_get_combined(self.ctx, self._stream(), C.c_void_p(vol.ctypes.data), C.c_void_p(iso.ctypes.data)),
+            self.ctx,
+        )
+        return vol, iso
+
+    def setCounting(self, on: bool):
+        check(self.lib.isaacb_set_counting(self.ctx, int(on)), self.ctx)
+
+    def setTiming(self, on: bool):
+        check(self.lib.isaacb_set_timing(self.ctx, int(on)), self.ctx)
+
+    def timings(self) -> dict:
+        """Milliseconds per phase of the last update + render (CUDA events on the launch stream)."""
+        ms = (C.c_float * _lib.TIMING_SLOTS)()
+        check(self.lib.isaacb_get_timing(self.ctx, self._stream(), ms), self.ctx)
+        return dict(zip(_lib.TIMING_NAMES, [float(v) for v in ms]))
+
+    def launchCounts(self) -> tuple[int, int]:
+        u = C.c_uint32(0)
+        r = C.c_uint32(0)
+        check(self.lib.isaacb_get_launch_count(self.ctx, C.byref(u), C.byref(r)), self.ctx)
+        return int(u.value), int(r.value)
+
+    def counters(self) -> tuple[int, int]:
+        v = C.c_uint64(0)
+        i = C.c_uint64(0)
+        check(self.lib.isaacb_get_counters(self.ctx, self._stream(), C.byref(v), C.byref(i)), self.ctx)
+        return int(v.value), int(i.value)
+
+
