@@ -208,6 +208,27 @@ isaacb_status isaacb_get_counters(isaacb_ctx* ctx, void* stream, uint64_t* volum
 isaacb_status isaacb_set_timing(isaacb_ctx* ctx, int32_t enabled);
 isaacb_status isaacb_get_timing(isaacb_ctx* ctx, void* stream, float ms[ISAACB_TIMING_SLOTS]);
 
+/* Min/max of one volume source after a functor chain, allocating nothing.
+ * No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc -- e.g. a simulation that reserves nearly all device memory for
+ * its own heap, or a loop that must not take cudaMalloc's implicit device
+ * synchronisation.  It needs no context.  `src` is the source (size[0]*size[1]*size[2]
+ * voxels, x fastest, feature_dim floats each), bytecode/params come from
+ * isaacb_parse_chain, `result` is 2 device floats (min, max), bit-identical to
+ * isaacb_minmax.  Scratch is one static device array of 2 MiB per GPU: sources
+ * with more than 262144 (x,y) columns are rejected (INVALID_ARG); the first call
+ * on a device resolves the array's address and should precede any stream
+ * capture; calls that overlap on the GPU race on the shared array.
+ * Asynchronous on `stream`; errors via isaacb_last_error(NULL). */
+isaacb_status isaacb_minmax_noalloc(
+    const float* src,
+    const uint32_t size[3],
+    uint32_t feature_dim,
+    const int32_t bytecode[ISAACB_MAX_FUNCTORS],
+    const float params[4 * ISAACB_MAX_FUNCTORS],
+    float* result,
+    void* stream);
+
 /* Number of kernels the last isaacb_update / isaacb_render enqueued. */
 isaacb_status isaacb_get_launch_count(isaacb_ctx* ctx, uint32_t* update_launches, uint32_t* render_launches);
 

@@ -105,6 +105,7 @@ SIGNATURES = {
     "isaacb_get_launch_count": (_i32, [_P, _u32p, _u32p]),
     "isaacb_set_timing": (_i32, [_P, _i32]),
     "isaacb_get_timing": (_i32, [_P, _P, _fp]),
+    "isaacb_minmax_noalloc": (_i32, [_P, _u32p, _u32, _i32p, _fp, _P, _P]),
 }
 
 

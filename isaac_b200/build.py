@@ -34,7 +34,14 @@ NVCC_FLAGS = [
     "-I",
     str(ROOT / "include"),
 ]
-SOURCES = ["api.cu", "kernels_merge.cu", "kernels_minmax.cu", "kernels_render.cu", "kernels_legacy.cu"]
+SOURCES = [
+    "api.cu",
+    "kernels_merge.cu",
+    "kernels_minmax.cu",
+    "kernels_render.cu",
+    "kernels_legacy.cu",
+    "minmax_static.cu",
+]
 
 
 def nvcc() -> str:

@@ -20,8 +20,21 @@ using namespace isaacb;
 
 namespace
 {
-    const char* kFunctorNames[6] = {"idem", "add", "mul", "length", "pow", "sum"};
     thread_local std::string g_createError;
+}
+
+namespace isaacb
+{
+    // error slot of calls that have no context (isaacb_last_error(NULL))
+    void set_global_error(const std::string& msg)
+    {
+        g_createError = msg;
+    }
+} // namespace isaacb
+
+namespace
+{
+    const char* kFunctorNames[6] = {"idem", "add", "mul", "length", "pow", "sum"};
 
     // Per-source body of IsaacVisualization::updateFunctions (lib/isaac.hpp:1084-1186).
     int parse_chain(const std::string& text, int32_t* bytecode, float* params)
