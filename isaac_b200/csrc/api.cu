@@ -5,6 +5,8 @@
 #include "../../include/isaac_b200.h"
 #include "isaacb_internal.h"
 
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cctype>
 #include <climits>
@@ -291,6 +293,10 @@ struct isaacb_ctx
     float* mmPartial = nullptr;
     float* mmResult = nullptr;
     unsigned long long* mmKeys = nullptr;
+    int32_t* errorFlag = nullptr;
+    // TMA tensor maps of the sources, re-encoded when a pointer changes
+    CUtensorMap tmap[kMaxSources]{};
+    const float* tmapPtr[kMaxSources]{};
     uint32_t updateLaunches = 0, renderLaunches = 0;
     bool timing = false;
     cudaEvent_t ev[2 * ISAACB_TIMING_SLOTS]{};
@@ -372,6 +378,26 @@ namespace
         return ISAACB_OK;
     }
 
+    PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+    {
+        static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+        static bool tried = false;
+        if(!tried)
+        {
+            tried = true;
+            void* f = nullptr;
+            cudaDriverEntryPointQueryResult q{};
+            if(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess
+               && q == cudaDriverEntryPointSuccess)
+                fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+        }
+        return fn;
+    }
+
+    // 3-D tensor map over a source seen as (X*featureDim, Y, Z) floats with box
+    // (16*featureDim, 9, 9): the region a merge brick needs, x start on a 16-byte boundary
+    bool encode_source_map(isaacb_ctx* c, int s);
+
     size_t brick_count(const Geom& g)
     {
         return size_t(g.nb[0]) * g.nb[1] * g.nb[2];
@@ -426,6 +452,44 @@ namespace
             if(c->iso[s] > 0.0f)
                 return true;
         return false;
+    }
+} // namespace
+
+namespace
+{
+    bool encode_source_map(isaacb_ctx* c, int s)
+    {
+        auto enc = tensor_map_encoder();
+        const float* src = c->src[s];
+        if(!enc || !src)
+            return false;
+        const uint64_t fd = c->desc.feature_dim[s];
+        const uint64_t X = uint64_t(c->g.ls[0]), Y = uint64_t(c->g.ls[1]), Z = uint64_t(c->g.ls[2]);
+        if((reinterpret_cast<uintptr_t>(src) & 15u) != 0 || ((X * fd) & 3u) != 0)
+            return false;
+        if(c->tmapPtr[s] == src)
+            return true;
+        cuuint64_t dims[3] = {X * fd, Y, Z};
+        cuuint64_t strides[2] = {X * fd * 4, X * Y * fd * 4};
+        cuuint32_t box[3] = {cuuint32_t(16 * fd), 9, 9};
+        cuuint32_t estr[3] = {1, 1, 1};
+        const CUresult r = enc(
+            &c->tmap[s],
+            CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+            3,
+            const_cast<float*>(src),
+            dims,
+            strides,
+            box,
+            estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if(r != CUDA_SUCCESS)
+            return false;
+        c->tmapPtr[s] = src;
+        return true;
     }
 } // namespace
 
@@ -494,6 +558,11 @@ extern "C"
             g.nb[i] = bricks_per_axis(g.ls[i]);
         }
         g.maxGss = std::max(g.gss[0], std::max(g.gss[1], g.gss[2]));
+        if(uint64_t(g.nb[0]) * g.nb[1] * g.nb[2] * kSlotsPerBrick >= (uint64_t(1) << 31))
+        {
+            delete c;
+            return fail(nullptr, ISAACB_INVALID_ARG, "isaacb_create: local volume too large for one context (>~1400^3)");
+        }
         // reference defaults (lib/isaac.hpp:720-793)
         c->lutHost.assign(size_t(c->nTotal) * c->ts * 4, 0.0f);
         for(int s = 0; s < c->nTotal; ++s)
@@ -537,6 +606,9 @@ extern "C"
         alloc((void**) &c->mmPartial, 2 * 148 * 8 * sizeof(float));
         alloc((void**) &c->mmResult, 2 * sizeof(float));
         alloc((void**) &c->mmKeys, 2 * sizeof(unsigned long long));
+        alloc((void**) &c->errorFlag, sizeof(int32_t));
+        if(e == cudaSuccess)
+            e = cudaMemset(c->errorFlag, 0, sizeof(int32_t));
         if(e == cudaSuccess)
             e = cudaMemset(c->isoLin, 0, size_t(g.ls[0]) * g.ls[1] * g.ls[2] * sizeof(uint32_t));
         if(e == cudaSuccess)
@@ -578,6 +650,7 @@ extern "C"
         cudaFree(c->mmPartial);
         cudaFree(c->mmResult);
         cudaFree(c->mmKeys);
+        cudaFree(c->errorFlag);
         for(auto& e : c->ev)
             if(e)
                 cudaEventDestroy(e);
@@ -807,11 +880,42 @@ extern "C"
                 p.iso[s] = c->iso[s];
                 p.totalWeight += c->weight[s];
             }
+            {
+                int e2 = 0;
+                const float m = std::frexp(p.totalWeight, &e2);
+                // an exact power of two whose reciprocal is a normal float
+                p.invTotalWeight = (m == 0.5f && e2 > -120 && e2 < 120) ? std::ldexp(1.0f, 1 - e2) : 0.0f;
+            }
             p.volQ = c->volQ;
             p.isoAQ = c->isoAQ;
             p.isoLin = c->isoLin;
             p.volFlag = c->volFlag;
             p.isoFlag = c->isoFlag;
+            p.errorFlag = c->errorFlag;
+            // stage sources with TMA when every active one is 16-byte aligned with
+            // rows of a multiple of 16 bytes and the tiles fit in shared memory
+            p.useTma = 1;
+            int bytes = 0, tx = 0;
+            for(int s = 0; s < c->nVol; ++s)
+            {
+                p.tileOffset[s] = -1;
+                if(!(c->weight[s] + c->iso[s] > 0.0f))
+                    continue;
+                if(!encode_source_map(c, s))
+                {
+                    p.useTma = 0;
+                    break;
+                }
+                p.tmap[s] = c->tmap[s];
+                p.tileOffset[s] = bytes;
+                const int tile = 16 * int(c->desc.feature_dim[s]) * kApron * kApron * 4;
+                bytes += (tile + 127) & ~127;
+                tx += tile;
+            }
+            p.tileBytes = bytes;
+            p.txBytes = tx;
+            if(bytes == 0 || bytes > 160 * 1024)
+                p.useTma = 0;
             {
                 for(int k = 0; k < ISAACB_TIMING_SLOTS; ++k)
                     c->evUsed[k] = false;
@@ -1007,7 +1111,14 @@ extern "C"
         cudaStream_t st = (cudaStream_t) stream;
         const size_t bytes = size_t(c->desc.framebuffer[0]) * c->desc.framebuffer[1] * 4;
         ISAACB_CUDA(c, cudaMemcpyAsync(rgba_host, c->color, bytes, cudaMemcpyDeviceToHost, st), "frame readback");
+        int32_t flag = 0;
+        ISAACB_CUDA(c, cudaMemcpyAsync(&flag, c->errorFlag, sizeof(flag), cudaMemcpyDeviceToHost, st), "error flag");
         ISAACB_CUDA(c, cudaStreamSynchronize(st), "isaacb_frame");
+        if(flag)
+        {
+            cudaMemsetAsync(c->errorFlag, 0, sizeof(int32_t), st);
+            return fail(c, ISAACB_TIMEOUT, "isaacb_frame: a bounded device wait gave up; the frame is incomplete");
+        }
         return ISAACB_OK;
     }
 

@@ -534,6 +534,50 @@ namespace isaacb
         return make_float4(byte_f(w, 0) / 255.0f, byte_f(w, 1) / 255.0f, byte_f(w, 2) / 255.0f, byte_f(w, 3) / 255.0f);
     }
 
+    // ------------------------------------------------------------- fast paths (FMA / ALU pipes only)
+    // The ray-march is issue-bound; these helpers keep its per-sample work off the
+    // XU pipe (conversions, rounding, reciprocal), which the exact forms above use.
+
+    // byte c of w as a float, exactly: the bit pattern 0x4B0000bb is 2^23 + b
+    __device__ __forceinline__ float ubyte_f(uint32_t w, int c)
+    {
+        return __int_as_float(int(__byte_perm(w, 0x4B000000u, 0x7440u + unsigned(c)))) - 8388608.0f;
+    }
+
+    // floor(x) as float and int for |x| < 2^22: adding 1.5*2^23 rounded toward -inf leaves
+    // floor(x) in the low mantissa bits (exact)
+    __device__ __forceinline__ void floor_split(float x, float& fl, int& ix)
+    {
+        const float t = __fadd_rd(x, 12582912.0f);
+        fl = t - 12582912.0f;
+        ix = __float_as_int(t) - 0x4B400000;
+    }
+
+    // trunc(x) as int for 0 <= x < 2^22 (exact): adding 2^23 rounded toward zero
+    __device__ __forceinline__ int trunc_nonneg(float x, float& tr)
+    {
+        const float t = __fadd_rz(x, 8388608.0f);
+        tr = t - 8388608.0f;
+        return __float_as_int(t) - 0x4B000000;
+    }
+
+    // round half away from zero of x in [0, 2^22) (roundf for non-negative x), exact
+    __device__ __forceinline__ int round_nonneg(float x)
+    {
+        float tr;
+        const int t = trunc_nonneg(x, tr);
+        return t + ((x - tr) >= 0.5f ? 1 : 0);
+    }
+
+    // lut_index with the same result for every input, NaN included, without the
+    // conversion pipe: clamp first (NaN -> 0), then round half away from zero
+    __device__ __forceinline__ int lut_index_fast(float v, int ts)
+    {
+        const float x = v * float(ts);
+        const float xc = fminf(fmaxf(x, 0.0f), float(ts));
+        return min(round_nonneg(xc), ts - 1);
+    }
+
     // pixel of a thread: a block of 256 threads covers 32x8 pixels and each warp an 8x4 tile
     __device__ __forceinline__ void thread_pixel(int& px, int& py)
     {

@@ -5,6 +5,7 @@
 #include "isaacb_device.cuh"
 
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace isaacb
@@ -24,11 +25,20 @@ namespace isaacb
         float weight[kMaxSources];
         float iso[kMaxSources];
         float totalWeight;
+        float invTotalWeight; // 2^-k when totalWeight == 2^k exactly, else 0
         uint4* volQ; // combined volume, quad bricks
         uint32_t* isoAQ; // combined iso alpha, quad bricks
         uint32_t* isoLin; // combined iso RGBA8, linear
         uint8_t* volFlag; // per brick: 1 if any texel (apron included) is non-zero
         uint8_t* isoFlag; // per brick: max alpha byte (apron included)
+        int32_t* errorFlag; // set when a bounded wait gives up
+        // TMA staging: one 3-D tensor map per source over (X*featureDim, Y, Z) floats,
+        // box (16*featureDim, 9, 9); useTma = 0 selects plain loads
+        int32_t useTma;
+        int32_t tileOffset[kMaxSources]; // byte offset of each source tile in dynamic smem (-1 = not loaded)
+        int32_t tileBytes; // dynamic smem bytes of all tiles (each padded to 128 bytes)
+        int32_t txBytes; // bytes the TMA boxes deliver (the mbarrier's transaction count)
+        alignas(64) CUtensorMap tmap[kMaxSources];
     };
     void launch_merge(const MergeParams& p, cudaStream_t s);
 

@@ -25,7 +25,14 @@ namespace isaacb
            31, 0,  54, 21, 58, 24, 17, 5,  28, 38, 56, 41, 11, 63, 14, 47, 37, 48, 42, 62, 12, 18,
            3,  35, 50, 44, 19, 1,  20, 34, 29, 25, 57, 4,  22, 8,  33, 53, 30, 55, 27, 7};
 
-    // applyDither3D (lib/isaac/isaac_dither_kernel.hpp:7-329), modes 0, 1, 2
+    // applyDither3D (lib/isaac/isaac_dither_kernel.hpp:7-329), modes 0, 1, 2, bit-exact,
+    // with truncation, floor and rounding done by exact magic-number adds on the FMA pipe
+    __device__ __forceinline__ uint32_t round_byte(float v)
+    {
+        // round(clamp(v,0,1)*255); clamp maps NaN to 0 as the GPU conversion does
+        return uint32_t(round_nonneg(fminf(fmaxf(v, 0.0f), 1.0f) * 255.0f));
+    }
+
     __device__ __forceinline__ uint32_t dither_rgba(int mode, int x, int y, int z, float4 c)
     {
         float v[4] = {c.x, c.y, c.z, c.w};
@@ -35,19 +42,28 @@ namespace isaacb
 #pragma unroll
             for(int i = 0; i < 4; ++i)
             {
-                int b = f2i(roundf(gclamp(v[i], 0.0f, 1.0f) * 255.0f));
-                out |= uint32_t(min(max(b, 0), 255)) << (8 * i);
+                // gclamp keeps the reference's NaN path (NaN -> byte 0)
+                const float cl = gclamp(v[i], 0.0f, 1.0f);
+                out |= (cl == cl ? uint32_t(round_nonneg(cl * 255.0f)) : 0u) << (8 * i);
             }
             return out;
         }
         const uint8_t* mask = (mode == 2) ? c_dither2 : c_dither1;
-        float d = float(mask[x % 4 + (y % 4) * 4 + (z % 4) * 16]) / 64.0f;
+        const float d = float(mask[x % 4 + (y % 4) * 4 + (z % 4) * 16]) / 64.0f;
 #pragma unroll
         for(int i = 0; i < 4; ++i)
         {
-            float s = v[i] * 255.0f;
-            int ci = f2i(s);
-            ci += (gfract(s) > d) ? 1 : 0;
+            // int(s) + (fract(s) > d), clamped to [0,255]; s is clamped to [-2,257] first,
+            // which changes no clamped result (NaN -> -2 -> 0, like the conversion's 0)
+            const float s = fminf(fmaxf(v[i] * 255.0f, -2.0f), 257.0f);
+            float tr;
+            int ti = trunc_nonneg(fabsf(s), tr);
+            if(s < 0.0f)
+                ti = -ti;
+            float fl;
+            int fi;
+            floor_split(s, fl, fi);
+            int ci = ti + ((s - fl) > d ? 1 : 0);
             out |= uint32_t(min(max(ci, 0), 255)) << (8 * i);
         }
         return out;
@@ -62,25 +78,53 @@ namespace isaacb
         v[3] = fdim > 3 ? __ldg(p + 3) : 0.0f;
     }
 
-    __global__ void __launch_bounds__(256) k_merge(const __grid_constant__ MergeParams p)
+    // ---------------------------------------------------------------- TMA / mbarrier helpers
+    __device__ __forceinline__ uint32_t smem_u32(const void* p)
     {
-        __shared__ uint32_t volS[kApron * kApron * kApron];
-        __shared__ uint32_t isoS[kApron * kApron * kApron];
-        __shared__ int isoMax;
+        return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+    }
+    __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t phase)
+    {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred P;\n mbarrier.test_wait.parity.shared::cta.b64 P, [%1], %2;\n selp.u32 %0, 1, 0, P;\n}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(phase)
+            : "memory");
+        return done != 0;
+    }
+    // bounded wait: about 0.5 s at most, then false
+    __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t phase)
+    {
+        for(int it = 0; it < (1 << 22); ++it)
+        {
+            if(mbar_test(bar, phase))
+                return true;
+            __nanosleep(100);
+        }
+        return false;
+    }
+
+    // the 9^3 texels of one brick; fetch(s, x, y, z, v) reads a clamped voxel
+    template<class Fetch>
+    __device__ __forceinline__ void merge_brick(
+        const MergeParams& p,
+        int bx,
+        int by,
+        int bz,
+        uint32_t* volS,
+        uint32_t* isoS,
+        int& anyVol,
+        int& myIsoMax,
+        Fetch fetch)
+    {
         const Geom& g = p.g;
-        const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
-        if(threadIdx.x == 0)
-            isoMax = 0;
-        __syncthreads();
-        int anyVol = 0;
-        int myIsoMax = 0;
         for(int t = threadIdx.x; t < kApron * kApron * kApron; t += blockDim.x)
         {
             const int lx = t % kApron, ly = (t / kApron) % kApron, lz = t / (kApron * kApron);
             const int x = iclamp(bx * 8 - 1 + lx, 0, g.ls[0] - 1);
             const int y = iclamp(by * 8 - 1 + ly, 0, g.ls[1] - 1);
             const int z = iclamp(bz * 8 - 1 + lz, 0, g.ls[2] - 1);
-            const size_t idx = (size_t(z) * g.ls[1] + y) * g.ls[0] + x;
             float4 vc = make_float4(0, 0, 0, 0), ic = make_float4(0, 0, 0, 0);
             for(int s = 0; s < p.nVol; ++s)
             {
@@ -89,9 +133,9 @@ namespace isaacb
                 if(!(vw + it > 0.0f))
                     continue;
                 float v[4];
-                read_voxel(p.src[s], p.fdim[s], idx, v);
+                fetch(s, x, y, z, v);
                 const float val = apply_chain(v, p.fdim[s], p.chain[s]);
-                const float4 c = __ldg(p.lut + size_t(s) * p.ts + lut_index(val, p.ts));
+                const float4 c = __ldg(p.lut + size_t(s) * p.ts + lut_index_fast(val, p.ts));
                 if(vw > 0.0f)
                 {
                     float a = c.w * vw;
@@ -107,23 +151,102 @@ namespace isaacb
                         ic = make_float4(c.x, c.y, c.z, a);
                 }
             }
-            vc = make_float4(vc.x / p.totalWeight, vc.y / p.totalWeight, vc.z / p.totalWeight, vc.w / p.totalWeight);
+            if(p.invTotalWeight != 0.0f)
+            {
+                // totalWeight is a power of two: x * 2^-k is the correctly rounded x / 2^k
+                vc = make_float4(vc.x * p.invTotalWeight, vc.y * p.invTotalWeight, vc.z * p.invTotalWeight, vc.w * p.invTotalWeight);
+            }
+            else
+            {
+                vc = make_float4(vc.x / p.totalWeight, vc.y / p.totalWeight, vc.z / p.totalWeight, vc.w / p.totalWeight);
+            }
             const uint32_t vb = dither_rgba(p.ditherMode, x, y, z, vc);
             volS[t] = vb;
             anyVol |= vb != 0u;
             if(p.writeIso)
             {
-                float iv[4] = {ic.x, ic.y, ic.z, ic.w};
-                uint32_t ib = 0;
-#pragma unroll
-                for(int i = 0; i < 4; ++i)
-                {
-                    int b = f2i(roundf(gclamp(iv[i], 0.0f, 1.0f) * 255.0f));
-                    ib |= uint32_t(min(max(b, 0), 255)) << (8 * i);
-                }
+                const uint32_t ib = round_byte(ic.x) | (round_byte(ic.y) << 8) | (round_byte(ic.z) << 16)
+                    | (round_byte(ic.w) << 24);
                 isoS[t] = ib;
                 myIsoMax = max(myIsoMax, int(ib >> 24));
             }
+        }
+    }
+
+    // One CTA per brick.  With TMA, thread 0 stages each active source's region
+    // [8b-4, 8b+12) x [8b-1, 8b+8) x [8b-1, 8b+8) (the x start rounded down to a
+    // 16-byte boundary; out-of-volume elements are never read) into shared memory
+    // with one cp.async.bulk.tensor per source, completing on an mbarrier.
+    template<bool TMA>
+    __global__ void __launch_bounds__(256) k_merge(const __grid_constant__ MergeParams p)
+    {
+        extern __shared__ __align__(128) unsigned char dsm[];
+        __shared__ uint32_t volS[kApron * kApron * kApron];
+        __shared__ uint32_t isoS[kApron * kApron * kApron];
+        __shared__ int isoMax;
+        __shared__ __align__(8) unsigned long long mbar;
+        const Geom& g = p.g;
+        const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
+        const int x0 = bx * 8 - 4, y0 = by * 8 - 1, z0 = bz * 8 - 1;
+        const uint32_t bar = smem_u32(&mbar);
+        // tiles start on a 128-byte boundary of the dynamic shared memory (128 spare bytes requested)
+        unsigned char* tiles = dsm + ((128u - (smem_u32(dsm) & 127u)) & 127u);
+        if(threadIdx.x == 0)
+        {
+            isoMax = 0;
+            if(TMA)
+            {
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1) : "memory");
+                asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            }
+        }
+        __syncthreads();
+        if(TMA)
+        {
+            if(threadIdx.x == 0)
+            {
+                asm volatile(
+                    "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(p.txBytes) : "memory");
+                for(int s = 0; s < p.nVol; ++s)
+                {
+                    if(p.tileOffset[s] < 0)
+                        continue;
+                    const uint32_t dst = smem_u32(tiles + p.tileOffset[s]);
+                    const uint64_t map = reinterpret_cast<uint64_t>(&p.tmap[s]);
+                    asm volatile(
+                        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+                        :
+                        : "r"(dst), "l"(map), "r"(x0 * p.fdim[s]), "r"(y0), "r"(z0), "r"(bar)
+                        : "memory");
+                }
+            }
+            if(!mbar_wait_bounded(bar, 0))
+            {
+                atomicOr(p.errorFlag, 1);
+                // let the copies land before the block's shared memory is released
+                mbar_wait_bounded(bar, 0);
+                return;
+            }
+        }
+        int anyVol = 0;
+        int myIsoMax = 0;
+        if(TMA)
+        {
+            merge_brick(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, [&](int s, int x, int y, int z, float(&v)[4]) {
+                const int fd = p.fdim[s];
+                const float* tile = reinterpret_cast<const float*>(tiles + p.tileOffset[s]);
+                const float* q = tile + ((z - z0) * kApron + (y - y0)) * (16 * fd) + (x - x0) * fd;
+                v[0] = q[0];
+                v[1] = fd > 1 ? q[1] : 0.0f;
+                v[2] = fd > 2 ? q[2] : 0.0f;
+                v[3] = fd > 3 ? q[3] : 0.0f;
+            });
+        }
+        else
+        {
+            merge_brick(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, [&](int s, int x, int y, int z, float(&v)[4]) {
+                read_voxel(p.src[s], p.fdim[s], (size_t(z) * g.ls[1] + y) * g.ls[0] + x, v);
+            });
         }
         if(p.writeIso)
             atomicMax(&isoMax, myIsoMax);
@@ -165,7 +288,15 @@ namespace isaacb
     void launch_merge(const MergeParams& p, cudaStream_t s)
     {
         dim3 grid(p.g.nb[0], p.g.nb[1], p.g.nb[2]);
-        k_merge<<<grid, 256, 0, s>>>(p);
+        if(p.useTma)
+        {
+            cudaFuncSetAttribute(k_merge<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, p.tileBytes + 128);
+            k_merge<true><<<grid, 256, p.tileBytes + 128, s>>>(p);
+        }
+        else
+        {
+            k_merge<false><<<grid, 256, 0, s>>>(p);
+        }
     }
 
     // ---------------------------------------------------------------- per-source bricks
