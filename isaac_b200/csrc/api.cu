@@ -294,6 +294,12 @@ struct isaacb_ctx
     float* mmResult = nullptr;
     unsigned long long* mmKeys = nullptr;
     int32_t* errorFlag = nullptr;
+    // count of all-zero bricks of the last merge, copied back asynchronously; the
+    // march checks brick emptiness only when the previous count was not zero
+    unsigned int* emptyDev = nullptr;
+    unsigned int* emptyPinned = nullptr;
+    cudaEvent_t emptyEvent = nullptr;
+    long long lastEmpty = -1;
     // TMA tensor maps of the sources, re-encoded when a pointer changes
     CUtensorMap tmap[kMaxSources]{};
     const float* tmapPtr[kMaxSources]{};
@@ -607,6 +613,11 @@ extern "C"
         alloc((void**) &c->mmResult, 2 * sizeof(float));
         alloc((void**) &c->mmKeys, 2 * sizeof(unsigned long long));
         alloc((void**) &c->errorFlag, sizeof(int32_t));
+        alloc((void**) &c->emptyDev, sizeof(unsigned int));
+        if(e == cudaSuccess)
+            e = cudaMallocHost((void**) &c->emptyPinned, sizeof(unsigned int));
+        if(e == cudaSuccess)
+            e = cudaEventCreateWithFlags(&c->emptyEvent, cudaEventDisableTiming);
         if(e == cudaSuccess)
             e = cudaMemset(c->errorFlag, 0, sizeof(int32_t));
         if(e == cudaSuccess)
@@ -651,6 +662,11 @@ extern "C"
         cudaFree(c->mmResult);
         cudaFree(c->mmKeys);
         cudaFree(c->errorFlag);
+        cudaFree(c->emptyDev);
+        if(c->emptyPinned)
+            cudaFreeHost(c->emptyPinned);
+        if(c->emptyEvent)
+            cudaEventDestroy(c->emptyEvent);
         for(auto& e : c->ev)
             if(e)
                 cudaEventDestroy(e);
@@ -876,6 +892,7 @@ extern "C"
                 p.src[s] = c->src[s];
                 p.fdim[s] = int32_t(c->desc.feature_dim[s]);
                 p.chain[s] = c->chain[s];
+                p.chainIdem[s] = (c->chain[s].op[0] == OP_IDEM && c->chain[s].op[1] == OP_IDEM && c->chain[s].op[2] == OP_IDEM) ? 1 : 0;
                 p.weight[s] = c->weight[s];
                 p.iso[s] = c->iso[s];
                 p.totalWeight += c->weight[s];
@@ -892,6 +909,8 @@ extern "C"
             p.volFlag = c->volFlag;
             p.isoFlag = c->isoFlag;
             p.errorFlag = c->errorFlag;
+            p.emptyBricks = c->emptyDev;
+            ISAACB_CUDA(c, cudaMemsetAsync(c->emptyDev, 0, sizeof(unsigned int), st), "empty brick counter");
             // stage sources with TMA when every active one is 16-byte aligned with
             // rows of a multiple of 16 bytes and the tiles fit in shared memory
             p.useTma = 1;
@@ -923,6 +942,15 @@ extern "C"
                 launch_merge(p, st);
             }
             c->updateLaunches++;
+            // the count comes back asynchronously; a later render reads it once the event completed
+            if(cudaEventQuery(c->emptyEvent) != cudaErrorNotReady)
+            {
+                ISAACB_CUDA(
+                    c,
+                    cudaMemcpyAsync(c->emptyPinned, c->emptyDev, sizeof(unsigned int), cudaMemcpyDeviceToHost, st),
+                    "empty brick count");
+                ISAACB_CUDA(c, cudaEventRecord(c->emptyEvent, st), "empty brick event");
+            }
             if(!p.writeIso && c->isoWritten)
             {
                 // the reference's iso texture is all zero when no source has an iso threshold
@@ -1006,6 +1034,10 @@ extern "C"
         p.totalWeightAll = 0.0f;
         for(int s = 0; s < c->nTotal; ++s)
             p.totalWeightAll += c->weight[s];
+        if(cudaEventQuery(c->emptyEvent) == cudaSuccess)
+            c->lastEmpty = (long long) *c->emptyPinned;
+        // either choice renders the same image; skipping only pays when bricks are empty
+        p.skipEmpty = c->lastEmpty != 0 ? 1 : 0;
         p.lut = c->lutDev;
         p.volQ = c->volQ;
         p.isoAQ = c->isoAQ;

@@ -578,6 +578,48 @@ namespace isaacb
         return min(round_nonneg(xc), ts - 1);
     }
 
+    // ------------------------------------------------------------- packed FP32 pairs (sm_100a f32x2)
+    // Two FP32 lanes per instruction; each lane rounds exactly like the scalar op.
+    struct f2p
+    {
+        unsigned long long v;
+    };
+    __device__ __forceinline__ f2p f2p_make(float lo, float hi)
+    {
+        f2p r;
+        asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
+        return r;
+    }
+    __device__ __forceinline__ void f2p_split(f2p a, float& lo, float& hi)
+    {
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
+    }
+    __device__ __forceinline__ f2p f2p_fma(f2p a, f2p b, f2p c)
+    {
+        f2p r;
+        asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+        return r;
+    }
+    __device__ __forceinline__ f2p f2p_mul(f2p a, f2p b)
+    {
+        f2p r;
+        asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+        return r;
+    }
+    __device__ __forceinline__ f2p f2p_add(f2p a, f2p b)
+    {
+        f2p r;
+        asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+        return r;
+    }
+    // bytes (c, c+1) of w as an exact float pair: 2^23 + b bit patterns minus 2^23
+    __device__ __forceinline__ f2p ubyte_pair(uint32_t w, int c, f2p bias)
+    {
+        const float lo = __int_as_float(int(__byte_perm(w, 0x4B000000u, 0x7440u + unsigned(c))));
+        const float hi = __int_as_float(int(__byte_perm(w, 0x4B000000u, 0x7440u + unsigned(c + 1))));
+        return f2p_add(f2p_make(lo, hi), bias);
+    }
+
     // pixel of a thread: a block of 256 threads covers 32x8 pixels and each warp an 8x4 tile
     __device__ __forceinline__ void thread_pixel(int& px, int& py)
     {

@@ -21,6 +21,7 @@ namespace isaacb
         const float* src[kMaxSources];
         int32_t fdim[kMaxSources];
         Chain chain[kMaxSources];
+        int32_t chainIdem[kMaxSources]; // 1: every functor is idem, the value is the x component
         const float4* lut; // nTotal * ts, source s at s*ts
         float weight[kMaxSources];
         float iso[kMaxSources];
@@ -32,6 +33,7 @@ namespace isaacb
         uint8_t* volFlag; // per brick: 1 if any texel (apron included) is non-zero
         uint8_t* isoFlag; // per brick: max alpha byte (apron included)
         int32_t* errorFlag; // set when a bounded wait gives up
+        unsigned int* emptyBricks; // count of all-zero bricks (zeroed by the host before the merge)
         // TMA staging: one 3-D tensor map per source over (X*featureDim, Y, Z) floats,
         // box (16*featureDim, 9, 9); useTma = 0 selects plain loads
         int32_t useTma;
@@ -117,6 +119,7 @@ namespace isaacb
         float aoWeight;
         int32_t aoFilter;
         float totalWeightAll;
+        int32_t skipEmpty; // the volume march checks per-brick emptiness
         const float4* lut;
         // combined textures
         const uint4* volQ;

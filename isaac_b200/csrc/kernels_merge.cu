@@ -33,7 +33,8 @@ namespace isaacb
         return uint32_t(round_nonneg(fminf(fmaxf(v, 0.0f), 1.0f) * 255.0f));
     }
 
-    __device__ __forceinline__ uint32_t dither_rgba(int mode, int x, int y, int z, float4 c)
+    // mask: the mode's 64-entry table (shared memory copy), unused for mode 0
+    __device__ __forceinline__ uint32_t dither_rgba(int mode, const uint8_t* mask, int x, int y, int z, float4 c)
     {
         float v[4] = {c.x, c.y, c.z, c.w};
         uint32_t out = 0;
@@ -48,8 +49,7 @@ namespace isaacb
             }
             return out;
         }
-        const uint8_t* mask = (mode == 2) ? c_dither2 : c_dither1;
-        const float d = float(mask[x % 4 + (y % 4) * 4 + (z % 4) * 16]) / 64.0f;
+        const float d = float(mask[(x & 3) + (y & 3) * 4 + (z & 3) * 16]) / 64.0f; // x, y, z >= 0
 #pragma unroll
         for(int i = 0; i < 4; ++i)
         {
@@ -105,7 +105,10 @@ namespace isaacb
         return false;
     }
 
-    // the 9^3 texels of one brick; fetch(s, x, y, z, v) reads a clamped voxel
+    // The 9^3 texels of one brick.  Each thread owns up to three texels (t, t+256,
+    // t+512) and keeps their colour sums in registers while the sources are visited
+    // in the outer loop, so per-source state (chain, table, weights) is uniform and
+    // loaded once.  fetch(s, x, y, z, v) reads a clamped voxel.
     template<class Fetch>
     __device__ __forceinline__ void merge_brick(
         const MergeParams& p,
@@ -116,62 +119,145 @@ namespace isaacb
         uint32_t* isoS,
         int& anyVol,
         int& myIsoMax,
+        const uint8_t* mask,
         Fetch fetch)
     {
+        constexpr int kPer = 3;
+        constexpr int kTex = kApron * kApron * kApron;
         const Geom& g = p.g;
-        for(int t = threadIdx.x; t < kApron * kApron * kApron; t += blockDim.x)
+        int xs[kPer], ys[kPer], zs[kPer];
+        float4 vc[kPer], ic[kPer];
+#pragma unroll
+        for(int j = 0; j < kPer; ++j)
         {
+            const int t = min(int(threadIdx.x) + 256 * j, kTex - 1);
             const int lx = t % kApron, ly = (t / kApron) % kApron, lz = t / (kApron * kApron);
-            const int x = iclamp(bx * 8 - 1 + lx, 0, g.ls[0] - 1);
-            const int y = iclamp(by * 8 - 1 + ly, 0, g.ls[1] - 1);
-            const int z = iclamp(bz * 8 - 1 + lz, 0, g.ls[2] - 1);
-            float4 vc = make_float4(0, 0, 0, 0), ic = make_float4(0, 0, 0, 0);
-            for(int s = 0; s < p.nVol; ++s)
-            {
-                const float vw = p.weight[s];
-                const float it = p.iso[s];
-                if(!(vw + it > 0.0f))
-                    continue;
-                float v[4];
-                fetch(s, x, y, z, v);
-                const float val = apply_chain(v, p.fdim[s], p.chain[s]);
-                const float4 c = __ldg(p.lut + size_t(s) * p.ts + lut_index_fast(val, p.ts));
+            xs[j] = iclamp(bx * 8 - 1 + lx, 0, g.ls[0] - 1);
+            ys[j] = iclamp(by * 8 - 1 + ly, 0, g.ls[1] - 1);
+            zs[j] = iclamp(bz * 8 - 1 + lz, 0, g.ls[2] - 1);
+            vc[j] = make_float4(0, 0, 0, 0);
+            ic[j] = make_float4(0, 0, 0, 0);
+        }
+        const int nMine = int(threadIdx.x) + 512 < kTex ? 3 : 2; // 729 texels over 256 threads
+        for(int s = 0; s < p.nVol; ++s)
+        {
+            const float vw = p.weight[s];
+            const float it = p.iso[s];
+            if(!(vw + it > 0.0f))
+                continue;
+            const float4* lut = p.lut + size_t(s) * p.ts;
+            auto accumulate = [&](int j, float val) {
+                const float4 c = __ldg(lut + lut_index_fast(val, p.ts));
                 if(vw > 0.0f)
                 {
-                    float a = c.w * vw;
-                    vc.x += c.x * a;
-                    vc.y += c.y * a;
-                    vc.z += c.z * a;
-                    vc.w += a;
+                    const float a = c.w * vw;
+                    vc[j].x += c.x * a;
+                    vc[j].y += c.y * a;
+                    vc[j].z += c.z * a;
+                    vc[j].w += a;
                 }
                 if(it > 0.0f)
                 {
-                    float a = c.w / it * 0.5f;
-                    if(ic.w < a)
-                        ic = make_float4(c.x, c.y, c.z, a);
+                    const float a = c.w / it * 0.5f;
+                    if(ic[j].w < a)
+                        ic[j] = make_float4(c.x, c.y, c.z, a);
                 }
-            }
-            if(p.invTotalWeight != 0.0f)
+            };
+            if(p.chainIdem[s] != 0)
             {
-                // totalWeight is a power of two: x * 2^-k is the correctly rounded x / 2^k
-                vc = make_float4(vc.x * p.invTotalWeight, vc.y * p.invTotalWeight, vc.z * p.invTotalWeight, vc.w * p.invTotalWeight);
+                // all functors idem: the value is the first component
+#pragma unroll
+                for(int j = 0; j < kPer; ++j)
+                {
+                    if(j < nMine)
+                        accumulate(j, fetch.first(s, xs[j], ys[j], zs[j]));
+                }
             }
             else
             {
-                vc = make_float4(vc.x / p.totalWeight, vc.y / p.totalWeight, vc.z / p.totalWeight, vc.w / p.totalWeight);
+#pragma unroll
+                for(int j = 0; j < kPer; ++j)
+                {
+                    if(j < nMine)
+                    {
+                        float v[4];
+                        fetch(s, xs[j], ys[j], zs[j], v);
+                        accumulate(j, apply_chain(v, p.fdim[s], p.chain[s]));
+                    }
+                }
             }
-            const uint32_t vb = dither_rgba(p.ditherMode, x, y, z, vc);
+        }
+#pragma unroll
+        for(int j = 0; j < kPer; ++j)
+        {
+            if(j >= nMine)
+                break;
+            const int t = int(threadIdx.x) + 256 * j;
+            float4 c = vc[j];
+            if(p.invTotalWeight != 0.0f)
+            {
+                // totalWeight is a power of two: x * 2^-k is the correctly rounded x / 2^k
+                c = make_float4(c.x * p.invTotalWeight, c.y * p.invTotalWeight, c.z * p.invTotalWeight, c.w * p.invTotalWeight);
+            }
+            else
+            {
+                c = make_float4(c.x / p.totalWeight, c.y / p.totalWeight, c.z / p.totalWeight, c.w / p.totalWeight);
+            }
+            const uint32_t vb = dither_rgba(p.ditherMode, mask, xs[j], ys[j], zs[j], c);
             volS[t] = vb;
             anyVol |= vb != 0u;
             if(p.writeIso)
             {
-                const uint32_t ib = round_byte(ic.x) | (round_byte(ic.y) << 8) | (round_byte(ic.z) << 16)
-                    | (round_byte(ic.w) << 24);
+                const float4 q = ic[j];
+                const uint32_t ib = round_byte(q.x) | (round_byte(q.y) << 8) | (round_byte(q.z) << 16) | (round_byte(q.w) << 24);
                 isoS[t] = ib;
                 myIsoMax = max(myIsoMax, int(ib >> 24));
             }
         }
     }
+
+    // voxel readers of merge_brick: the TMA-staged tile in shared memory, or global memory
+    struct TileFetch
+    {
+        const MergeParams& p;
+        const unsigned char* tiles;
+        int x0, y0, z0;
+        __device__ __forceinline__ const float* at(int s, int x, int y, int z) const
+        {
+            const int fd = p.fdim[s];
+            const float* tile = reinterpret_cast<const float*>(tiles + p.tileOffset[s]);
+            return tile + ((z - z0) * kApron + (y - y0)) * (16 * fd) + (x - x0) * fd;
+        }
+        __device__ __forceinline__ float first(int s, int x, int y, int z) const
+        {
+            return *at(s, x, y, z);
+        }
+        __device__ __forceinline__ void operator()(int s, int x, int y, int z, float (&v)[4]) const
+        {
+            const int fd = p.fdim[s];
+            const float* q = at(s, x, y, z);
+            v[0] = q[0];
+            v[1] = fd > 1 ? q[1] : 0.0f;
+            v[2] = fd > 2 ? q[2] : 0.0f;
+            v[3] = fd > 3 ? q[3] : 0.0f;
+        }
+    };
+    struct GlobalFetch
+    {
+        const MergeParams& p;
+        __device__ __forceinline__ size_t idx(int x, int y, int z) const
+        {
+            return (size_t(z) * p.g.ls[1] + y) * p.g.ls[0] + x;
+        }
+        __device__ __forceinline__ float first(int s, int x, int y, int z) const
+        {
+            return __ldg(p.src[s] + idx(x, y, z) * p.fdim[s]);
+        }
+        __device__ __forceinline__ void operator()(int s, int x, int y, int z, float (&v)[4]) const
+        {
+            read_voxel(p.src[s], p.fdim[s], idx(x, y, z), v);
+        }
+    };
 
     // One CTA per brick.  With TMA, thread 0 stages each active source's region
     // [8b-4, 8b+12) x [8b-1, 8b+8) x [8b-1, 8b+8) (the x start rounded down to a
@@ -185,6 +271,9 @@ namespace isaacb
         __shared__ uint32_t isoS[kApron * kApron * kApron];
         __shared__ int isoMax;
         __shared__ __align__(8) unsigned long long mbar;
+        __shared__ uint8_t sMask[64];
+        if(threadIdx.x < 64)
+            sMask[threadIdx.x] = p.ditherMode == 2 ? c_dither2[threadIdx.x] : c_dither1[threadIdx.x];
         const Geom& g = p.g;
         const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
         const int x0 = bx * 8 - 4, y0 = by * 8 - 1, z0 = bz * 8 - 1;
@@ -232,21 +321,11 @@ namespace isaacb
         int myIsoMax = 0;
         if(TMA)
         {
-            merge_brick(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, [&](int s, int x, int y, int z, float(&v)[4]) {
-                const int fd = p.fdim[s];
-                const float* tile = reinterpret_cast<const float*>(tiles + p.tileOffset[s]);
-                const float* q = tile + ((z - z0) * kApron + (y - y0)) * (16 * fd) + (x - x0) * fd;
-                v[0] = q[0];
-                v[1] = fd > 1 ? q[1] : 0.0f;
-                v[2] = fd > 2 ? q[2] : 0.0f;
-                v[3] = fd > 3 ? q[3] : 0.0f;
-            });
+            merge_brick(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, sMask, TileFetch{p, tiles, x0, y0, z0});
         }
         else
         {
-            merge_brick(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, [&](int s, int x, int y, int z, float(&v)[4]) {
-                read_voxel(p.src[s], p.fdim[s], (size_t(z) * g.ls[1] + y) * g.ls[0] + x, v);
-            });
+            merge_brick(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, sMask, GlobalFetch{p});
         }
         if(p.writeIso)
             atomicMax(&isoMax, myIsoMax);
@@ -255,6 +334,8 @@ namespace isaacb
         if(threadIdx.x == 0)
         {
             p.volFlag[brick] = anyVol ? 1 : 0;
+            if(!anyVol)
+                atomicAdd(p.emptyBricks, 1u);
             if(p.writeIso)
                 p.isoFlag[brick] = uint8_t(isoMax);
         }

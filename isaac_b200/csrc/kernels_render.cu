@@ -164,12 +164,49 @@ namespace isaacb
     }
 
     // ------------------------------------------------------------------ iso
+    // interpolated alpha byte (0..255 scale) of the iso alpha quads at c = pos - 0.5,
+    // FMA/ALU pipes only; brick index and emptiness (max alpha <= 127) returned
+    template<bool LINEAR>
+    __device__ __forceinline__ float iso_alpha_fast(const FrameParams& p, float cx, float cy, float cz, int& brick)
+    {
+        const Geom& g = p.g;
+        const float lo = LINEAR ? -1.0f : 0.0f;
+        cx = fminf(fmaxf(cx, lo), float(g.ls[0] - 1));
+        cy = fminf(fmaxf(cy, lo), float(g.ls[1] - 1));
+        cz = fminf(fmaxf(cz, lo), float(g.ls[2] - 1));
+        const int magic = 0x4B400000 - 1;
+        const float tx = __fadd_rd(cx, 12582912.0f), ty = __fadd_rd(cy, 12582912.0f), tz = __fadd_rd(cz, 12582912.0f);
+        const int ax = __float_as_int(tx) - magic, ay = __float_as_int(ty) - magic, az = __float_as_int(tz) - magic;
+        brick = ((az >> 3) * g.nb[1] + (ay >> 3)) * g.nb[0] + (ax >> 3);
+        const uint32_t slot = uint32_t(brick) * uint32_t(kSlotsPerBrick) + uint32_t((ax & 7) | ((ay & 7) << 3) | ((az & 7) << 6));
+        if(!LINEAR)
+            return ubyte_f(__ldg(p.isoAQ + slot), 0);
+        const uint32_t A = __ldg(p.isoAQ + slot), B = __ldg(p.isoAQ + slot + 64);
+        const float fx = cx - (tx - 12582912.0f), fy = cy - (ty - 12582912.0f), fz = cz - (tz - 12582912.0f);
+        const float gx = 1.0f - fx, gy = 1.0f - fy, gz = 1.0f - fz;
+        const float w00 = gx * gy, w10 = fx * gy, w01 = gx * fy, w11 = fx * fy;
+        float v = ubyte_f(A, 0) * (w00 * gz);
+        v = fmaf(ubyte_f(A, 1), w10 * gz, v);
+        v = fmaf(ubyte_f(A, 2), w01 * gz, v);
+        v = fmaf(ubyte_f(A, 3), w11 * gz, v);
+        v = fmaf(ubyte_f(B, 0), w00 * fz, v);
+        v = fmaf(ubyte_f(B, 1), w10 * fz, v);
+        v = fmaf(ubyte_f(B, 2), w01 * fz, v);
+        v = fmaf(ubyte_f(B, 3), w11 * fz, v);
+        return v;
+    }
+
+    // CombinedIsoRenderKernel (lib/isaac/isaac_iso_kernel.hpp:25-128).  The march
+    // samples alpha with the fast path and skips bricks whose alpha bytes are all
+    // <= 127 (a trilinear value there is below the 0.5 threshold); when a hit
+    // follows skipped samples, the previous sample's value is evaluated for the
+    // depth interpolation.  Hit colour and gradient use the exact sampler.
+    template<bool LINEAR>
     __global__ void __launch_bounds__(256) k_iso(const __grid_constant__ FrameParams p)
     {
         int px, py;
         thread_pixel(px, py);
         unsigned long long n = 0;
-        const bool linear = p.interpolation != 0;
         if(px < p.v.W && py < p.v.H)
         {
             Ray ray = pixel_to_ray(p.v, p.g, px, py);
@@ -180,22 +217,57 @@ namespace isaacb
                 if(!(ray.endDepth <= ray.startDepth))
                 {
                     const March m = march_setup(ray, p.g, p.v.scale, p.step);
+                    const float off = LINEAR ? 0.5f : 0.0f;
+                    const float c0x = m.startU.x - off, c0y = m.startU.y - off, c0z = m.startU.z - off;
+                    const float inv255 = 1.0f / 255.0f;
                     bool hit = false;
                     float depth = ray.endDepth;
                     float4 hitColor = make_float4(0, 0, 0, 0);
                     float3 hitNormal = f3(0, 0, 0);
                     float oldValue = 0.0f;
-                    for(int i = m.startSteps; i <= m.endSteps && !hit; i++)
+                    bool oldKnown = true;
+                    int curBrick = -1;
+                    bool skip = false;
+                    int i = m.startSteps;
+                    for(; i <= m.endSteps; ++i)
                     {
-                        ++n;
-                        const float3 pos = march_pos(m, i);
-                        const bool first = ray.isClipped && i == m.startSteps;
-                        const float t = float(i) * m.stepU;
-                        const float value = sample_alpha(p.isoAQ, p.g, pos, linear);
+                        const float fi = float(i);
+                        const float cx = fmaf(m.stepVec.x, fi, c0x), cy = fmaf(m.stepVec.y, fi, c0y),
+                                    cz = fmaf(m.stepVec.z, fi, c0z);
+                        int brick;
+                        const float a = iso_alpha_fast<LINEAR>(p, cx, cy, cz, brick);
+                        if(brick != curBrick)
+                        {
+                            curBrick = brick;
+                            skip = __ldg(p.isoFlag + brick) <= 127;
+                        }
+                        if(skip)
+                        {
+                            oldKnown = false;
+                            continue;
+                        }
+                        const float value = a * inv255;
+                        if(!oldKnown)
+                        {
+                            int b2;
+                            const float fj = float(i - 1);
+                            oldValue = (i == m.startSteps)
+                                ? 0.0f
+                                : iso_alpha_fast<LINEAR>(
+                                      p,
+                                      fmaf(m.stepVec.x, fj, c0x),
+                                      fmaf(m.stepVec.y, fj, c0y),
+                                      fmaf(m.stepVec.z, fj, c0z),
+                                      b2)
+                                    * inv255;
+                        }
                         const float tmp = oldValue;
                         oldValue = value;
+                        oldKnown = true;
                         if(value < 0.5f)
                             continue;
+                        const bool first = ray.isClipped && i == m.startSteps;
+                        const float t = fi * m.stepU;
                         if(first)
                             depth = ray.startDepth;
                         else
@@ -203,15 +275,15 @@ namespace isaacb
                         hit = true;
                         const float3 np = add3(ray.start, muls3(ray.dir, depth));
                         const float3 pu = div3(np, p.v.scale);
-                        hitColor = sample_linear_rgba8(p.isoLin, p.g, pu, linear);
+                        hitColor = sample_linear_rgba8(p.isoLin, p.g, pu, LINEAR);
                         hitColor.w = 1.0f;
                         float3 gr;
-                        gr.x = sample_linear_rgba8(p.isoLin, p.g, add3(pu, f3(1, 0, 0)), linear).w
-                            - sample_linear_rgba8(p.isoLin, p.g, sub3(pu, f3(1, 0, 0)), linear).w;
-                        gr.y = sample_linear_rgba8(p.isoLin, p.g, add3(pu, f3(0, 1, 0)), linear).w
-                            - sample_linear_rgba8(p.isoLin, p.g, sub3(pu, f3(0, 1, 0)), linear).w;
-                        gr.z = sample_linear_rgba8(p.isoLin, p.g, add3(pu, f3(0, 0, 1)), linear).w
-                            - sample_linear_rgba8(p.isoLin, p.g, sub3(pu, f3(0, 0, 1)), linear).w;
+                        gr.x = sample_linear_rgba8(p.isoLin, p.g, add3(pu, f3(1, 0, 0)), LINEAR).w
+                            - sample_linear_rgba8(p.isoLin, p.g, sub3(pu, f3(1, 0, 0)), LINEAR).w;
+                        gr.y = sample_linear_rgba8(p.isoLin, p.g, add3(pu, f3(0, 1, 0)), LINEAR).w
+                            - sample_linear_rgba8(p.isoLin, p.g, sub3(pu, f3(0, 1, 0)), LINEAR).w;
+                        gr.z = sample_linear_rgba8(p.isoLin, p.g, add3(pu, f3(0, 0, 1)), LINEAR).w
+                            - sample_linear_rgba8(p.isoLin, p.g, sub3(pu, f3(0, 0, 1)), LINEAR).w;
                         float gl = length3(gr);
                         if(first || gl == 0.0f)
                         {
@@ -219,7 +291,10 @@ namespace isaacb
                             gl = 1.0f;
                         }
                         hitNormal = divs3(neg3(gr), gl);
+                        ++i;
+                        break;
                     }
+                    n += (unsigned long long) (i - m.startSteps);
                     if(hit)
                     {
                         p.color[o] = to_byte4(hitColor);
@@ -238,7 +313,10 @@ namespace isaacb
     void launch_iso(const FrameParams& p, cudaStream_t s)
     {
         dim3 grid((p.v.W + 31) / 32, (p.v.H + 7) / 8);
-        k_iso<<<grid, 256, 0, s>>>(p);
+        if(p.interpolation)
+            k_iso<true><<<grid, 256, 0, s>>>(p);
+        else
+            k_iso<false><<<grid, 256, 0, s>>>(p);
     }
 
     // ------------------------------------------------------------------ SSAO
@@ -290,7 +368,7 @@ namespace isaacb
     // CLAMP keeps every coordinate inside the volume; a LINEAR ray whose first and
     // last sample lie strictly inside needs no per-sample clamp (positions are affine
     // in the step index, rounding is far below the 1e-3 margin).
-    template<bool LINEAR, bool CLAMP>
+    template<bool LINEAR, bool CLAMP, bool SKIP>
     __device__ __forceinline__ float4 march_combined(
         const FrameParams& p,
         const March& m,
@@ -326,12 +404,12 @@ namespace isaacb
                         tz = __fadd_rd(cz, 12582912.0f);
             const int ax = __float_as_int(tx) - magic, ay = __float_as_int(ty) - magic, az = __float_as_int(tz) - magic;
             const int brick = ((az >> 3) * nb1 + (ay >> 3)) * nb0 + (ax >> 3);
-            if(brick != curBrick)
+            if(SKIP && brick != curBrick)
             {
                 curBrick = brick;
                 empty = __ldg(p.volFlag + brick) == 0;
             }
-            if(empty)
+            if(SKIP && empty)
             {
                 // last step index whose position stays inside this brick's sample region
                 // [8b-1, 8b+7) per axis, with a 1e-3-step margin against rounding
@@ -362,23 +440,20 @@ namespace isaacb
                 const float fx = cx - (tx - 12582912.0f), fy = cy - (ty - 12582912.0f), fz = cz - (tz - 12582912.0f);
                 const float gx = 1.0f - fx, gy = 1.0f - fy, gz = 1.0f - fz;
                 const float w00 = gx * gy, w10 = fx * gy, w01 = gx * fy, w11 = fx * fy;
-                const float a00 = w00 * gz, a10 = w10 * gz, a01 = w01 * gz, a11 = w11 * gz;
-                const float b00 = w00 * fz, b10 = w10 * fz, b01 = w01 * fz, b11 = w11 * fz;
-                float r[4];
+                const float wt[8] = {w00 * gz, w10 * gz, w01 * gz, w11 * gz, w00 * fz, w10 * fz, w01 * fz, w11 * fz};
+                const uint32_t tap[8] = {A.x, A.y, A.z, A.w, B.x, B.y, B.z, B.w};
+                // (r,g) and (b,a) accumulate as packed FP32 pairs, one FFMA2 each per tap
+                const f2p bias = f2p_make(-8388608.0f, -8388608.0f);
+                f2p rg = f2p_make(0.0f, 0.0f), ba = f2p_make(0.0f, 0.0f);
 #pragma unroll
-                for(int c = 0; c < 4; ++c)
+                for(int k = 0; k < 8; ++k)
                 {
-                    float v = ubyte_f(A.x, c) * a00;
-                    v = fmaf(ubyte_f(A.y, c), a10, v);
-                    v = fmaf(ubyte_f(A.z, c), a01, v);
-                    v = fmaf(ubyte_f(A.w, c), a11, v);
-                    v = fmaf(ubyte_f(B.x, c), b00, v);
-                    v = fmaf(ubyte_f(B.y, c), b10, v);
-                    v = fmaf(ubyte_f(B.z, c), b01, v);
-                    v = fmaf(ubyte_f(B.w, c), b11, v);
-                    r[c] = v;
+                    const f2p wk = f2p_make(wt[k], wt[k]);
+                    rg = f2p_fma(ubyte_pair(tap[k], 0, bias), wk, rg);
+                    ba = f2p_fma(ubyte_pair(tap[k], 2, bias), wk, ba);
                 }
-                r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+                f2p_split(rg, r0, r1);
+                f2p_split(ba, r2, r3);
             }
             else
             {
@@ -414,7 +489,7 @@ namespace isaacb
         return ok;
     }
 
-    template<bool VOLUME, bool LINEAR>
+    template<bool VOLUME, bool LINEAR, bool SKIP>
     __global__ void __launch_bounds__(256) k_shade_volume(const __grid_constant__ FrameParams p)
     {
         int px, py;
@@ -436,9 +511,9 @@ namespace isaacb
                         const float factor = m.factor * p.totalWeightAll;
                         float4 color;
                         if(LINEAR && march_in_range(p.g, m))
-                            color = march_combined<LINEAR, false>(p, m, factor, n);
+                            color = march_combined<LINEAR, false, SKIP>(p, m, factor, n);
                         else
-                            color = march_combined<LINEAR, true>(p, m, factor, n);
+                            color = march_combined<LINEAR, true, SKIP>(p, m, factor, n);
                         const float4 solid = from_byte4(p.color[o]);
                         const float r = 1.0f - color.w;
                         color = make_float4(color.x + r * solid.x, color.y + r * solid.y, color.z + r * solid.z, color.w + r * solid.w);
@@ -455,10 +530,20 @@ namespace isaacb
     {
         dim3 grid((p.v.W + 31) / 32, (p.v.H + 7) / 8);
         if(!volume)
-            k_shade_volume<false, false><<<grid, 256, 0, s>>>(p);
+            k_shade_volume<false, false, false><<<grid, 256, 0, s>>>(p);
         else if(p.interpolation)
-            k_shade_volume<true, true><<<grid, 256, 0, s>>>(p);
+        {
+            if(p.skipEmpty)
+                k_shade_volume<true, true, true><<<grid, 256, 0, s>>>(p);
+            else
+                k_shade_volume<true, true, false><<<grid, 256, 0, s>>>(p);
+        }
         else
-            k_shade_volume<true, false><<<grid, 256, 0, s>>>(p);
+        {
+            if(p.skipEmpty)
+                k_shade_volume<true, false, true><<<grid, 256, 0, s>>>(p);
+            else
+                k_shade_volume<true, false, false><<<grid, 256, 0, s>>>(p);
+        }
     }
 } // namespace isaacb
