@@ -42,6 +42,13 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="isaac_b200", choices=["isaac_b200", "reference"])
+    ap.add_argument(
+        "--scene",
+        default="precision",
+        choices=["precision", "gaussian", "full"],
+        help="precision: N sources of size^3 (default); gaussian: 128^3 scalar + curl at 512x512; "
+        "full: 3 x 256^3 + 1M particles, iso, 2 clipping planes, SSAO at 1080p",
+    )
     ap.add_argument("--size", type=int, default=512, help="edge of each cubic source volume")
     ap.add_argument("--sources", type=int, default=4)
     ap.add_argument("--width", type=int, default=1920)
@@ -123,52 +130,135 @@ class ClockSampler:
         return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def apply_scene_defaults(args):
+    """The gaussian and full scenes fix their own sizes."""
+    if args.scene == "gaussian":
+        args.size, args.width, args.height, args.sources = 128, 512, 512, 2
+    elif args.scene == "full":
+        args.size, args.sources = 256, 3
+        args.width = args.width or 1920
+        args.height = args.height or 1080
+
+
+class Scene:
+    """Inputs of one benchmark scene (device tensors) and its settings."""
+
+    def __init__(self):
+        self.volumes = []  # (tensor, featureDim)
+        self.functions = []
+        self.transfer = []
+        self.iso = []
+        self.particles = None  # (offsets, positions, attributes, radius, cells)
+        self.clips = []
+        self.ao = False
+        self.P = self.MV = None
+
+
 def build_scene(args, device):
     import torch
 
     from isaac_b200 import scenes
 
     n = args.size
-    seeds = (6, 7, 8, 9, 10, 11, 12, 13)[: args.sources]
-    slopes = (-5.0 / 3.0, -2.0, -3.0, -11.0 / 3.0, -5.0 / 3.0, -2.0, -3.0, -11.0 / 3.0)[: args.sources]
-    fields = scenes.precision_scene(n, seeds=seeds, slopes=slopes, device=device)
-    tfs = [scenes.transfer_4point(0.7 * i) for i in range(args.sources)]
-    P, MV = scenes.camera(args.width, args.height, seed=3, distance=2.5)
-    torch.cuda.synchronize() if device != "cpu" else None
-    return fields, tfs, P, MV
+    sc = Scene()
+    if args.scene == "precision":
+        seeds = (6, 7, 8, 9, 10, 11, 12, 13)[: args.sources]
+        slopes = (-5.0 / 3.0, -2.0, -3.0, -11.0 / 3.0, -5.0 / 3.0, -2.0, -3.0, -11.0 / 3.0)[: args.sources]
+        fields = scenes.precision_scene(n, seeds=seeds, slopes=slopes, device=device)
+        sc.volumes = [(f, 1) for f in fields]
+        sc.functions = ["idem"] * len(fields)
+        sc.transfer = [scenes.transfer_4point(0.7 * i) for i in range(len(fields))]
+        sc.P, sc.MV = scenes.camera(args.width, args.height, seed=3, distance=2.5)
+    elif args.scene == "gaussian":
+        scalar, curl = scenes.gaussian_scene(n, seed=1, device=device)
+        sc.volumes = [(scalar.contiguous(), 1), (curl.contiguous(), 3)]
+        sc.functions = ["idem", "length"]
+        tf = scenes.transfer_4point(0.3)
+        sc.transfer = [tf, tf]
+        sc.P, sc.MV = scenes.camera(args.width, args.height, seed=1, distance=2.5, tilt=0.0)
+    else:
+        dens, E, s, p90 = scenes.density_gradient_scene(n, device=device)
+        sc.volumes = [(dens, 1), (E, 3), (s, 1)]
+        sc.functions = ["mul(2),add(1)", "length", "idem", "length"]
+        k = int(round(p90 * 1024))
+        sc.transfer = [
+            scenes.transfer_4point(0.2),
+            scenes.transfer_4point(1.4),
+            {0: (0.2, 0.6, 0.9, 0.0), max(k - 1, 1): (0.2, 0.6, 0.9, 0.0), k: (0.9, 0.8, 0.2, 1.0), 1024: (0.9, 0.8, 0.2, 1.0)},
+            {0: (0.1, 0.3, 1.0, 1.0), 1024: (1.0, 0.2, 0.1, 1.0)},
+        ]
+        sc.iso = [0.0, 0.0, 0.5]
+        off, pos, attr = scenes.particles_uniform(1_000_000, (n, n, n), seed=5, device=device)
+        sc.particles = (off, pos, attr, 0.25, (n, n, n))
+        sc.clips = [(0.3, 0.0, 0.0, -1.0, 0.1, 0.0), (0.0, 0.0, -0.4, 0.2, 0.1, 1.0)]
+        sc.ao = True
+        sc.P, sc.MV = scenes.camera(args.width, args.height, seed=2, distance=2.5)
+    if device != "cpu":
+        torch.cuda.synchronize()
+    return sc
 
 
-def make_viz(args, fields, tfs, P, MV):
-    from isaac_b200 import IsaacVisualization, VolumeSource
+def make_viz(args, sc):
+    from isaac_b200 import IsaacVisualization, ParticleSource, VolumeSource
 
     n = args.size
-    vols = [VolumeSource(f"field{i}", f, feature_dim=1, persistent=True) for i, f in enumerate(fields)]
-    viz = IsaacVisualization("bench", (args.width, args.height), (n, n, n), (n, n, n), (1, 1, 1), (0, 0, 0), vols)
-    for i, tf in enumerate(tfs):
+    vols = [VolumeSource(f"src{i}", t, feature_dim=fd, persistent=True) for i, (t, fd) in enumerate(sc.volumes)]
+    parts = []
+    pcells = (1, 1, 1)
+    if sc.particles is not None:
+        off, pos, attr, radius, pcells = sc.particles
+        parts = [ParticleSource("particles", off, pos, attr, radius=radius)]
+    viz = IsaacVisualization("bench", (args.width, args.height), (n, n, n), (n, n, n), pcells, (0, 0, 0), vols, parts)
+    viz._bench_keep = (vols, parts)
+    for i, f in enumerate(sc.functions):
+        viz.functions[i] = f
+    viz.updateFunctions()
+    for i, tf in enumerate(sc.transfer):
         viz.setTransferPoints(i, tf)
+    for i, v in enumerate(sc.iso):
+        viz.setIsoThreshold(i, v)
+    for c in sc.clips:
+        viz.addClipping(*c)
+    viz.setAmbientOcclusion(sc.ao, 0.5)
     viz.setInterpolation(True)
     viz.setStep(0.5)
-    viz.setCamera(P, MV)
+    viz.setCamera(sc.P, sc.MV)
     if args.renderer == "per_source":
         viz.setRenderOptimization(False)
         dt = {"f32": 0, "bf16": 1, "f16": 2}[args.dtype]
-        for i in range(len(fields)):
+        for i in range(len(sc.volumes)):
             viz.setStorage(i, dt)
     return viz
 
 
-def oracle_for(args, host_fields, tfs, P, MV):
+def oracle_for(args, sc):
     from oracle import oracle as O
 
     n = args.size
-    k = len(host_fields)
-    o = O.Oracle((args.width, args.height), (n, n, n), (n, n, n), (1, 1, 1), (0, 0, 0), (1, 1, 1), [1] * k, [1] * k, k)
-    for i, f in enumerate(host_fields):
-        o.set_source(i, f)
-        o.set_transfer(i, tfs[i])
+    nv = len(sc.volumes)
+    fds = [fd for _, fd in sc.volumes]
+    npart = 1 if sc.particles is not None else 0
+    pcells = sc.particles[4] if npart else (1, 1, 1)
+    if npart:
+        fds = fds + [int(sc.particles[2].shape[1])]
+    o = O.Oracle((args.width, args.height), (n, n, n), (n, n, n), pcells, (0, 0, 0), (1, 1, 1), fds, [1] * len(fds), nv)
+    for i, (t, _) in enumerate(sc.volumes):
+        o.set_source(i, t.cpu().numpy())
+    if npart:
+        off, pos, attr, radius, _ = sc.particles
+        o.set_particles(nv, off.cpu().numpy(), pos.cpu().numpy(), attr.cpu().numpy(), None, radius)
+    for i, f in enumerate(sc.functions):
+        o.set_functions(i, f)
+    for i, tf in enumerate(sc.transfer):
+        o.set_transfer(i, tf)
+    for i, v in enumerate(sc.iso):
+        o.set_iso(i, v)
+    for c in sc.clips:
+        o.add_clipping(*c)
+    o.set_ao(sc.ao, 0.5)
     o.set_interpolation(True)
     o.set_step(0.5)
-    o.set_camera(P, MV)
+    o.set_camera(sc.P, sc.MV)
     if args.renderer == "per_source":
         o.set_optimized(False)
     return o
@@ -203,10 +293,9 @@ def run_reference(args):
     if rank != 0:
         return 0
     dev = "cuda" if torch.cuda.is_available() else "cpu"
-    fields, tfs, P, MV = build_scene(args, dev)
-    host = [f.cpu().numpy() for f in fields]
-    del fields
-    o = oracle_for(args, host, tfs, P, MV)
+    sc = build_scene(args, dev)
+    o = oracle_for(args, sc)
+    del sc
     frame_times, sps = [], []
     rows = args.cpu_rows
     info = None
@@ -244,14 +333,24 @@ def run_reference(args):
 
 
 def metric_name(args):
-    return f"fps @{args.width}x{args.height}, {args.sources}x{args.size}^3 f32 sources, plain GPU ray-caster"
+    if args.scene == "precision":
+        return f"fps @{args.width}x{args.height}, {args.sources}x{args.size}^3 f32 sources, plain GPU ray-caster"
+    if args.scene == "gaussian":
+        return "fps @512x512, 128^3 scalar + curl sources, plain GPU ray-caster"
+    return f"fps @{args.width}x{args.height}, 3x256^3 sources + 1M particles, iso, 2 clip planes, SSAO"
 
 
 def config_of(args):
+    names = {
+        "precision": f"precision scene: {args.sources} x {args.size}^3 float32 spectral sources",
+        "gaussian": "8-Gaussian 128^3 scalar + analytic curl (chain length)",
+        "full": "full-feature scene: lognormal density, its gradient (length), iso scalar, 1M particles, 2 clip planes, SSAO",
+    }
     return {
-        "workload": f"precision scene: {args.sources} x {args.size}^3 float32 spectral sources, "
+        "workload": f"{names[args.scene]}, "
         f"{args.width}x{args.height}, trilinear, step 0.5, {args.renderer} renderer"
         + (f" ({args.dtype} bricks)" if args.renderer == "per_source" else ""),
+        "scene": args.scene,
         "sources": args.sources,
         "volume": args.size,
         "framebuffer": [args.width, args.height],
@@ -263,6 +362,7 @@ def config_of(args):
 
 def main():
     args = parse_args()
+    apply_scene_defaults(args)
     if args.impl == "reference":
         return run_reference(args)
 
@@ -290,8 +390,9 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    fields, tfs, P, MV = build_scene(args, "cuda")
-    viz = make_viz(args, fields, tfs, P, MV)
+    sc = build_scene(args, "cuda")
+    viz = make_viz(args, sc)
+    fields = [t for t, _ in sc.volumes]
 
     # samples of one frame, counted by the kernels (untimed)
     viz.setCounting(True)
@@ -338,7 +439,8 @@ def main():
     viz.setTiming(False)
     vol_ms = acc.get("shade_volume", 0.0)
     peak, peak_kind = measured_peaks()
-    bytes_per_sample = 32 if args.renderer == "combined" else {"f32": 4, "bf16": 2, "f16": 2}[args.dtype] * 8 * args.sources
+    esz = {"f32": 4, "bf16": 2, "f16": 2}[args.dtype]
+    bytes_per_sample = 32 if args.renderer == "combined" else esz * 8 * sum(fd for _, fd in sc.volumes)
     achieved = samples * bytes_per_sample / (vol_ms * 1e-3) / 1e9 if vol_ms > 0 else None
     traffic = None
     prof = ROOT / "profiles" / "traffic.json"
@@ -395,8 +497,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            host = [f.cpu().numpy() for f in fields]
-            o = oracle_for(args, host, tfs, P, MV)
+            o = oracle_for(args, sc)
             frame_s, sps, rows, merge_s, band_s, cs, threads = cpu_sample(args, o, args.cpu_rows)
             cpu = {
                 "value": 1.0 / frame_s,

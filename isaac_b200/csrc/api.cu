@@ -898,6 +898,23 @@ extern "C"
                 p.totalWeight += c->weight[s];
             }
             {
+                // colour sums are finite and >= 0 when every active table entry and weight is
+                bool nonneg = p.totalWeight > 0.0f && std::isfinite(p.totalWeight);
+                for(int s = 0; s < c->nVol && nonneg; ++s)
+                {
+                    if(!(c->weight[s] > 0.0f))
+                    {
+                        if(c->weight[s] < 0.0f || c->weight[s] != c->weight[s])
+                            nonneg = false;
+                        continue;
+                    }
+                    const float* l = c->lutHost.data() + size_t(s) * c->ts * 4;
+                    for(size_t k = 0; k < size_t(c->ts) * 4 && nonneg; ++k)
+                        nonneg = l[k] >= 0.0f && std::isfinite(l[k]);
+                }
+                p.nonNegative = nonneg ? 1 : 0;
+            }
+            {
                 int e2 = 0;
                 const float m = std::frexp(p.totalWeight, &e2);
                 // an exact power of two whose reciprocal is a normal float

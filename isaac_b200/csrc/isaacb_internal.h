@@ -27,6 +27,7 @@ namespace isaacb
         float iso[kMaxSources];
         float totalWeight;
         float invTotalWeight; // 2^-k when totalWeight == 2^k exactly, else 0
+        int32_t nonNegative; // every colour sum is finite and >= 0 (tables and weights >= 0, total > 0)
         uint4* volQ; // combined volume, quad bricks
         uint32_t* isoAQ; // combined iso alpha, quad bricks
         uint32_t* isoLin; // combined iso RGBA8, linear

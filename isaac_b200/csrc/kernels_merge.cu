@@ -33,6 +33,32 @@ namespace isaacb
         return uint32_t(round_nonneg(fminf(fmaxf(v, 0.0f), 1.0f) * 255.0f));
     }
 
+    // dither for colours known to be finite and >= 0 (every table entry and weight >= 0,
+    // total weight > 0): int(s) = floor(s), so one magic-number floor serves both terms
+    __device__ __forceinline__ uint32_t dither_rgba_nonneg(int mode, const uint8_t* mask, int x, int y, int z, float4 c)
+    {
+        const float v[4] = {c.x, c.y, c.z, c.w};
+        uint32_t out = 0;
+        if(mode == 0)
+        {
+#pragma unroll
+            for(int i = 0; i < 4; ++i)
+                out |= uint32_t(min(round_nonneg(fminf(v[i], 1.0f) * 255.0f), 255)) << (8 * i);
+            return out;
+        }
+        const float d = float(mask[(x & 3) + (y & 3) * 4 + (z & 3) * 16]) / 64.0f;
+#pragma unroll
+        for(int i = 0; i < 4; ++i)
+        {
+            const float s = fminf(v[i] * 255.0f, 257.0f);
+            float fl;
+            int fi;
+            floor_split(s, fl, fi);
+            out |= uint32_t(min(fi + ((s - fl) > d ? 1 : 0), 255)) << (8 * i);
+        }
+        return out;
+    }
+
     // mask: the mode's 64-entry table (shared memory copy), unused for mode 0
     __device__ __forceinline__ uint32_t dither_rgba(int mode, const uint8_t* mask, int x, int y, int z, float4 c)
     {
@@ -109,7 +135,7 @@ namespace isaacb
     // t+512) and keeps their colour sums in registers while the sources are visited
     // in the outer loop, so per-source state (chain, table, weights) is uniform and
     // loaded once.  fetch(s, x, y, z, v) reads a clamped voxel.
-    template<class Fetch>
+    template<bool ISO, class Fetch>
     __device__ __forceinline__ void merge_brick(
         const MergeParams& p,
         int bx,
@@ -156,7 +182,7 @@ namespace isaacb
                     vc[j].z += c.z * a;
                     vc[j].w += a;
                 }
-                if(it > 0.0f)
+                if(ISO && it > 0.0f)
                 {
                     const float a = c.w / it * 0.5f;
                     if(ic[j].w < a)
@@ -203,10 +229,11 @@ namespace isaacb
             {
                 c = make_float4(c.x / p.totalWeight, c.y / p.totalWeight, c.z / p.totalWeight, c.w / p.totalWeight);
             }
-            const uint32_t vb = dither_rgba(p.ditherMode, mask, xs[j], ys[j], zs[j], c);
+            const uint32_t vb = p.nonNegative ? dither_rgba_nonneg(p.ditherMode, mask, xs[j], ys[j], zs[j], c)
+                                              : dither_rgba(p.ditherMode, mask, xs[j], ys[j], zs[j], c);
             volS[t] = vb;
             anyVol |= vb != 0u;
-            if(p.writeIso)
+            if(ISO)
             {
                 const float4 q = ic[j];
                 const uint32_t ib = round_byte(q.x) | (round_byte(q.y) << 8) | (round_byte(q.z) << 16) | (round_byte(q.w) << 24);
@@ -263,8 +290,8 @@ namespace isaacb
     // [8b-4, 8b+12) x [8b-1, 8b+8) x [8b-1, 8b+8) (the x start rounded down to a
     // 16-byte boundary; out-of-volume elements are never read) into shared memory
     // with one cp.async.bulk.tensor per source, completing on an mbarrier.
-    template<bool TMA>
-    __global__ void __launch_bounds__(256) k_merge(const __grid_constant__ MergeParams p)
+    template<bool TMA, bool ISO>
+    __global__ void __launch_bounds__(256, 5) k_merge(const __grid_constant__ MergeParams p)
     {
         extern __shared__ __align__(128) unsigned char dsm[];
         __shared__ uint32_t volS[kApron * kApron * kApron];
@@ -321,13 +348,13 @@ namespace isaacb
         int myIsoMax = 0;
         if(TMA)
         {
-            merge_brick(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, sMask, TileFetch{p, tiles, x0, y0, z0});
+            merge_brick<ISO>(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, sMask, TileFetch{p, tiles, x0, y0, z0});
         }
         else
         {
-            merge_brick(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, sMask, GlobalFetch{p});
+            merge_brick<ISO>(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, sMask, GlobalFetch{p});
         }
-        if(p.writeIso)
+        if(ISO)
             atomicMax(&isoMax, myIsoMax);
         anyVol = __syncthreads_or(anyVol);
         const size_t brick = (size_t(bz) * g.nb[1] + by) * g.nb[0] + bx;
@@ -336,7 +363,7 @@ namespace isaacb
             p.volFlag[brick] = anyVol ? 1 : 0;
             if(!anyVol)
                 atomicAdd(p.emptyBricks, 1u);
-            if(p.writeIso)
+            if(ISO)
                 p.isoFlag[brick] = uint8_t(isoMax);
         }
         for(int s = threadIdx.x; s < kSlotsPerBrick; s += blockDim.x)
@@ -345,14 +372,14 @@ namespace isaacb
             const int t = (lz * kApron + ly) * kApron + lx;
             uint4 q = make_uint4(volS[t], volS[t + 1], volS[t + kApron], volS[t + kApron + 1]);
             p.volQ[brick * kSlotsPerBrick + s] = q;
-            if(p.writeIso)
+            if(ISO)
             {
                 uint32_t a = (isoS[t] >> 24) | ((isoS[t + 1] >> 24) << 8) | ((isoS[t + kApron] >> 24) << 16)
                     | ((isoS[t + kApron + 1] >> 24) << 24);
                 p.isoAQ[brick * kSlotsPerBrick + s] = a;
             }
         }
-        if(p.writeIso)
+        if(ISO)
         {
             // interior voxels 8b..8b+7 of this brick in the linear iso texture
             for(int t = threadIdx.x; t < 512; t += blockDim.x)
@@ -371,13 +398,21 @@ namespace isaacb
         dim3 grid(p.g.nb[0], p.g.nb[1], p.g.nb[2]);
         if(p.useTma)
         {
-            cudaFuncSetAttribute(k_merge<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, p.tileBytes + 128);
-            k_merge<true><<<grid, 256, p.tileBytes + 128, s>>>(p);
+            if(p.writeIso)
+            {
+                cudaFuncSetAttribute(k_merge<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, p.tileBytes + 128);
+                k_merge<true, true><<<grid, 256, p.tileBytes + 128, s>>>(p);
+            }
+            else
+            {
+                cudaFuncSetAttribute(k_merge<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, p.tileBytes + 128);
+                k_merge<true, false><<<grid, 256, p.tileBytes + 128, s>>>(p);
+            }
         }
+        else if(p.writeIso)
+            k_merge<false, true><<<grid, 256, 0, s>>>(p);
         else
-        {
-            k_merge<false><<<grid, 256, 0, s>>>(p);
-        }
+            k_merge<false, false><<<grid, 256, 0, s>>>(p);
     }
 
     // ---------------------------------------------------------------- per-source bricks
