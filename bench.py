@@ -45,10 +45,14 @@ def parse_args():
     ap.add_argument(
         "--scene",
         default="precision",
-        choices=["precision", "gaussian", "full"],
+        choices=["precision", "gaussian", "full", "batch"],
         help="precision: N sources of size^3 (default); gaussian: 128^3 scalar + curl at 512x512; "
-        "full: 3 x 256^3 + 1M particles, iso, 2 clipping planes, SSAO at 1080p",
+        "full: 3 x 256^3 + 1M particles, iso, 2 clipping planes, SSAO at 1080p; "
+        "batch: the precision sources over 4 timesteps, 16 views of uneven resolution in one launch",
     )
+    ap.add_argument("--timesteps", type=int, default=4, help="batch scene: timesteps (contexts)")
+    ap.add_argument("--shift", type=float, default=0.05, help="batch scene: advection per timestep, fraction of the box")
+    ap.add_argument("--no-autotune", action="store_true", help="batch scene: keep the default launch shape")
     ap.add_argument("--size", type=int, default=512, help="edge of each cubic source volume")
     ap.add_argument("--sources", type=int, default=4)
     ap.add_argument("--width", type=int, default=1920)
@@ -333,6 +337,11 @@ def run_reference(args):
 
 
 def metric_name(args):
+    if args.scene == "batch":
+        return (
+            f"batch frames/s: 16 views (4x256^2, 4x720p, 4x1080p, 4x2048x1152) over {args.timesteps} timesteps "
+            f"of {args.sources}x{args.size}^3 f32 sources, one persistent launch under a CUDA graph"
+        )
     if args.scene == "precision":
         return f"fps @{args.width}x{args.height}, {args.sources}x{args.size}^3 f32 sources, plain GPU ray-caster"
     if args.scene == "gaussian":
@@ -345,7 +354,20 @@ def config_of(args):
         "precision": f"precision scene: {args.sources} x {args.size}^3 float32 spectral sources",
         "gaussian": "8-Gaussian 128^3 scalar + analytic curl (chain length)",
         "full": "full-feature scene: lognormal density, its gradient (length), iso scalar, 1M particles, 2 clip planes, SSAO",
+        "batch": f"batching scene: {args.timesteps} timesteps (advected {args.shift} box/step) of {args.sources} x "
+        f"{args.size}^3 float32 spectral sources, 16 views of uneven resolution",
     }
+    if args.scene == "batch":
+        return {
+            "workload": names["batch"] + ", trilinear, step 0.5, combined renderer, 4 merges + 1 persistent render per step",
+            "scene": "batch",
+            "sources": args.sources,
+            "volume": args.size,
+            "timesteps": args.timesteps,
+            "views": [list(r) for r in _batch_resolutions()],
+            "parallelism": "replicas",
+            "l2": "inputs larger than L2 (sources and textures are > 126 MB)",
+        }
     return {
         "workload": f"{names[args.scene]}, "
         f"{args.width}x{args.height}, trilinear, step 0.5, {args.renderer} renderer"
@@ -360,11 +382,300 @@ def config_of(args):
     }
 
 
+# ---------------------------------------------------------------------------- batching scene
+def _batch_resolutions():
+    from isaac_b200 import scenes
+
+    return scenes.BATCH_RESOLUTIONS
+
+
+def build_batch_scenes(args, device):
+    """One Scene per timestep: the precision sources advected by t * shift of the box along x."""
+    import torch
+
+    from isaac_b200 import scenes
+
+    seeds = (6, 7, 8, 9, 10, 11, 12, 13)[: args.sources]
+    slopes = (-5.0 / 3.0, -2.0, -3.0, -11.0 / 3.0, -5.0 / 3.0, -2.0, -3.0, -11.0 / 3.0)[: args.sources]
+    out = []
+    for t in range(args.timesteps):
+        sc = Scene()
+        fields = scenes.precision_scene(args.size, seeds=seeds, slopes=slopes, device=device, shift=t * args.shift)
+        sc.volumes = [(f, 1) for f in fields]
+        sc.functions = ["idem"] * len(fields)
+        sc.transfer = [scenes.transfer_4point(0.7 * i) for i in range(len(fields))]
+        sc.P, sc.MV = scenes.camera(256, 256, seed=3, distance=2.5)
+        out.append(sc)
+    if device != "cpu":
+        torch.cuda.synchronize()
+    return out
+
+
+def _small(args):
+    """The contexts of a batch keep only a small framebuffer of their own."""
+    a = argparse.Namespace(**vars(args))
+    a.width = a.height = 256
+    return a
+
+
+def cpu_batch_sample(args, o, views, rows_hint=0):
+    """Oracle time of one batch frame, from a bounded sample: one merge (every
+    timestep's merge costs the same) and, per resolution class, a band of rows
+    of the class's first view (views 0, 4, 8, 12 show timestep 0), extrapolated
+    to the class's four views.  Returns (seconds, sample description, threads)."""
+    from oracle import oracle as O
+
+    threads = O.num_threads()
+    t0 = time.perf_counter()
+    o.update()
+    merge_s = time.perf_counter() - t0
+    total = args.timesteps * merge_s
+    per_class = len(views) // 4
+    parts = []
+    for c in range(4):
+        ts, w, h, P, MV = views[c * per_class]
+        rows = min(h, rows_hint or max(8, 2 * threads))
+        r0 = h // 2 - rows // 2
+        o.set_framebuffer(w, h)
+        o.set_camera(P, MV)
+        t1 = time.perf_counter()
+        o.render(rows=(r0, r0 + rows))
+        band = time.perf_counter() - t1
+        total += per_class * band * h / rows
+        parts.append(f"{rows}/{h} rows of {w}x{h}")
+    desc = (
+        f"one merge of {args.sources}x{args.size}^3 ({merge_s:.2f} s) x {args.timesteps} timesteps + "
+        f"per resolution class a band ({', '.join(parts)}) x {per_class} views, extrapolated to a batch frame"
+    )
+    return total, desc, threads
+
+
+def run_reference_batch(args):
+    import torch
+
+    from isaac_b200 import scenes
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    a = argparse.Namespace(**vars(args))
+    a.timesteps = 1
+    sc = build_batch_scenes(a, dev)[0]
+    o = oracle_for(_small(args), sc)
+    del sc
+    views = scenes.batch_views(timesteps=args.timesteps)
+    times = []
+    desc, threads = "", 1
+    for i in range(args.warmup + args.steps):
+        t, desc, threads = cpu_batch_sample(args, o, views, args.cpu_rows)
+        if i >= args.warmup:
+            times.append(t)
+    sec = sorted(times)[len(times) // 2]
+    v = 1.0 / sec
+    line = {
+        "metric": metric_name(args),
+        "value": v,
+        "unit": "batch frames/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": sec * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "impl": "reference",
+        "config": config_of(args),
+        "views_per_s": v * len(views),
+        "cpu_baseline": {"value": v, "unit": "batch frames/s", "cores": threads, "kind": "port", "sample": desc},
+        "e2e": {"value": v, "unit": "batch frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CPU backend not buildable here (alpaka/Boost/glm/IceT/MPI absent); oracle/ CPU restatement timed instead",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batch(args, world, rank, local, barrier, max_over_ranks):
+    """All views of all timesteps per step: the timesteps' merges and one
+    persistent render launch, replayed as one captured CUDA graph."""
+    import torch
+
+    from isaac_b200 import scenes
+    from isaac_b200.batch import IsaacBatch
+
+    steps_sc = build_batch_scenes(args, "cuda")
+    small = _small(args)
+    vis = [make_viz(small, sc) for sc in steps_sc]
+    views = scenes.batch_views(timesteps=args.timesteps)
+    batch = IsaacBatch(vis, views)
+    stream = torch.cuda.Stream()
+    tuned = None
+    with torch.cuda.stream(stream):
+        batch.render(update=True)
+        batch.setCounting(True)
+        batch.render(update=False)
+        samples = batch.samples()
+        batch.setCounting(False)
+        if not args.no_autotune:
+            cfg, tms = batch.autotune()
+            tuned = {"tile": [cfg.tile_w, cfg.tile_h], "blocks_per_sm": cfg.blocks_per_sm, "skip_empty": cfg.skip_empty,
+                     "render_ms": tms}
+        cfg = batch.config
+        batch.capture(update=True)
+        for _ in range(args.warmup):
+            batch.launchGraph()
+    stream.synchronize()
+
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            batch.launchGraph()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clk.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    value = world * 1000.0 / ms
+
+    # phases (events on the launch stream): the merges, the persistent render, and the same
+    # views drawn with one launch per view for comparison
+    nt = max(3, min(args.steps, 8))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    singles = [IsaacBatch(vis, [v]) for v in views]
+    for s1 in singles:
+        s1.setConfig(cfg.tile_w, cfg.tile_h, cfg.blocks_per_sm, cfg.skip_empty)
+    merge_ms = render_ms = single_ms = 0.0
+    with torch.cuda.stream(stream):
+        for _ in range(nt):
+            ev[0].record(stream)
+            for v in vis:
+                v.update()
+            ev[1].record(stream)
+            batch.render(update=False)
+            ev[2].record(stream)
+            for s1 in singles:
+                s1.render(update=False)
+            ev[3].record(stream)
+            ev[3].synchronize()
+            merge_ms += ev[0].elapsed_time(ev[1]) / nt
+            render_ms += ev[1].elapsed_time(ev[2]) / nt
+            single_ms += ev[2].elapsed_time(ev[3]) / nt
+    for s1 in singles:
+        s1.close()
+    peak, peak_kind = measured_peaks()
+    achieved = samples * 32 / (render_ms * 1e-3) / 1e9 if render_ms > 0 else None
+    roofline = {
+        "bound": "hbm",
+        "kernel": "k_batch (persistent multi-view shading + volume ray-march)",
+        "achieved": achieved,
+        "peak": peak,
+        "peak_kind": peak_kind,
+        "unit": "GB/s",
+        "frac": (achieved / peak) if achieved else None,
+        "traffic": None,
+        "algorithmic_bytes_per_sample": 32,
+        "samples_per_launch": samples,
+        "kernel_ms": render_ms,
+    }
+
+    e2e = None
+    if not args.no_e2e:
+        fields = [t for sc in steps_sc for t, _ in sc.volumes]
+        host_src = [f.cpu().pin_memory() for f in fields]
+        host_frames = [torch.empty(f.shape, dtype=torch.uint8).pin_memory() for f in batch.frames]
+        h2d = sum(h.numel() * h.element_size() for h in host_src)
+        d2h = sum(h.numel() for h in host_frames)
+
+        def e2e_step():
+            for h, d in zip(host_src, fields):
+                d.copy_(h, non_blocking=True)
+            batch.launchGraph()
+            for h, d in zip(host_frames, batch.frames):
+                h.copy_(d, non_blocking=True)
+            stream.synchronize()
+
+        with torch.cuda.stream(stream):
+            for _ in range(2):
+                e2e_step()
+            ne = max(3, min(args.steps, 5))
+            barrier()
+            torch.cuda.synchronize()
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            for _ in range(ne):
+                e2e_step()
+            t1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e2e_ms = max_over_ranks(t0.elapsed_time(t1) / ne)
+        e2e = {"value": world * 1000.0 / e2e_ms, "unit": "batch frames/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms}
+        del host_src, host_frames
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            o = oracle_for(small, steps_sc[0])
+            sec, desc, threads = cpu_batch_sample(args, o, views, args.cpu_rows)
+            cpu = {"value": 1.0 / sec, "unit": "batch frames/s", "cores": threads, "kind": "port", "sample": desc}
+            del o
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "batch frames/s", "cores": None, "kind": "port", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        pixels = sum(w * h for _, w, h, _, _ in views)
+        line = {
+            "metric": metric_name(args),
+            "value": value,
+            "unit": "batch frames/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded spectral fields, advected per timestep)",
+            "config": config_of(args),
+            "views_per_s": value * len(views),
+            "mpixels_per_s": value * pixels / 1e6,
+            "gsamples_per_s": samples * value / 1e9,
+            "samples_per_frame": samples,
+            "phases_ms": {"merges": merge_ms, "render": render_ms, "render_one_launch_per_view": single_ms},
+            "launch": {"tile": [cfg.tile_w, cfg.tile_h], "blocks_per_sm": cfg.blocks_per_sm, "skip_empty": cfg.skip_empty,
+                       "autotuned": tuned, "cuda_graph": True},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clocks,
+            "gpu_launches": args.steps * (len(vis) + 1),
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    for v in vis:
+        v.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse_args()
     apply_scene_defaults(args)
     if args.impl == "reference":
-        return run_reference(args)
+        return run_reference_batch(args) if args.scene == "batch" else run_reference(args)
 
     import numpy as np
     import torch
@@ -389,6 +700,9 @@ def main():
         t = torch.tensor([v], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    if args.scene == "batch":
+        return run_batch(args, world, rank, local, barrier, max_over_ranks)
 
     sc = build_scene(args, "cuda")
     viz = make_viz(args, sc)

@@ -229,6 +229,59 @@ isaacb_status isaacb_minmax_noalloc(
     float* result,
     void* stream);
 
+/* ---- Batched views (no counterpart in the reference, which draws one view per
+ * doVisualization).  A batch renders many views of one or more contexts -- e.g.
+ * the timesteps of a simulation, each its own context -- in ONE persistent
+ * launch whose CTAs take 256-pixel tiles from a work queue.  Views draw the
+ * combined volume exactly as isaacb_render does for a context without particle
+ * sources, iso thresholds or SSAO (those contexts are rejected). */
+typedef struct isaacb_view
+{
+    uint32_t ctx_index; /* index into the batch's context array */
+    uint32_t width, height;
+    uint32_t reserved;
+    double projection[16]; /* column major, as isaacb_set_camera */
+    double modelview[16];
+    uint8_t* rgba_dev; /* width*height*4 bytes of device memory */
+} isaacb_view;
+
+typedef struct isaacb_batch_config
+{
+    uint32_t tile_w, tile_h; /* tile_w*tile_h == 256, tile_w % 8 == 0, tile_h % 4 == 0 */
+    uint32_t blocks_per_sm; /* 0 = as many as fit */
+    int32_t skip_empty; /* 1 check per-brick emptiness, 0 never, -1 per context (default) */
+} isaacb_batch_config;
+
+typedef struct isaacb_batch isaacb_batch;
+
+isaacb_status isaacb_batch_create(
+    isaacb_ctx* const* ctxs,
+    uint32_t n_ctx,
+    const isaacb_view* views,
+    uint32_t n_views,
+    isaacb_batch** out);
+isaacb_status isaacb_batch_destroy(isaacb_batch* batch);
+isaacb_status isaacb_batch_set_config(isaacb_batch* batch, const isaacb_batch_config* cfg);
+isaacb_status isaacb_batch_get_config(const isaacb_batch* batch, isaacb_batch_config* cfg);
+/* New camera of one view; takes effect at the next render or graph launch. */
+isaacb_status isaacb_batch_set_camera(isaacb_batch* batch, uint32_t view, const double projection[16], const double modelview[16]);
+/* One batch frame on `stream`: with `update`, the merge of every context first
+ * (isaacb_update), then the persistent launch over all views.  Asynchronous. */
+isaacb_status isaacb_batch_render(isaacb_batch* batch, void* stream, int32_t update);
+/* Capture the same work (merges when `update`, queue reset, persistent launch)
+ * into a CUDA graph; isaacb_batch_launch_graph replays it.  `stream` must not be
+ * the legacy default stream.  Transfer tables, weights and cameras are read at
+ * capture time for the merges and at launch time for the views. */
+isaacb_status isaacb_batch_capture(isaacb_batch* batch, void* stream, int32_t update);
+isaacb_status isaacb_batch_launch_graph(isaacb_batch* batch, void* stream);
+/* Time every tile shape x occupancy x skipping candidate on the current views
+ * (CUDA events, a few launches each), keep the fastest, return it and its time.
+ * Synchronous on `stream`. */
+isaacb_status isaacb_batch_autotune(isaacb_batch* batch, void* stream, isaacb_batch_config* best, float* best_ms);
+/* Ray-march loop trips of the last batch render (counting costs one atomic per warp). */
+isaacb_status isaacb_batch_set_counting(isaacb_batch* batch, int32_t enabled);
+isaacb_status isaacb_batch_get_samples(isaacb_batch* batch, void* stream, uint64_t* samples);
+
 /* Number of kernels the last isaacb_update / isaacb_render enqueued. */
 isaacb_status isaacb_get_launch_count(isaacb_ctx* ctx, uint32_t* update_launches, uint32_t* render_launches);
 

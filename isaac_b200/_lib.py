@@ -51,6 +51,31 @@ class Desc(C.Structure):
     ]
 
 
+class View(C.Structure):
+    """``isaacb_view``: one camera of a batch, rendered into ``rgba_dev``."""
+
+    _fields_ = [
+        ("ctx_index", C.c_uint32),
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("projection", C.c_double * 16),
+        ("modelview", C.c_double * 16),
+        ("rgba_dev", C.c_void_p),
+    ]
+
+
+class BatchConfig(C.Structure):
+    """``isaacb_batch_config``: tile shape, CTAs per SM and empty-brick skipping."""
+
+    _fields_ = [
+        ("tile_w", C.c_uint32),
+        ("tile_h", C.c_uint32),
+        ("blocks_per_sm", C.c_uint32),
+        ("skip_empty", C.c_int32),
+    ]
+
+
 class IsaacError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
@@ -106,6 +131,17 @@ SIGNATURES = {
     "isaacb_set_timing": (_i32, [_P, _i32]),
     "isaacb_get_timing": (_i32, [_P, _P, _fp]),
     "isaacb_minmax_noalloc": (_i32, [_P, _u32p, _u32, _i32p, _fp, _P, _P]),
+    "isaacb_batch_create": (_i32, [C.POINTER(_P), _u32, C.POINTER(View), _u32, C.POINTER(_P)]),
+    "isaacb_batch_destroy": (_i32, [_P]),
+    "isaacb_batch_set_config": (_i32, [_P, C.POINTER(BatchConfig)]),
+    "isaacb_batch_get_config": (_i32, [_P, C.POINTER(BatchConfig)]),
+    "isaacb_batch_set_camera": (_i32, [_P, _u32, _dp, _dp]),
+    "isaacb_batch_render": (_i32, [_P, _P, _i32]),
+    "isaacb_batch_capture": (_i32, [_P, _P, _i32]),
+    "isaacb_batch_launch_graph": (_i32, [_P, _P]),
+    "isaacb_batch_autotune": (_i32, [_P, _P, C.POINTER(BatchConfig), _fp]),
+    "isaacb_batch_set_counting": (_i32, [_P, _i32]),
+    "isaacb_batch_get_samples": (_i32, [_P, _P, _u64p]),
 }
 
 

@@ -41,6 +41,7 @@ SOURCES = [
     "kernels_render.cu",
     "kernels_legacy.cu",
     "minmax_static.cu",
+    "kernels_batch.cu",
 ]
 
 

@@ -497,6 +497,82 @@ namespace
         c->tmapPtr[s] = src;
         return true;
     }
+
+    // the merge's launch parameters from a context's state (no launch, no stream work)
+    void prepare_merge(isaacb_ctx* c, MergeParams& p)
+    {
+        p.g = c->g;
+        p.nVol = c->nVol;
+        p.ts = c->ts;
+        p.ditherMode = c->ditherMode;
+        p.writeIso = any_iso_active(c) ? 1 : 0;
+        p.lut = c->lutDev;
+        p.totalWeight = 0.0f;
+        for(int s = 0; s < c->nVol; ++s)
+        {
+            p.src[s] = c->src[s];
+            p.fdim[s] = int32_t(c->desc.feature_dim[s]);
+            p.chain[s] = c->chain[s];
+            p.chainIdem[s] = (c->chain[s].op[0] == OP_IDEM && c->chain[s].op[1] == OP_IDEM && c->chain[s].op[2] == OP_IDEM) ? 1 : 0;
+            p.weight[s] = c->weight[s];
+            p.iso[s] = c->iso[s];
+            p.totalWeight += c->weight[s];
+        }
+        {
+            // colour sums are finite and >= 0 when every active table entry and weight is
+            bool nonneg = p.totalWeight > 0.0f && std::isfinite(p.totalWeight);
+            for(int s = 0; s < c->nVol && nonneg; ++s)
+            {
+                if(!(c->weight[s] > 0.0f))
+                {
+                    if(c->weight[s] < 0.0f || c->weight[s] != c->weight[s])
+                        nonneg = false;
+                    continue;
+                }
+                const float* l = c->lutHost.data() + size_t(s) * c->ts * 4;
+                for(size_t k = 0; k < size_t(c->ts) * 4 && nonneg; ++k)
+                    nonneg = l[k] >= 0.0f && std::isfinite(l[k]);
+            }
+            p.nonNegative = nonneg ? 1 : 0;
+        }
+        {
+            int e2 = 0;
+            const float m = std::frexp(p.totalWeight, &e2);
+            // an exact power of two whose reciprocal is a normal float
+            p.invTotalWeight = (m == 0.5f && e2 > -120 && e2 < 120) ? std::ldexp(1.0f, 1 - e2) : 0.0f;
+        }
+        p.volQ = c->volQ;
+        p.isoAQ = c->isoAQ;
+        p.isoLin = c->isoLin;
+        p.volFlag = c->volFlag;
+        p.isoFlag = c->isoFlag;
+        p.errorFlag = c->errorFlag;
+        p.emptyBricks = c->emptyDev;
+        // stage sources with TMA when every active one is 16-byte aligned with
+        // rows of a multiple of 16 bytes and the tiles fit in shared memory
+        p.useTma = 1;
+        int bytes = 0, tx = 0;
+        for(int s = 0; s < c->nVol; ++s)
+        {
+            p.tileOffset[s] = -1;
+            if(!(c->weight[s] + c->iso[s] > 0.0f))
+                continue;
+            if(!encode_source_map(c, s))
+            {
+                p.useTma = 0;
+                break;
+            }
+            p.tmap[s] = c->tmap[s];
+            p.tileOffset[s] = bytes;
+            const int tile = 16 * int(c->desc.feature_dim[s]) * kApron * kApron * 4;
+            bytes += (tile + 127) & ~127;
+            tx += tile;
+        }
+        p.tileBytes = bytes;
+        p.txBytes = tx;
+        if(bytes == 0 || bytes > 160 * 1024)
+            p.useTma = 0;
+    }
 } // namespace
 
 extern "C"
@@ -880,78 +956,8 @@ extern "C"
         if(c->renderer == ISAACB_RENDERER_COMBINED)
         {
             MergeParams p{};
-            p.g = c->g;
-            p.nVol = c->nVol;
-            p.ts = c->ts;
-            p.ditherMode = c->ditherMode;
-            p.writeIso = any_iso_active(c) ? 1 : 0;
-            p.lut = c->lutDev;
-            p.totalWeight = 0.0f;
-            for(int s = 0; s < c->nVol; ++s)
-            {
-                p.src[s] = c->src[s];
-                p.fdim[s] = int32_t(c->desc.feature_dim[s]);
-                p.chain[s] = c->chain[s];
-                p.chainIdem[s] = (c->chain[s].op[0] == OP_IDEM && c->chain[s].op[1] == OP_IDEM && c->chain[s].op[2] == OP_IDEM) ? 1 : 0;
-                p.weight[s] = c->weight[s];
-                p.iso[s] = c->iso[s];
-                p.totalWeight += c->weight[s];
-            }
-            {
-                // colour sums are finite and >= 0 when every active table entry and weight is
-                bool nonneg = p.totalWeight > 0.0f && std::isfinite(p.totalWeight);
-                for(int s = 0; s < c->nVol && nonneg; ++s)
-                {
-                    if(!(c->weight[s] > 0.0f))
-                    {
-                        if(c->weight[s] < 0.0f || c->weight[s] != c->weight[s])
-                            nonneg = false;
-                        continue;
-                    }
-                    const float* l = c->lutHost.data() + size_t(s) * c->ts * 4;
-                    for(size_t k = 0; k < size_t(c->ts) * 4 && nonneg; ++k)
-                        nonneg = l[k] >= 0.0f && std::isfinite(l[k]);
-                }
-                p.nonNegative = nonneg ? 1 : 0;
-            }
-            {
-                int e2 = 0;
-                const float m = std::frexp(p.totalWeight, &e2);
-                // an exact power of two whose reciprocal is a normal float
-                p.invTotalWeight = (m == 0.5f && e2 > -120 && e2 < 120) ? std::ldexp(1.0f, 1 - e2) : 0.0f;
-            }
-            p.volQ = c->volQ;
-            p.isoAQ = c->isoAQ;
-            p.isoLin = c->isoLin;
-            p.volFlag = c->volFlag;
-            p.isoFlag = c->isoFlag;
-            p.errorFlag = c->errorFlag;
-            p.emptyBricks = c->emptyDev;
+            prepare_merge(c, p);
             ISAACB_CUDA(c, cudaMemsetAsync(c->emptyDev, 0, sizeof(unsigned int), st), "empty brick counter");
-            // stage sources with TMA when every active one is 16-byte aligned with
-            // rows of a multiple of 16 bytes and the tiles fit in shared memory
-            p.useTma = 1;
-            int bytes = 0, tx = 0;
-            for(int s = 0; s < c->nVol; ++s)
-            {
-                p.tileOffset[s] = -1;
-                if(!(c->weight[s] + c->iso[s] > 0.0f))
-                    continue;
-                if(!encode_source_map(c, s))
-                {
-                    p.useTma = 0;
-                    break;
-                }
-                p.tmap[s] = c->tmap[s];
-                p.tileOffset[s] = bytes;
-                const int tile = 16 * int(c->desc.feature_dim[s]) * kApron * kApron * 4;
-                bytes += (tile + 127) & ~127;
-                tx += tile;
-            }
-            p.tileBytes = bytes;
-            p.txBytes = tx;
-            if(bytes == 0 || bytes > 160 * 1024)
-                p.useTma = 0;
             {
                 for(int k = 0; k < ISAACB_TIMING_SLOTS; ++k)
                     c->evUsed[k] = false;
@@ -1324,6 +1330,452 @@ extern "C"
             *upd = c->updateLaunches;
         if(ren)
             *ren = c->renderLaunches;
+        return ISAACB_OK;
+    }
+}
+
+// ---------------------------------------------------------------------------- batched views
+struct isaacb_batch
+{
+    std::vector<isaacb_ctx*> ctxs;
+    std::vector<isaacb_view> views;
+    isaacb_batch_config cfg{32, 8, 0, -1};
+    BatchCtx* ctxDev = nullptr;
+    BatchView* viewDev = nullptr;
+    BatchCtx* ctxPinned = nullptr;
+    BatchView* viewPinned = nullptr;
+    cudaEvent_t tableEvent = nullptr;
+    int32_t* counter = nullptr;
+    unsigned long long* samples = nullptr;
+    bool counting = false;
+    int totalTiles = 0;
+    int numSMs = 148;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graphExec = nullptr;
+    bool graphUpdate = false;
+    std::vector<MergeParams> graphMerges; // merge parameters a captured graph holds
+};
+
+namespace
+{
+    isaacb_status batch_fail(isaacb_status st, const std::string& m)
+    {
+        return fail(nullptr, st, m);
+    }
+
+    // a context can join a batch when a view of it is the combined volume alone
+    bool batchable(const isaacb_ctx* c, std::string& why)
+    {
+        if(c->renderer != ISAACB_RENDERER_COMBINED)
+            why = "per-source renderer";
+        else if(any_iso_active(c))
+            why = "iso threshold set";
+        else if(c->aoEnabled && c->aoWeight > 0.0f)
+            why = "SSAO enabled";
+        else
+        {
+            for(int s = 0; s < c->nPart; ++s)
+                if(c->weight[c->nVol + s] != 0.0f)
+                {
+                    why = "particle source with weight";
+                    return false;
+                }
+            return true;
+        }
+        return false;
+    }
+
+    void view_inverse(const double* proj, const double* mv, float* out)
+    {
+        float P[16], MV[16], PM[16];
+        for(int i = 0; i < 16; ++i)
+        {
+            P[i] = float(proj[i]);
+            MV[i] = float(mv[i]);
+        }
+        mul4(P, MV, PM);
+        inverse4(PM, out);
+    }
+
+    // host mirror of the device tables from the contexts' current state; uploaded on `st`
+    isaacb_status batch_refresh(isaacb_batch* b, cudaStream_t st)
+    {
+        if(cudaEventSynchronize(b->tableEvent) != cudaSuccess)
+            return batch_fail(ISAACB_CUDA_ERROR, "batch table staging wait");
+        for(size_t i = 0; i < b->ctxs.size(); ++i)
+        {
+            isaacb_ctx* c = b->ctxs[i];
+            if(cudaEventQuery(c->emptyEvent) == cudaSuccess)
+                c->lastEmpty = (long long) *c->emptyPinned;
+            BatchCtx& t = b->ctxPinned[i];
+            std::memset(&t, 0, sizeof(t));
+            t.g = c->g;
+            t.volQ = c->volQ;
+            t.volFlag = c->volFlag;
+            t.step = c->step;
+            t.totalWeightAll = 0.0f;
+            for(int s = 0; s < c->nTotal; ++s)
+                t.totalWeightAll += c->weight[s];
+            t.interpolation = c->interpolation;
+            t.skipEmpty = b->cfg.skip_empty >= 0 ? b->cfg.skip_empty : (c->lastEmpty != 0 ? 1 : 0);
+            t.volume = t.totalWeightAll > 0.0f ? 1 : 0;
+            t.renderMode = c->renderMode;
+            t.aoWeight = c->aoWeight;
+            t.bg = make_float4(c->bg[0], c->bg[1], c->bg[2], c->bg[3]);
+            t.bgSwizzled = make_float4(c->bg[3], c->bg[2], c->bg[1], 0.0f);
+            t.scale = make_float3(c->desc.scale[0], c->desc.scale[1], c->desc.scale[2]);
+            t.clipCount = c->clipCount;
+            std::memcpy(t.clipPos, c->clipPos, sizeof(t.clipPos));
+            std::memcpy(t.clipNrm, c->clipNrm, sizeof(t.clipNrm));
+        }
+        int base = 0;
+        for(size_t v = 0; v < b->views.size(); ++v)
+        {
+            const isaacb_view& iv = b->views[v];
+            BatchView& t = b->viewPinned[v];
+            view_inverse(iv.projection, iv.modelview, t.inv);
+            t.W = int32_t(iv.width);
+            t.H = int32_t(iv.height);
+            t.ctx = int32_t(iv.ctx_index);
+            t.tilesX = int32_t((iv.width + b->cfg.tile_w - 1) / b->cfg.tile_w);
+            t.tiles = t.tilesX * int32_t((iv.height + b->cfg.tile_h - 1) / b->cfg.tile_h);
+            t.tileBase = base;
+            t.out = reinterpret_cast<uchar4*>(iv.rgba_dev);
+            base += t.tiles;
+        }
+        b->totalTiles = base;
+        cudaError_t e = cudaMemcpyAsync(b->ctxDev, b->ctxPinned, b->ctxs.size() * sizeof(BatchCtx), cudaMemcpyHostToDevice, st);
+        if(e == cudaSuccess)
+            e = cudaMemcpyAsync(b->viewDev, b->viewPinned, b->views.size() * sizeof(BatchView), cudaMemcpyHostToDevice, st);
+        if(e == cudaSuccess)
+            e = cudaEventRecord(b->tableEvent, st);
+        if(e != cudaSuccess)
+            return batch_fail(ISAACB_CUDA_ERROR, std::string("batch table upload: ") + cudaGetErrorString(e));
+        return ISAACB_OK;
+    }
+
+    int batch_blocks(const isaacb_batch* b)
+    {
+        const int maxb = batch_max_blocks_per_sm();
+        const int per = (b->cfg.blocks_per_sm == 0 || int(b->cfg.blocks_per_sm) > maxb) ? maxb : int(b->cfg.blocks_per_sm);
+        return b->numSMs * per;
+    }
+
+    // the stream work of one batch frame; `capture` leaves out the read-back of the empty-brick counts
+    isaacb_status batch_enqueue(isaacb_batch* b, cudaStream_t st, bool update, bool capture)
+    {
+        if(update)
+        {
+            for(isaacb_ctx* c : b->ctxs)
+            {
+                for(int s = 0; s < c->nVol; ++s)
+                    if(!c->src[s] && (c->weight[s] != 0.0f || c->iso[s] != 0.0f))
+                        return batch_fail(ISAACB_NOT_READY, "isaacb_batch: a source has no memory");
+                MergeParams p{};
+                prepare_merge(c, p);
+                if(capture)
+                    b->graphMerges.push_back(p);
+                if(cudaMemsetAsync(c->emptyDev, 0, sizeof(unsigned int), st) != cudaSuccess)
+                    return batch_fail(ISAACB_CUDA_ERROR, "isaacb_batch: empty brick counter");
+                launch_merge(p, st);
+                if(!capture && cudaEventQuery(c->emptyEvent) != cudaErrorNotReady)
+                {
+                    if(cudaMemcpyAsync(c->emptyPinned, c->emptyDev, sizeof(unsigned int), cudaMemcpyDeviceToHost, st)
+                           != cudaSuccess
+                       || cudaEventRecord(c->emptyEvent, st) != cudaSuccess)
+                        return batch_fail(ISAACB_CUDA_ERROR, "isaacb_batch: empty brick count");
+                }
+            }
+        }
+        if(cudaMemsetAsync(b->counter, 0, sizeof(int32_t), st) != cudaSuccess)
+            return batch_fail(ISAACB_CUDA_ERROR, "isaacb_batch: queue reset");
+        BatchParams bp{};
+        bp.ctxs = b->ctxDev;
+        bp.views = b->viewDev;
+        bp.nViews = int32_t(b->views.size());
+        bp.totalTiles = b->totalTiles;
+        bp.tileW = int32_t(b->cfg.tile_w);
+        bp.tileH = int32_t(b->cfg.tile_h);
+        bp.counter = b->counter;
+        bp.samples = b->counting ? b->samples : nullptr;
+        if(b->counting && cudaMemsetAsync(b->samples, 0, sizeof(unsigned long long), st) != cudaSuccess)
+            return batch_fail(ISAACB_CUDA_ERROR, "isaacb_batch: sample counter reset");
+        launch_batch(bp, batch_blocks(b), st);
+        const cudaError_t e = cudaGetLastError();
+        if(e != cudaSuccess)
+            return batch_fail(ISAACB_CUDA_ERROR, std::string("isaacb_batch launch: ") + cudaGetErrorString(e));
+        return ISAACB_OK;
+    }
+
+    isaacb_status batch_upload_luts(isaacb_batch* b, cudaStream_t st)
+    {
+        for(isaacb_ctx* c : b->ctxs)
+        {
+            const isaacb_status r = upload_lut(c, st);
+            if(r != ISAACB_OK)
+                return batch_fail(r, c->lastError);
+        }
+        return ISAACB_OK;
+    }
+
+    void batch_drop_graph(isaacb_batch* b)
+    {
+        if(b->graphExec)
+            cudaGraphExecDestroy(b->graphExec);
+        if(b->graph)
+            cudaGraphDestroy(b->graph);
+        b->graphExec = nullptr;
+        b->graph = nullptr;
+        b->graphMerges.clear();
+    }
+
+    // true when a context's merge parameters changed since the graph was captured
+    bool batch_graph_stale(const isaacb_batch* b)
+    {
+        if(!b->graphUpdate)
+            return false;
+        for(size_t i = 0; i < b->ctxs.size(); ++i)
+        {
+            MergeParams p{};
+            prepare_merge(b->ctxs[i], p);
+            if(i >= b->graphMerges.size() || std::memcmp(&p, &b->graphMerges[i], sizeof(MergeParams)) != 0)
+                return true;
+        }
+        return false;
+    }
+} // namespace
+
+extern "C"
+{
+    isaacb_status isaacb_batch_create(
+        isaacb_ctx* const* ctxs,
+        uint32_t n_ctx,
+        const isaacb_view* views,
+        uint32_t n_views,
+        isaacb_batch** out)
+    {
+        if(!ctxs || !views || !out || n_ctx == 0 || n_views == 0 || n_ctx > 4096 || n_views > 4096)
+            return batch_fail(ISAACB_INVALID_ARG, "isaacb_batch_create: bad arguments");
+        *out = nullptr;
+        for(uint32_t i = 0; i < n_ctx; ++i)
+        {
+            std::string why;
+            if(!ctxs[i])
+                return batch_fail(ISAACB_INVALID_ARG, "isaacb_batch_create: null context");
+            if(!batchable(ctxs[i], why))
+                return batch_fail(ISAACB_INVALID_ARG, "isaacb_batch_create: context " + std::to_string(i) + ": " + why);
+        }
+        for(uint32_t v = 0; v < n_views; ++v)
+            if(views[v].ctx_index >= n_ctx || views[v].width == 0 || views[v].height == 0 || views[v].width > 16384
+               || views[v].height > 16384 || !views[v].rgba_dev)
+                return batch_fail(ISAACB_INVALID_ARG, "isaacb_batch_create: bad view " + std::to_string(v));
+        isaacb_batch* b = new isaacb_batch;
+        b->ctxs.assign(ctxs, ctxs + n_ctx);
+        b->views.assign(views, views + n_views);
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&b->numSMs, cudaDevAttrMultiProcessorCount, dev);
+        cudaError_t e = cudaMalloc(&b->ctxDev, n_ctx * sizeof(BatchCtx));
+        if(e == cudaSuccess)
+            e = cudaMalloc(&b->viewDev, n_views * sizeof(BatchView));
+        if(e == cudaSuccess)
+            e = cudaMallocHost(&b->ctxPinned, n_ctx * sizeof(BatchCtx));
+        if(e == cudaSuccess)
+            e = cudaMallocHost(&b->viewPinned, n_views * sizeof(BatchView));
+        if(e == cudaSuccess)
+            e = cudaMalloc(&b->counter, sizeof(int32_t));
+        if(e == cudaSuccess)
+            e = cudaMalloc(&b->samples, sizeof(unsigned long long));
+        if(e == cudaSuccess)
+            e = cudaEventCreateWithFlags(&b->tableEvent, cudaEventDisableTiming);
+        if(e != cudaSuccess)
+        {
+            isaacb_batch_destroy(b);
+            return batch_fail(e == cudaErrorMemoryAllocation ? ISAACB_OOM : ISAACB_CUDA_ERROR, "isaacb_batch_create: allocation");
+        }
+        *out = b;
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_batch_destroy(isaacb_batch* b)
+    {
+        if(!b)
+            return ISAACB_OK;
+        batch_drop_graph(b);
+        cudaFree(b->ctxDev);
+        cudaFree(b->viewDev);
+        if(b->ctxPinned)
+            cudaFreeHost(b->ctxPinned);
+        if(b->viewPinned)
+            cudaFreeHost(b->viewPinned);
+        cudaFree(b->counter);
+        cudaFree(b->samples);
+        if(b->tableEvent)
+            cudaEventDestroy(b->tableEvent);
+        delete b;
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_batch_set_config(isaacb_batch* b, const isaacb_batch_config* cfg)
+    {
+        if(!b || !cfg || cfg->tile_w * cfg->tile_h != 256 || cfg->tile_w % 8 != 0 || cfg->tile_h % 4 != 0
+           || cfg->skip_empty < -1 || cfg->skip_empty > 1)
+            return batch_fail(ISAACB_INVALID_ARG, "isaacb_batch_set_config: tiles must be 256 pixels, width % 8, height % 4");
+        b->cfg = *cfg;
+        batch_drop_graph(b);
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_batch_get_config(const isaacb_batch* b, isaacb_batch_config* cfg)
+    {
+        if(!b || !cfg)
+            return ISAACB_INVALID_ARG;
+        *cfg = b->cfg;
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_batch_set_camera(isaacb_batch* b, uint32_t v, const double* proj, const double* mv)
+    {
+        if(!b || v >= b->views.size() || !proj || !mv)
+            return batch_fail(ISAACB_INVALID_ARG, "isaacb_batch_set_camera: bad arguments");
+        std::memcpy(b->views[v].projection, proj, sizeof(double) * 16);
+        std::memcpy(b->views[v].modelview, mv, sizeof(double) * 16);
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_batch_render(isaacb_batch* b, void* stream, int32_t update)
+    {
+        if(!b)
+            return ISAACB_INVALID_ARG;
+        cudaStream_t st = (cudaStream_t) stream;
+        isaacb_status r = batch_upload_luts(b, st);
+        if(r == ISAACB_OK)
+            r = batch_refresh(b, st);
+        if(r == ISAACB_OK)
+            r = batch_enqueue(b, st, update != 0, false);
+        return r;
+    }
+
+    isaacb_status isaacb_batch_capture(isaacb_batch* b, void* stream, int32_t update)
+    {
+        if(!b || !stream)
+            return batch_fail(ISAACB_INVALID_ARG, "isaacb_batch_capture: needs a non-default stream");
+        cudaStream_t st = (cudaStream_t) stream;
+        isaacb_status r = batch_upload_luts(b, st);
+        if(r == ISAACB_OK)
+            r = batch_refresh(b, st);
+        if(r != ISAACB_OK)
+            return r;
+        batch_drop_graph(b);
+        if(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return batch_fail(ISAACB_CUDA_ERROR, "isaacb_batch_capture: begin capture");
+        r = batch_enqueue(b, st, update != 0, true);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(st, &g);
+        if(r != ISAACB_OK || e != cudaSuccess)
+        {
+            if(g)
+                cudaGraphDestroy(g);
+            return r != ISAACB_OK ? r : batch_fail(ISAACB_CUDA_ERROR, "isaacb_batch_capture: end capture");
+        }
+        if(cudaGraphInstantiate(&b->graphExec, g, 0) != cudaSuccess)
+        {
+            cudaGraphDestroy(g);
+            return batch_fail(ISAACB_CUDA_ERROR, "isaacb_batch_capture: instantiate");
+        }
+        b->graph = g;
+        b->graphUpdate = update != 0;
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_batch_launch_graph(isaacb_batch* b, void* stream)
+    {
+        if(!b || !b->graphExec)
+            return batch_fail(ISAACB_NOT_READY, "isaacb_batch_launch_graph: no captured graph");
+        cudaStream_t st = (cudaStream_t) stream;
+        // functors, weights, storage or source memory changed: the merges in the graph are out of date
+        if(batch_graph_stale(b))
+        {
+            const bool update = b->graphUpdate;
+            const isaacb_status rc = isaacb_batch_capture(b, stream, update ? 1 : 0);
+            if(rc != ISAACB_OK)
+                return rc;
+        }
+        // cameras and frame settings live in device tables the graph reads
+        isaacb_status r = batch_upload_luts(b, st);
+        if(r == ISAACB_OK)
+            r = batch_refresh(b, st);
+        if(r != ISAACB_OK)
+            return r;
+        const cudaError_t e = cudaGraphLaunch(b->graphExec, st);
+        if(e != cudaSuccess)
+            return batch_fail(ISAACB_CUDA_ERROR, std::string("isaacb_batch_launch_graph: ") + cudaGetErrorString(e));
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_batch_autotune(isaacb_batch* b, void* stream, isaacb_batch_config* best, float* best_ms)
+    {
+        if(!b)
+            return ISAACB_INVALID_ARG;
+        cudaStream_t st = (cudaStream_t) stream;
+        const uint32_t shapes[4][2] = {{32, 8}, {16, 16}, {8, 32}, {64, 4}};
+        const int maxb = batch_max_blocks_per_sm();
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        isaacb_batch_config keep = b->cfg, bestCfg = b->cfg;
+        float bestT = 3.0e38f;
+        isaacb_status r = ISAACB_OK;
+        for(const auto& sh : shapes)
+            for(int per = 1; per <= maxb && r == ISAACB_OK; per = (per == maxb ? maxb + 1 : std::min(maxb, per * 2)))
+                for(int skip = 0; skip <= 1 && r == ISAACB_OK; ++skip)
+                {
+                    b->cfg = isaacb_batch_config{sh[0], sh[1], uint32_t(per), skip};
+                    r = isaacb_batch_render(b, st, 0); // warm-up
+                    cudaEventRecord(e0, st);
+                    for(int k = 0; k < 3 && r == ISAACB_OK; ++k)
+                        r = isaacb_batch_render(b, st, 0);
+                    cudaEventRecord(e1, st);
+                    cudaEventSynchronize(e1);
+                    float ms = 0.0f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    ms /= 3.0f;
+                    if(r == ISAACB_OK && ms < bestT)
+                    {
+                        bestT = ms;
+                        bestCfg = b->cfg;
+                    }
+                }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        b->cfg = r == ISAACB_OK ? bestCfg : keep;
+        batch_drop_graph(b);
+        if(best)
+            *best = b->cfg;
+        if(best_ms)
+            *best_ms = bestT;
+        return r;
+    }
+
+    isaacb_status isaacb_batch_set_counting(isaacb_batch* b, int32_t on)
+    {
+        if(!b)
+            return ISAACB_INVALID_ARG;
+        b->counting = on != 0;
+        batch_drop_graph(b);
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_batch_get_samples(isaacb_batch* b, void* stream, uint64_t* samples)
+    {
+        if(!b || !samples)
+            return ISAACB_INVALID_ARG;
+        unsigned long long h = 0;
+        cudaStream_t st = (cudaStream_t) stream;
+        if(cudaMemcpyAsync(&h, b->samples, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess
+           || cudaStreamSynchronize(st) != cudaSuccess)
+            return batch_fail(ISAACB_CUDA_ERROR, "isaacb_batch_get_samples");
+        *samples = h;
         return ISAACB_OK;
     }
 }

@@ -28,17 +28,34 @@ namespace isaacb
         return make_float4(1.0f, 0.0f, 0.0f, a);
     }
 
-    __device__ __forceinline__ void shade_pixel(const FrameParams& p, int px, int py, size_t o)
+    // the settings ShadingKernel reads
+    struct ShadeParams
     {
-        float4 color = from_byte4(p.color[o]);
-        const float3 normal = f3(p.normal[3 * o], p.normal[3 * o + 1], p.normal[3 * o + 2]);
-        const float aoStrength = 1.0f - p.ao[o];
-        const int mode = p.renderMode;
+        int32_t renderMode;
+        float aoWeight;
+        float4 bg;
+    };
+
+    // ShadingKernel on one pixel's G-buffer values: colour and depth are updated in place
+    __device__ __forceinline__ void shade_values(
+        const ShadeParams& sp,
+        const View& v,
+        const Geom& g,
+        int px,
+        int py,
+        uchar4& gcolor,
+        float3 normal,
+        float aoRaw,
+        float& depth)
+    {
+        float4 color = from_byte4(gcolor);
+        const float aoStrength = 1.0f - aoRaw;
+        const int mode = sp.renderMode;
         if(mode == 7)
             color = hsva_rank0(color.w);
         if(mode < 3 || mode == 7)
         {
-            const Ray ray = pixel_to_ray(p.v, p.g, px, py);
+            const Ray ray = pixel_to_ray(v, g, px, py);
             const float3 lightDir = neg3(ray.dir);
             float lightFactor = fabsf(dot3(normal, lightDir));
             const float3 halfVector = normalize3(add3(neg3(ray.dir), lightDir));
@@ -48,7 +65,7 @@ namespace isaacb
             specular *= 0.5f;
             if(mode == 1)
                 specular = 0.0f;
-            const float w = p.aoWeight;
+            const float w = sp.aoWeight;
             const float aoFactor = ((1.0f - w) + w * aoStrength);
             lightFactor += aoFactor;
             lightFactor *= 0.5f;
@@ -57,37 +74,46 @@ namespace isaacb
             sh.y = gmin(color.y * lightFactor + specular, 1.0f);
             sh.z = gmin(color.z * lightFactor + specular, 1.0f);
             sh.w = color.w;
-            p.color[o] = to_byte4(sh);
+            gcolor = to_byte4(sh);
             if(mode == 2 || mode == 7)
-                p.depth[o] = 0.0f;
+                depth = 0.0f;
         }
         else if(mode == 3)
         {
-            p.color[o] = to_byte4(make_float4(p.bg.w, p.bg.z, p.bg.y, color.w));
+            gcolor = to_byte4(make_float4(sp.bg.w, sp.bg.z, sp.bg.y, color.w));
         }
         else if(mode == 4)
         {
-            p.color[o] = to_byte4(make_float4(normal.x * 0.5f + 0.5f, normal.y * 0.5f + 0.5f, normal.z * 0.5f + 0.5f, color.w));
-            p.depth[o] = 0.0f;
+            gcolor = to_byte4(make_float4(normal.x * 0.5f + 0.5f, normal.y * 0.5f + 0.5f, normal.z * 0.5f + 0.5f, color.w));
+            depth = 0.0f;
         }
         else if(mode == 5)
         {
-            const float d = p.depth[o] / float(p.g.maxGss);
-            p.color[o] = to_byte4(make_float4(d, d, d, color.w));
-            p.depth[o] = 0.0f;
+            const float d = depth / float(g.maxGss);
+            gcolor = to_byte4(make_float4(d, d, d, color.w));
+            depth = 0.0f;
         }
         else if(mode == 6)
         {
-            const float w = p.aoWeight;
+            const float w = sp.aoWeight;
             const float aoFactor = ((1.0f - w) + w * aoStrength);
-            p.color[o] = to_byte4(make_float4(aoFactor, aoFactor, aoFactor, color.w));
-            p.depth[o] = 0.0f;
+            gcolor = to_byte4(make_float4(aoFactor, aoFactor, aoFactor, color.w));
+            depth = 0.0f;
         }
         else if(mode == 8)
         {
-            p.color[o] = to_byte4(hsva_rank0(1.0f));
-            p.depth[o] = 0.0f;
+            gcolor = to_byte4(hsva_rank0(1.0f));
+            depth = 0.0f;
         }
     }
 
+    __device__ __forceinline__ void shade_pixel(const FrameParams& p, int px, int py, size_t o)
+    {
+        const ShadeParams sp{p.renderMode, p.aoWeight, p.bg};
+        uchar4 c = p.color[o];
+        float d = p.depth[o];
+        shade_values(sp, p.v, p.g, px, py, c, f3(p.normal[3 * o], p.normal[3 * o + 1], p.normal[3 * o + 2]), p.ao[o], d);
+        p.color[o] = c;
+        p.depth[o] = d;
+    }
 } // namespace isaacb

@@ -143,6 +143,51 @@ namespace isaacb
         unsigned long long* counters; // [0] volume samples, [1] iso samples; null = off
     };
 
+    // -------------------------------------------------------------- batched views
+    // one context (e.g. one timestep) of a batch: its texture and frame settings
+    struct BatchCtx
+    {
+        Geom g;
+        const uint4* volQ;
+        const uint8_t* volFlag;
+        float step;
+        float totalWeightAll;
+        int32_t interpolation;
+        int32_t skipEmpty;
+        int32_t volume; // totalWeightAll > 0
+        int32_t renderMode;
+        float aoWeight;
+        float4 bg;
+        float4 bgSwizzled;
+        float3 scale;
+        int32_t clipCount;
+        float clipPos[kMaxClip][3];
+        float clipNrm[kMaxClip][3];
+    };
+    // one view of a batch: camera inverse, size, context and output
+    struct BatchView
+    {
+        float inv[16];
+        int32_t W, H;
+        int32_t ctx;
+        int32_t tilesX;
+        int32_t tileBase;
+        int32_t tiles;
+        uchar4* out;
+    };
+    struct BatchParams
+    {
+        const BatchCtx* ctxs;
+        const BatchView* views;
+        int32_t nViews;
+        int32_t totalTiles;
+        int32_t tileW, tileH; // tileW * tileH == 256, tileW % 8 == 0, tileH % 4 == 0
+        int32_t* counter; // work queue head, zero before the launch
+        unsigned long long* samples; // optional sample counter
+    };
+    void launch_batch(const BatchParams& p, int blocks, cudaStream_t s);
+    int batch_max_blocks_per_sm();
+
     void launch_clear_particles(const FrameParams& p, cudaStream_t s);
     void launch_iso(const FrameParams& p, cudaStream_t s);
     void launch_iso_per_source(const FrameParams& p, cudaStream_t s);

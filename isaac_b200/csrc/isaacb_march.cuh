@@ -1,0 +1,150 @@
+// The combined-texture ray-march shared by the single-view and the batched
+// kernels.  Included by the kernel translation units only.
+#pragma once
+
+#include "isaacb_internal.h"
+
+namespace isaacb
+{
+    // the texture a march reads: geometry, quad bricks and per-brick emptiness
+    struct VolTexRef
+    {
+        Geom g;
+        const uint4* volQ;
+        const uint8_t* volFlag;
+    };
+
+    // Front-to-back march of CombinedVolumeRenderKernel (lib/isaac/isaac_volume_kernel.hpp:61-87)
+    // at the reference's sample positions.  Differences from the exact form, all far
+    // below one output LSB and covered by the parity tests:
+    //  * pos - 0.5 is one fmaf per axis, the trilinear is evaluated as 8 FP32 weights,
+    //    and the /255 normalisation is folded into the per-ray factor;
+    //  * bytes become floats through a byte permute (no conversion pipe);
+    //  * empty-space skipping: a brick whose texels (apron included) are all zero
+    //    yields exactly zero samples, so the samples inside it are counted but not
+    //    evaluated -- adding zero leaves the colour unchanged.
+    // CLAMP keeps every coordinate inside the volume; a LINEAR ray whose first and
+    // last sample lie strictly inside needs no per-sample clamp (positions are affine
+    // in the step index, rounding is far below the 1e-3 margin).
+    template<bool LINEAR, bool CLAMP, bool SKIP>
+    __device__ __forceinline__ float4 march_combined(
+        const VolTexRef& p,
+        const March& m,
+        float factor,
+        unsigned long long& count)
+    {
+        const Geom& g = p.g;
+        const float k = factor / 255.0f;
+        const float off = LINEAR ? 0.5f : 0.0f;
+        const float c0x = m.startU.x - off, c0y = m.startU.y - off, c0z = m.startU.z - off;
+        const float svx = m.stepVec.x, svy = m.stepVec.y, svz = m.stepVec.z;
+        const float lo = LINEAR ? -1.0f : 0.0f;
+        const float hx = float(g.ls[0] - 1), hy = float(g.ls[1] - 1), hz = float(g.ls[2] - 1);
+        const int nb0 = g.nb[0], nb1 = g.nb[1];
+        const uint32_t* __restrict__ q32 = reinterpret_cast<const uint32_t*>(p.volQ);
+        // floor(c) + 1 (the apron-shifted coordinate) straight from the magic-number add
+        const int magic = 0x4B400000 - 1;
+        float4 color = make_float4(0, 0, 0, 0);
+        int curBrick = -1;
+        bool empty = false;
+        const float fs = float(m.startSteps), fe = float(m.endSteps);
+        float fi = fs;
+        while(fi <= fe)
+        {
+            float cx = fmaf(svx, fi, c0x), cy = fmaf(svy, fi, c0y), cz = fmaf(svz, fi, c0z);
+            if(CLAMP)
+            {
+                cx = fminf(fmaxf(cx, lo), hx);
+                cy = fminf(fmaxf(cy, lo), hy);
+                cz = fminf(fmaxf(cz, lo), hz);
+            }
+            const float tx = __fadd_rd(cx, 12582912.0f), ty = __fadd_rd(cy, 12582912.0f),
+                        tz = __fadd_rd(cz, 12582912.0f);
+            const int ax = __float_as_int(tx) - magic, ay = __float_as_int(ty) - magic, az = __float_as_int(tz) - magic;
+            const int brick = ((az >> 3) * nb1 + (ay >> 3)) * nb0 + (ax >> 3);
+            if(SKIP && brick != curBrick)
+            {
+                curBrick = brick;
+                empty = __ldg(p.volFlag + brick) == 0;
+            }
+            if(SKIP && empty)
+            {
+                // last step index whose position stays inside this brick's sample region
+                // [8b-1, 8b+7) per axis, with a 1e-3-step margin against rounding
+                float tEnd = 3.0e38f;
+                const float bl[3] = {float(ax & ~7) - 1.0f, float(ay & ~7) - 1.0f, float(az & ~7) - 1.0f};
+                const float sv[3] = {svx, svy, svz};
+                const float c0[3] = {c0x, c0y, c0z};
+#pragma unroll
+                for(int a = 0; a < 3; ++a)
+                {
+                    if(sv[a] > 0.0f)
+                        tEnd = fminf(tEnd, (bl[a] + 8.0f - c0[a]) / sv[a]);
+                    else if(sv[a] < 0.0f)
+                        tEnd = fminf(tEnd, (bl[a] - c0[a]) / sv[a]);
+                }
+                // margin: 1e-3 steps plus the float rounding of tEnd itself
+                const float last = fminf(fmaxf(floorf(tEnd - (1.0e-3f + 1.0e-6f * fabsf(tEnd))), fi), fe);
+                fi = last + 1.0f;
+                continue;
+            }
+            const uint32_t slot = uint32_t(brick) * uint32_t(kSlotsPerBrick)
+                + uint32_t((ax & 7) | ((ay & 7) << 3) | ((az & 7) << 6));
+            float r0, r1, r2, r3;
+            if(LINEAR)
+            {
+                const uint4 A = __ldg(p.volQ + slot);
+                const uint4 B = __ldg(p.volQ + slot + 64);
+                const float fx = cx - (tx - 12582912.0f), fy = cy - (ty - 12582912.0f), fz = cz - (tz - 12582912.0f);
+                const float gx = 1.0f - fx, gy = 1.0f - fy, gz = 1.0f - fz;
+                const float w00 = gx * gy, w10 = fx * gy, w01 = gx * fy, w11 = fx * fy;
+                const float wt[8] = {w00 * gz, w10 * gz, w01 * gz, w11 * gz, w00 * fz, w10 * fz, w01 * fz, w11 * fz};
+                const uint32_t tap[8] = {A.x, A.y, A.z, A.w, B.x, B.y, B.z, B.w};
+                // (r,g) and (b,a) accumulate as packed FP32 pairs, one FFMA2 each per tap
+                const f2p bias = f2p_make(-8388608.0f, -8388608.0f);
+                f2p rg = f2p_make(0.0f, 0.0f), ba = f2p_make(0.0f, 0.0f);
+#pragma unroll
+                for(int k = 0; k < 8; ++k)
+                {
+                    const f2p wk = f2p_make(wt[k], wt[k]);
+                    rg = f2p_fma(ubyte_pair(tap[k], 0, bias), wk, rg);
+                    ba = f2p_fma(ubyte_pair(tap[k], 2, bias), wk, ba);
+                }
+                f2p_split(rg, r0, r1);
+                f2p_split(ba, r2, r3);
+            }
+            else
+            {
+                const uint32_t w = __ldg(q32 + size_t(slot) * 4);
+                r0 = ubyte_f(w, 0), r1 = ubyte_f(w, 1), r2 = ubyte_f(w, 2), r3 = ubyte_f(w, 3);
+            }
+            const float s = (1.0f - color.w) * k;
+            color.x = fmaf(s, r0, color.x);
+            color.y = fmaf(s, r1, color.y);
+            color.z = fmaf(s, r2, color.z);
+            color.w = fmaf(s, r3, color.w);
+            fi += 1.0f;
+            if(color.w > 0.99f)
+                break;
+        }
+        count += (unsigned long long) (fminf(fi, fe + 1.0f) - fs);
+        return color;
+    }
+
+    // a LINEAR ray needs no clamp if both end samples are inside [-1, L) by a margin
+    __device__ __forceinline__ bool march_in_range(const Geom& g, const March& m)
+    {
+        const float fs = float(m.startSteps), fe = float(m.endSteps);
+        const float c0[3] = {m.startU.x - 0.5f, m.startU.y - 0.5f, m.startU.z - 0.5f};
+        const float sv[3] = {m.stepVec.x, m.stepVec.y, m.stepVec.z};
+        bool ok = true;
+#pragma unroll
+        for(int a = 0; a < 3; ++a)
+        {
+            const float a0 = fmaf(sv[a], fs, c0[a]), a1 = fmaf(sv[a], fe, c0[a]);
+            ok = ok && fminf(a0, a1) >= -0.999f && fmaxf(a0, a1) <= float(g.ls[a]) - 0.001f;
+        }
+        return ok;
+    }
+
+} // namespace isaacb

@@ -60,8 +60,11 @@ def gaussian_scene(n: int, seed: int = 1, device="cpu"):
     return scalar.to(torch.float32).contiguous(), curl.to(torch.float32).contiguous()
 
 
-def spectral_field(n: int, slope: float, seed: int, device="cpu") -> torch.Tensor:
-    """Zero-mean, unit-variance Gaussian random field on n^3 with P(k) ~ k^slope (float32)."""
+def spectral_field(n: int, slope: float, seed: int, device="cpu", shift: float = 0.0) -> torch.Tensor:
+    """Zero-mean, unit-variance Gaussian random field on n^3 with P(k) ~ k^slope (float32).
+
+    ``shift`` advects the periodic field along x (the fastest axis) by that
+    fraction of the box, as a phase shift of every Fourier mode."""
     g = _gen(seed, device)
     noise = torch.randn((n, n, n), generator=g, device=device, dtype=torch.float32)
     f = torch.fft.rfftn(noise)
@@ -70,6 +73,9 @@ def spectral_field(n: int, slope: float, seed: int, device="cpu") -> torch.Tenso
     KX, KY, KZ = torch.meshgrid(kx, kx, kz, indexing="ij")
     k = torch.sqrt(KX * KX + KY * KY + KZ * KZ)
     amp = torch.where(k > 0, k.clamp_min(1e-12) ** (slope / 2.0), torch.zeros_like(k))
+    if shift:
+        # f(x - s) <-> F(k) exp(-2 pi i k s), s in cells along the last axis
+        amp = amp * torch.exp(torch.complex(torch.zeros_like(KZ), -2.0 * math.pi * KZ * (shift * n)))
     field = torch.fft.irfftn(f * amp, s=(n, n, n))
     field = (field - field.mean()) / field.std()
     return field.to(torch.float32).contiguous()
@@ -102,9 +108,26 @@ def density_gradient_scene(n: int, seeds=(2, 3, 4), device="cpu"):
     return dens, E, s, p90
 
 
-def precision_scene(n: int, seeds=(6, 7, 8, 9), slopes=(-5.0 / 3.0, -2.0, -3.0, -11.0 / 3.0), device="cpu"):
-    """Four scalar spectral fields in [0,1]."""
-    return [unit_range(spectral_field(n, s, sd, device)) for sd, s in zip(seeds, slopes)]
+def precision_scene(
+    n: int, seeds=(6, 7, 8, 9), slopes=(-5.0 / 3.0, -2.0, -3.0, -11.0 / 3.0), device="cpu", shift: float = 0.0
+):
+    """Four scalar spectral fields in [0,1] (advected by ``shift`` of the box along x)."""
+    return [unit_range(spectral_field(n, s, sd, device, shift)) for sd, s in zip(seeds, slopes)]
+
+
+# the batching workload: 16 views of uneven resolution over 4 timesteps
+BATCH_RESOLUTIONS = [(256, 256)] * 4 + [(1280, 720)] * 4 + [(1920, 1080)] * 4 + [(2048, 1152)] * 4
+
+
+def batch_views(resolutions=None, timesteps: int = 4, seed0: int = 100, distance: float = 2.5):
+    """(timestep, width, height, projection, modelview) per view: view i shows
+    timestep i mod ``timesteps`` from a seeded camera on the orbit sphere."""
+    res = BATCH_RESOLUTIONS if resolutions is None else resolutions
+    out = []
+    for i, (w, h) in enumerate(res):
+        P, MV = camera(w, h, seed=seed0 + i, distance=distance)
+        out.append((i % timesteps, w, h, P, MV))
+    return out
 
 
 def particles_uniform(count: int, cells, seed: int = 5, device="cpu"):

@@ -830,6 +830,16 @@ namespace orc
             gNormal.assign(size_t(W) * H, V3<T>{0, 0, 0});
         }
 
+        void setFramebuffer(int w, int h)
+        {
+            W = w;
+            H = h;
+            gColor.assign(size_t(W) * H * 4, 0);
+            gDepth.assign(size_t(W) * H, 0);
+            gAo.assign(size_t(W) * H, 0);
+            gNormal.assign(size_t(W) * H, V3<T>{0, 0, 0});
+        }
+
         // updateTransfer (lib/isaac.hpp:1244-1266) on a description map whose
         // insert keeps the first value of a duplicated key.  Entries outside
         // [first key, last key) keep their previous values.
@@ -2090,6 +2100,12 @@ extern "C"
             std::memcpy(c->proj, proj, sizeof(double) * 16);
             std::memcpy(c->mv, mv, sizeof(double) * 16);
         });
+    }
+    // a new framebuffer size (the reference fixes it at construction; this
+    // lets one oracle stand in for views of several sizes of the same scene)
+    void or_set_framebuffer(void* p, int w, int h)
+    {
+        OR_DISPATCH((OrHandle*) p, c->setFramebuffer(w, h));
     }
     void or_update(void* p)
     {

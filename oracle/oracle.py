@@ -46,6 +46,7 @@ SIG = {
     "or_set_dither_mode": (None, [_P, C.c_int]),
     "or_set_background": (None, [_P, _fp]),
     "or_set_camera": (None, [_P, _dp, _dp]),
+    "or_set_framebuffer": (None, [_P, C.c_int, C.c_int]),
     "or_update": (None, [_P]),
     "or_render": (None, [_P, _u8p, C.c_int, C.c_int]),
     "or_minmax": (None, [_P, _fp, _fp]),
@@ -221,6 +222,10 @@ class Oracle:
         p = np.ascontiguousarray(P, dtype=np.float64).reshape(16)
         m = np.ascontiguousarray(MV, dtype=np.float64).reshape(16)
         self.lib.or_set_camera(self.ctx, _ptr(p, _dp), _ptr(m, _dp))
+
+    def set_framebuffer(self, w: int, h: int):
+        self.lib.or_set_framebuffer(self.ctx, int(w), int(h))
+        self.W, self.H = int(w), int(h)
 
     def update(self):
         self.lib.or_update(self.ctx)

@@ -74,3 +74,18 @@ def test_create_rejects_bad_descriptors_without_gpu():
     d.feature_dim[0] = 1
     d.guard_size[0] = 1
     assert lib.isaacb_create(C.byref(d), C.byref(ctx)) == _lib.INVALID_ARG
+
+
+def test_batch_rejects_bad_arguments_without_gpu():
+    lib = _lib.load()
+    out = C.c_void_p()
+    views = (_lib.View * 1)()
+    ctxs = (C.c_void_p * 1)()
+    assert lib.isaacb_batch_create(None, 1, views, 1, C.byref(out)) == _lib.INVALID_ARG
+    assert lib.isaacb_batch_create(ctxs, 0, views, 1, C.byref(out)) == _lib.INVALID_ARG
+    assert lib.isaacb_batch_create(ctxs, 1, views, 1, C.byref(out)) == _lib.INVALID_ARG  # null context
+    assert b"null context" in lib.isaacb_last_error(None)
+    assert lib.isaacb_batch_destroy(None) == _lib.OK
+    assert lib.isaacb_batch_render(None, None, 0) == _lib.INVALID_ARG
+    assert lib.isaacb_batch_launch_graph(None, None) == _lib.NOT_READY
+    assert lib.isaacb_batch_set_config(None, None) == _lib.INVALID_ARG
