@@ -270,8 +270,10 @@ isaacb_status isaacb_batch_set_camera(isaacb_batch* batch, uint32_t view, const 
 isaacb_status isaacb_batch_render(isaacb_batch* batch, void* stream, int32_t update);
 /* Capture the same work (merges when `update`, queue reset, persistent launch)
  * into a CUDA graph; isaacb_batch_launch_graph replays it.  `stream` must not be
- * the legacy default stream.  Transfer tables, weights and cameras are read at
- * capture time for the merges and at launch time for the views. */
+ * the legacy default stream.  Cameras, transfer tables and shading settings
+ * are read at every launch; when a context's merge inputs (functors, weights,
+ * storage, source memory) changed since the capture, the next launch
+ * recaptures. */
 isaacb_status isaacb_batch_capture(isaacb_batch* batch, void* stream, int32_t update);
 isaacb_status isaacb_batch_launch_graph(isaacb_batch* batch, void* stream);
 /* Time every tile shape x occupancy x skipping candidate on the current views
@@ -281,6 +283,87 @@ isaacb_status isaacb_batch_autotune(isaacb_batch* batch, void* stream, isaacb_ba
 /* Ray-march loop trips of the last batch render (counting costs one atomic per warp). */
 isaacb_status isaacb_batch_set_counting(isaacb_batch* batch, int32_t enabled);
 isaacb_status isaacb_batch_get_samples(isaacb_batch* batch, void* stream, uint64_t* samples);
+
+/* ---- Tensor-core convolution (no counterpart in the reference): the
+ * building block of the learned frame reconstructor, exposed for testing.
+ * Tensors are NHWC bf16 in device memory, channel counts multiples of 8.
+ *
+ * isaacb_conv_forward computes y[p][co] = sum_{tap,ci} x[in(p,tap)][ci] * w[co][tap*c_in+ci]
+ * over the out_h x out_w grid, with in(p,tap) = p*stride - pad + tap per axis
+ * (zero outside the in_h x in_w input), or, with `transposed`,
+ * in(p,tap) = (p + pad - tap) / stride where that divides exactly (the
+ * input-gradient form).  `w` is bf16 [roundup(c_out,16)][roundup(ksize^2*c_in,64)],
+ * zero padded.  Epilogue, in order: + bias[co] (optional), ReLU (`relu`),
+ * * (mask > 0) with `mask` NHWC like y (optional), + the existing output
+ * (`accumulate`); stored as bf16 `y`, or FP32 `y_f32` when that is set.
+ *
+ * isaacb_conv_wgrad adds sum_p x[in(p,tap)][ci] * dy[p][co] into the FP32
+ * matrix dw[(tap*c_in+ci)][roundup(c_out,16)] (forward gather form).
+ *
+ * `error_flag` (optional, device int) is set when a bounded wait inside the
+ * kernel gave up.  Asynchronous on `stream`; errors via isaacb_last_error(NULL). */
+typedef struct isaacb_conv_args
+{
+    const void* x;
+    const void* w;
+    const float* bias;
+    void* y;
+    float* y_f32;
+    const void* mask;
+    const void* dy;
+    float* dw;
+    int32_t* error_flag;
+    uint32_t batch, in_h, in_w, c_in;
+    uint32_t out_h, out_w, c_out;
+    uint32_t ksize, stride, pad;
+    int32_t transposed, relu, accumulate;
+} isaacb_conv_args;
+
+isaacb_status isaacb_conv_forward(const isaacb_conv_args* args, void* stream);
+isaacb_status isaacb_conv_wgrad(const isaacb_conv_args* args, void* stream);
+
+/* ---- Learned frame reconstructor (no counterpart in the reference).  A
+ * 4-level convolutional U-Net (32/64/96/128 channels, 216,464 parameters, bf16
+ * weights, FP32 accumulation on the tensor cores) rebuilds a full-size RGBA8
+ * frame from a half-size render: frame = bilinear x2 of the half-size frame
+ * + the network's residual.  Frames are RGBA8 rows, row 0 = bottom, in device
+ * memory.  Training and inference run on the GPU in the library's own
+ * forward and backward kernels. */
+typedef struct isaacb_recon isaacb_recon;
+
+uint32_t isaacb_recon_param_count(void);
+/* Buffers for up to `max_batch` half-size inputs of max_h x max_w; weights
+ * He-initialised from `seed`. */
+isaacb_status isaacb_recon_create(uint32_t max_batch, uint32_t max_h, uint32_t max_w, uint64_t seed, isaacb_recon** out);
+isaacb_status isaacb_recon_destroy(isaacb_recon* recon);
+/* FP32 parameters, per layer the weights [c_out][ky][kx][c_in] then the bias. */
+isaacb_status isaacb_recon_get_params(isaacb_recon* recon, float* host);
+isaacb_status isaacb_recon_set_params(isaacb_recon* recon, const float* host);
+/* One optimiser step on `batch` pairs: half-size frames low[index[b]]
+ * (h x w) against full-size targets high[index[b]] (2h x 2w); index may be
+ * NULL for 0..batch-1.  The mean squared error (RGBA in [0,1]) is written to
+ * loss_dev when it is set.  With grads_host set, the step computes the
+ * gradient, copies it there (layout of the parameters) and does NOT update. */
+isaacb_status isaacb_recon_train_step(
+    isaacb_recon* recon,
+    const uint8_t* low,
+    const uint8_t* high,
+    const int32_t* index,
+    uint32_t batch,
+    uint32_t h,
+    uint32_t w,
+    float learning_rate,
+    float* loss_dev,
+    float* grads_host,
+    void* stream);
+/* One full-size frame (2h x 2w) from one half-size frame (h x w). */
+isaacb_status isaacb_recon_infer(isaacb_recon* recon, const uint8_t* low, uint32_t h, uint32_t w, uint8_t* out, void* stream);
+/* Reads and clears the flag the kernels raise when a bounded wait gave up. */
+isaacb_status isaacb_recon_error(isaacb_recon* recon, int32_t* flag);
+/* The method without the network: bilinear x2 alone (2h x 2w RGBA8). */
+isaacb_status isaacb_upsample_bilinear2(const uint8_t* low, uint32_t h, uint32_t w, uint8_t* out, void* stream);
+/* Adds the sum of squared byte differences of two RGBA8 images to *sum_dev. */
+isaacb_status isaacb_image_sq_error(const uint8_t* a, const uint8_t* b, uint64_t bytes, unsigned long long* sum_dev, void* stream);
 
 /* Number of kernels the last isaacb_update / isaacb_render enqueued. */
 isaacb_status isaacb_get_launch_count(isaacb_ctx* ctx, uint32_t* update_launches, uint32_t* render_launches);

@@ -76,6 +76,35 @@ class BatchConfig(C.Structure):
     ]
 
 
+class ConvArgs(C.Structure):
+    """``isaacb_conv_args``: one tensor-core convolution (forward, input- or weight-gradient)."""
+
+    _fields_ = [
+        ("x", C.c_void_p),
+        ("w", C.c_void_p),
+        ("bias", C.c_void_p),
+        ("y", C.c_void_p),
+        ("y_f32", C.c_void_p),
+        ("mask", C.c_void_p),
+        ("dy", C.c_void_p),
+        ("dw", C.c_void_p),
+        ("error_flag", C.c_void_p),
+        ("batch", C.c_uint32),
+        ("in_h", C.c_uint32),
+        ("in_w", C.c_uint32),
+        ("c_in", C.c_uint32),
+        ("out_h", C.c_uint32),
+        ("out_w", C.c_uint32),
+        ("c_out", C.c_uint32),
+        ("ksize", C.c_uint32),
+        ("stride", C.c_uint32),
+        ("pad", C.c_uint32),
+        ("transposed", C.c_int32),
+        ("relu", C.c_int32),
+        ("accumulate", C.c_int32),
+    ]
+
+
 class IsaacError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
@@ -142,6 +171,18 @@ SIGNATURES = {
     "isaacb_batch_autotune": (_i32, [_P, _P, C.POINTER(BatchConfig), _fp]),
     "isaacb_batch_set_counting": (_i32, [_P, _i32]),
     "isaacb_batch_get_samples": (_i32, [_P, _P, _u64p]),
+    "isaacb_conv_forward": (_i32, [C.POINTER(ConvArgs), _P]),
+    "isaacb_conv_wgrad": (_i32, [C.POINTER(ConvArgs), _P]),
+    "isaacb_recon_param_count": (_u32, []),
+    "isaacb_recon_create": (_i32, [_u32, _u32, _u32, C.c_uint64, C.POINTER(_P)]),
+    "isaacb_recon_destroy": (_i32, [_P]),
+    "isaacb_recon_get_params": (_i32, [_P, _fp]),
+    "isaacb_recon_set_params": (_i32, [_P, _fp]),
+    "isaacb_recon_train_step": (_i32, [_P, _P, _P, _P, _u32, _u32, _u32, _f, _P, _P, _P]),
+    "isaacb_recon_infer": (_i32, [_P, _P, _u32, _u32, _P, _P]),
+    "isaacb_recon_error": (_i32, [_P, _i32p]),
+    "isaacb_upsample_bilinear2": (_i32, [_P, _u32, _u32, _P, _P]),
+    "isaacb_image_sq_error": (_i32, [_P, _P, C.c_uint64, _P, _P]),
 }
 
 

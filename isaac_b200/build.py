@@ -42,6 +42,8 @@ SOURCES = [
     "kernels_legacy.cu",
     "minmax_static.cu",
     "kernels_batch.cu",
+    "recon_gemm.cu",
+    "recon.cu",
 ]
 
 

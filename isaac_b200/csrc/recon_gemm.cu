@@ -1,0 +1,662 @@
+// Convolutions as implicit GEMMs on the sm_100a tensor cores (tcgen05).
+//
+// Forward and input-gradient ("dgrad") passes share k_conv_gemm:
+//   Y[p][n] = sum_k A[p][k] * Wp[n][k],  k = tap * Cg + c,
+// where A is the im2col gather of the NHWC bf16 source (never materialised:
+// each CTA gathers its 128-row x 64-column K-slices straight into shared
+// memory with zero-filling cp.async), Wp is the packed bf16 weight matrix
+// held whole in shared memory, and the FP32 accumulator lives in TMEM.  One
+// thread issues the MMAs (M=128, N=Npad, K=16 per instruction) and commits
+// them to per-stage mbarriers that recycle the shared-memory stages; the
+// epilogue reads TMEM with tcgen05.ld and fuses bias, ReLU, the ReLU mask of
+// the backward pass, accumulation into an existing gradient and the bf16 or
+// FP32 store.  The gather has two forms:
+//   forward     input pixel = out * stride - pad + tap
+//   transposed  input pixel = (out + pad - tap) / stride when divisible
+// The transposed form with the per-tap transposed weights is the gradient
+// of the forward form with respect to its input.
+//
+// The weight gradient ("wgrad") is k_conv_wgrad:
+//   dW[(tap, ci)][co] = sum_p X[in(p, tap)][ci] * dY[p][co]
+// with both operands MN-major (channels contiguous in NHWC), the pixel axis
+// as the reduction split over CTAs, and FP32 partial sums added atomically.
+//
+// Every mbarrier wait is bounded; on a timeout the kernel raises the error
+// flag, stops issuing work, waits (bounded) for its MMAs and frees its TMEM.
+#include "../../include/isaac_b200.h"
+#include "isaacb_internal.h"
+#include "isaacb_conv.h"
+#include "isaacb_tc.cuh"
+
+#include <cuda_bf16.h>
+#include <string>
+
+namespace isaacb
+{
+    void set_global_error(const std::string& msg);
+
+    namespace
+    {
+        using bf16 = __nv_bfloat16;
+        constexpr int kThreads = 256;
+        constexpr int kStages = 4;
+        constexpr int kTileM = 128;
+        constexpr int kChunkK = 64; // K elements per pipeline stage
+        constexpr int kStageBytesA = kTileM * kChunkK * 2; // 16 KiB
+
+        __host__ __device__ inline uint32_t tmem_columns(int n)
+        {
+            uint32_t c = 32;
+            while(c < uint32_t(n))
+                c <<= 1;
+            return c;
+        }
+
+        __device__ __forceinline__ void raise_error(int* flag, bool& abortLocal)
+        {
+            abortLocal = true;
+            if(flag)
+                atomicExch(flag, 1);
+        }
+
+        __device__ __forceinline__ uint4 pack_bf16x8(const float (&v)[8])
+        {
+            uint4 o;
+            __nv_bfloat162 h;
+            h = __floats2bfloat162_rn(v[0], v[1]);
+            o.x = *reinterpret_cast<uint32_t*>(&h);
+            h = __floats2bfloat162_rn(v[2], v[3]);
+            o.y = *reinterpret_cast<uint32_t*>(&h);
+            h = __floats2bfloat162_rn(v[4], v[5]);
+            o.z = *reinterpret_cast<uint32_t*>(&h);
+            h = __floats2bfloat162_rn(v[6], v[7]);
+            o.w = *reinterpret_cast<uint32_t*>(&h);
+            return o;
+        }
+        __device__ __forceinline__ void unpack_bf16x8(uint4 u, float (&v)[8])
+        {
+            const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+            for(int i = 0; i < 4; ++i)
+            {
+                v[2 * i] = __uint_as_float(w[i] << 16);
+                v[2 * i + 1] = __uint_as_float(w[i] & 0xFFFF0000u);
+            }
+        }
+
+        // ------------------------------------------------------------------ forward / dgrad
+        __global__ void __launch_bounds__(kThreads, 1) k_conv_gemm(const __grid_constant__ ConvGemmParams p)
+        {
+            extern __shared__ unsigned char dsm[];
+            __shared__ uint32_t sTmem;
+            __shared__ __align__(8) uint64_t sEmpty[kStages];
+            __shared__ __align__(8) uint64_t sDone;
+            unsigned char* base = dsm + ((128u - (tc::smem_addr(dsm) & 127u)) & 127u);
+            const uint32_t sB = tc::smem_addr(base);
+            const uint32_t sA = sB + uint32_t(p.Npad) * uint32_t(p.Kpad) * 2u;
+            const int tid = threadIdx.x;
+            const uint32_t cols = tmem_columns(p.Npad);
+            if(tid < 32)
+            {
+                tc::tmem_alloc(&sTmem, cols);
+                tc::tmem_relinquish();
+            }
+            if(tid == 0)
+            {
+                for(int s = 0; s < kStages; ++s)
+                    tc::mbar_init(&sEmpty[s], 1);
+                tc::mbar_init(&sDone, 1);
+                tc::mbar_init_fence();
+            }
+            bool abortLocal = false, aborted = false;
+            // the whole packed weight matrix, canonical K-major: core (n/8, k/8) at (n/8)*Kpad*16 + (k/8)*128
+            {
+                const int kb = p.Kpad / 8;
+                const int pieces = p.Npad * kb;
+                for(int i = tid; i < pieces; i += kThreads)
+                {
+                    const int n = i / kb, k8 = i - n * kb;
+                    const uint32_t dst = sB + uint32_t(n >> 3) * uint32_t(p.Kpad) * 16u + uint32_t(k8) * 128u + uint32_t(n & 7) * 16u;
+                    tc::cp_async16(dst, p.w + size_t(n) * p.Kpad + size_t(k8) * 8, 16);
+                }
+                tc::cp_async_commit();
+                tc::cp_async_wait<0>();
+                tc::fence_async_smem();
+            }
+            tc::fence_before_sync();
+            __syncthreads();
+            tc::fence_after_sync();
+            const uint32_t tmem = sTmem;
+
+            const int P = p.B * p.Ho * p.Wo;
+            const int nTiles = (P + kTileM - 1) / kTileM;
+            const int nk = p.Kpad / kChunkK;
+            const int taps = p.ks * p.ks;
+            const int m = tid & (kTileM - 1);
+            const int jBase = tid >> 7;
+            const uint32_t idesc = tc::idesc_bf16(kTileM, p.Npad, false, false);
+            const uint32_t sboB = uint32_t(p.Kpad) * 16u;
+            uint32_t G0 = 0;
+            uint32_t donePhase = 0;
+
+            for(int tile = blockIdx.x; tile < nTiles; tile += gridDim.x)
+            {
+                const int pix = tile * kTileM + m;
+                const bool valid = pix < P;
+                int b = 0, oy = 0, ox = 0;
+                if(valid)
+                {
+                    ox = pix % p.Wo;
+                    const int t = pix / p.Wo;
+                    oy = t % p.Ho;
+                    b = t / p.Ho;
+                }
+                auto load_chunk = [&](int kc, uint32_t G) {
+                    const uint32_t stage = sA + (G % kStages) * uint32_t(kStageBytesA);
+#pragma unroll
+                    for(int q = 0; q < 4; ++q)
+                    {
+                        const int j = jBase + 2 * q;
+                        const int k = kc * kChunkK + j * 8;
+                        const int t = k / p.Cg;
+                        const int c = k - t * p.Cg;
+                        const bf16* src = p.x;
+                        uint32_t bytes = 0;
+                        if(valid && t < taps)
+                        {
+                            const int ty = t / p.ks, tx = t - ty * p.ks;
+                            int iy, ix;
+                            bool ok;
+                            if(!p.transposed)
+                            {
+                                iy = oy * p.stride - p.pad + ty;
+                                ix = ox * p.stride - p.pad + tx;
+                                ok = iy >= 0 && ix >= 0 && iy < p.H && ix < p.W;
+                            }
+                            else
+                            {
+                                const int ny = oy + p.pad - ty, nx = ox + p.pad - tx;
+                                ok = ny >= 0 && nx >= 0 && (ny % p.stride) == 0 && (nx % p.stride) == 0;
+                                iy = ny / p.stride;
+                                ix = nx / p.stride;
+                                ok = ok && iy < p.H && ix < p.W;
+                            }
+                            if(ok)
+                            {
+                                src = p.x + ((size_t(b) * p.H + iy) * p.W + ix) * p.Cg + c;
+                                bytes = 16;
+                            }
+                        }
+                        const uint32_t dst = stage + uint32_t(m >> 3) * 1024u + uint32_t(j) * 128u + uint32_t(m & 7) * 16u;
+                        tc::cp_async16(dst, src, bytes);
+                    }
+                };
+
+                for(int c = 0; c < kStages - 1; ++c)
+                {
+                    if(c < nk)
+                    {
+                        const uint32_t G = G0 + c;
+                        if(G >= kStages && !tc::mbar_wait(&sEmpty[G % kStages], ((G / kStages) - 1) & 1))
+                            raise_error(p.errorFlag, abortLocal);
+                        load_chunk(c, G);
+                    }
+                    tc::cp_async_commit();
+                }
+                for(int kc = 0; kc < nk; ++kc)
+                {
+                    const int kn = kc + kStages - 1;
+                    if(kn < nk)
+                    {
+                        const uint32_t G = G0 + kn;
+                        if(G >= kStages && !tc::mbar_wait(&sEmpty[G % kStages], ((G / kStages) - 1) & 1))
+                            raise_error(p.errorFlag, abortLocal);
+                        load_chunk(kn, G);
+                    }
+                    tc::cp_async_commit();
+                    tc::cp_async_wait<kStages - 1>();
+                    tc::fence_async_smem();
+                    if(__syncthreads_or(abortLocal))
+                    {
+                        aborted = true;
+                        break;
+                    }
+                    if(tid == 0)
+                    {
+                        tc::fence_after_sync();
+                        const uint32_t G = G0 + kc;
+                        const uint32_t stage = sA + (G % kStages) * uint32_t(kStageBytesA);
+#pragma unroll
+                        for(int j = 0; j < kChunkK / 16; ++j)
+                        {
+                            const uint64_t ad = tc::smem_desc(stage + uint32_t(j) * 256u, 128u, 1024u);
+                            const uint64_t bd = tc::smem_desc(sB + uint32_t(kc * 8 + 2 * j) * 128u, 128u, sboB);
+                            tc::mma_bf16(tmem, ad, bd, idesc, (kc | j) != 0 ? 1u : 0u);
+                        }
+                        tc::mma_commit(&sEmpty[G % kStages]);
+                    }
+                }
+                tc::cp_async_wait<0>();
+                if(tid == 0)
+                    tc::mma_commit(&sDone);
+                if(!tc::mbar_wait(&sDone, donePhase))
+                    raise_error(p.errorFlag, abortLocal);
+                donePhase ^= 1u;
+                G0 += uint32_t(nk);
+                if(__syncthreads_or(abortLocal))
+                {
+                    aborted = true;
+                    break;
+                }
+                tc::fence_after_sync();
+
+                // epilogue: thread = TMEM lane = tile row; the two warpgroups split the columns
+                {
+                    const int warp = tid >> 5;
+                    const uint32_t lane0 = uint32_t(warp & 3) * 32u;
+                    const int half = warp >> 2;
+                    const int cpw = p.Npad / 2;
+                    for(int c0 = half * cpw; c0 < (half + 1) * cpw; c0 += 8)
+                    {
+                        float v[8];
+                        tc::tmem_ld8(tmem + (lane0 << 16) + uint32_t(c0), v);
+                        tc::tmem_wait_ld();
+                        if(!valid || c0 >= p.Cout)
+                            continue;
+                        const size_t o = size_t(pix) * p.Cout + c0;
+                        if(p.bias)
+                        {
+#pragma unroll
+                            for(int i = 0; i < 8; ++i)
+                                v[i] += __ldg(p.bias + c0 + i);
+                        }
+                        if(p.relu)
+                        {
+#pragma unroll
+                            for(int i = 0; i < 8; ++i)
+                                v[i] = fmaxf(v[i], 0.0f);
+                        }
+                        if(p.mask)
+                        {
+                            float mk[8];
+                            unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(p.mask + o)), mk);
+#pragma unroll
+                            for(int i = 0; i < 8; ++i)
+                                v[i] = mk[i] > 0.0f ? v[i] : 0.0f;
+                        }
+                        if(p.yf)
+                        {
+                            float4* dst = reinterpret_cast<float4*>(p.yf + o);
+                            if(p.accumulate)
+                            {
+                                const float4 a = dst[0], bq = dst[1];
+                                v[0] += a.x, v[1] += a.y, v[2] += a.z, v[3] += a.w;
+                                v[4] += bq.x, v[5] += bq.y, v[6] += bq.z, v[7] += bq.w;
+                            }
+                            dst[0] = make_float4(v[0], v[1], v[2], v[3]);
+                            dst[1] = make_float4(v[4], v[5], v[6], v[7]);
+                        }
+                        else
+                        {
+                            uint4* dst = reinterpret_cast<uint4*>(p.y + o);
+                            if(p.accumulate)
+                            {
+                                float a[8];
+                                unpack_bf16x8(*dst, a);
+#pragma unroll
+                                for(int i = 0; i < 8; ++i)
+                                    v[i] += a[i];
+                            }
+                            *dst = pack_bf16x8(v);
+                        }
+                    }
+                }
+                tc::fence_before_sync();
+                __syncthreads();
+            }
+            // drain: every MMA this CTA issued has completed before TMEM is released
+            if(aborted)
+            {
+                if(tid == 0)
+                    tc::mma_commit(&sDone);
+                tc::mbar_wait(&sDone, donePhase);
+            }
+            tc::fence_before_sync();
+            __syncthreads();
+            if(tid < 32)
+                tc::tmem_dealloc(tmem, cols);
+        }
+
+        // ------------------------------------------------------------------ weight gradient
+        __global__ void __launch_bounds__(kThreads, 1) k_conv_wgrad(const __grid_constant__ WgradParams p)
+        {
+            extern __shared__ unsigned char dsm[];
+            __shared__ uint32_t sTmem;
+            __shared__ __align__(8) uint64_t sEmpty[kStages];
+            __shared__ __align__(8) uint64_t sDone;
+            unsigned char* base = dsm + ((128u - (tc::smem_addr(dsm) & 127u)) & 127u);
+            const uint32_t stageB = uint32_t(p.Npad) * 128u; // Npad/8 core rows x 8 pixel blocks x 128 B
+            const uint32_t stageBytes = uint32_t(kStageBytesA) + stageB;
+            const uint32_t s0 = tc::smem_addr(base);
+            const int tid = threadIdx.x;
+            const uint32_t cols = tmem_columns(p.Npad);
+            if(tid < 32)
+            {
+                tc::tmem_alloc(&sTmem, cols);
+                tc::tmem_relinquish();
+            }
+            if(tid == 0)
+            {
+                for(int s = 0; s < kStages; ++s)
+                    tc::mbar_init(&sEmpty[s], 1);
+                tc::mbar_init(&sDone, 1);
+                tc::mbar_init_fence();
+            }
+            bool abortLocal = false, aborted = false;
+            tc::fence_before_sync();
+            __syncthreads();
+            tc::fence_after_sync();
+            const uint32_t tmem = sTmem;
+
+            const int P = p.B * p.Ho * p.Wo;
+            const int nChunks = (P + kChunkK - 1) / kChunkK;
+            const int c0 = blockIdx.y * p.chunksPerSplit;
+            const int c1 = min(nChunks, c0 + p.chunksPerSplit);
+            const int nk = c1 - c0;
+            const int mTile = blockIdx.x;
+            const uint32_t idesc = tc::idesc_bf16(kTileM, p.Npad, true, true);
+            const int bPieces = (p.Npad / 8) * kChunkK;
+
+            auto load_chunk = [&](int kc, uint32_t G) {
+                const uint32_t stA = s0 + (G % kStages) * stageBytes;
+                const uint32_t stB = stA + uint32_t(kStageBytesA);
+                // A: 16 row blocks (8 channels of one tap) x 64 pixels
+#pragma unroll
+                for(int q = 0; q < 4; ++q)
+                {
+                    const int id = q * kThreads + tid;
+                    const int px = id & (kChunkK - 1), mb = id >> 6;
+                    const int r0 = mTile * kTileM + mb * 8;
+                    const int pix = kc * kChunkK + px;
+                    const bf16* src = p.x;
+                    uint32_t bytes = 0;
+                    if(r0 < p.Mtot && pix < P)
+                    {
+                        const int t = r0 / p.Cin, c = r0 - t * p.Cin;
+                        const int ty = t / p.ks, tx = t - ty * p.ks;
+                        const int ox = pix % p.Wo, tt = pix / p.Wo;
+                        const int oy = tt % p.Ho, b = tt / p.Ho;
+                        const int iy = oy * p.stride - p.pad + ty, ix = ox * p.stride - p.pad + tx;
+                        if(iy >= 0 && ix >= 0 && iy < p.H && ix < p.W)
+                        {
+                            src = p.x + ((size_t(b) * p.H + iy) * p.W + ix) * p.Cin + c;
+                            bytes = 16;
+                        }
+                    }
+                    tc::cp_async16(stA + uint32_t(mb) * 1024u + uint32_t(px >> 3) * 128u + uint32_t(px & 7) * 16u, src, bytes);
+                }
+                // B: Npad/8 column blocks x 64 pixels of dY
+                for(int id = tid; id < bPieces; id += kThreads)
+                {
+                    const int px = id & (kChunkK - 1), nb = id >> 6;
+                    const int pix = kc * kChunkK + px;
+                    const bf16* src = p.dy;
+                    uint32_t bytes = 0;
+                    if(pix < P && nb * 8 < p.Cout)
+                    {
+                        src = p.dy + size_t(pix) * p.Cout + nb * 8;
+                        bytes = 16;
+                    }
+                    tc::cp_async16(stB + uint32_t(nb) * 1024u + uint32_t(px >> 3) * 128u + uint32_t(px & 7) * 16u, src, bytes);
+                }
+            };
+
+            for(int c = 0; c < kStages - 1; ++c)
+            {
+                if(c < nk)
+                    load_chunk(c0 + c, uint32_t(c));
+                tc::cp_async_commit();
+            }
+            for(int kc = 0; kc < nk; ++kc)
+            {
+                const int kn = kc + kStages - 1;
+                if(kn < nk)
+                {
+                    const uint32_t G = uint32_t(kn);
+                    if(G >= kStages && !tc::mbar_wait(&sEmpty[G % kStages], ((G / kStages) - 1) & 1))
+                        raise_error(p.errorFlag, abortLocal);
+                    load_chunk(c0 + kn, G);
+                }
+                tc::cp_async_commit();
+                tc::cp_async_wait<kStages - 1>();
+                tc::fence_async_smem();
+                if(__syncthreads_or(abortLocal))
+                {
+                    aborted = true;
+                    break;
+                }
+                if(tid == 0)
+                {
+                    tc::fence_after_sync();
+                    const uint32_t stA = s0 + (uint32_t(kc) % kStages) * stageBytes;
+                    const uint32_t stB = stA + uint32_t(kStageBytesA);
+#pragma unroll
+                    for(int j = 0; j < kChunkK / 16; ++j)
+                    {
+                        const uint64_t ad = tc::smem_desc(stA + uint32_t(j) * 256u, 128u, 1024u);
+                        const uint64_t bd = tc::smem_desc(stB + uint32_t(j) * 256u, 128u, 1024u);
+                        tc::mma_bf16(tmem, ad, bd, idesc, (kc | j) != 0 ? 1u : 0u);
+                    }
+                    tc::mma_commit(&sEmpty[uint32_t(kc) % kStages]);
+                }
+            }
+            tc::cp_async_wait<0>();
+            if(tid == 0)
+                tc::mma_commit(&sDone);
+            if(!aborted && !tc::mbar_wait(&sDone, 0))
+                raise_error(p.errorFlag, abortLocal);
+            aborted = __syncthreads_or(abortLocal) != 0;
+            tc::fence_after_sync();
+            if(aborted)
+            {
+                // one more bounded wait: the MMAs must be done before TMEM is released
+                if(tid == 0)
+                    tc::mma_commit(&sDone);
+                tc::mbar_wait(&sDone, 1);
+            }
+            else if(nk > 0)
+            {
+                const int warp = tid >> 5;
+                const uint32_t lane0 = uint32_t(warp & 3) * 32u;
+                const int half = warp >> 2;
+                const int cpw = p.Npad / 2;
+                const int row = mTile * kTileM + (tid & (kTileM - 1));
+                for(int cc = half * cpw; cc < (half + 1) * cpw; cc += 8)
+                {
+                    float v[8];
+                    tc::tmem_ld8(tmem + (lane0 << 16) + uint32_t(cc), v);
+                    tc::tmem_wait_ld();
+                    if(row >= p.Mtot)
+                        continue;
+#pragma unroll
+                    for(int i = 0; i < 8; ++i)
+                        if(cc + i < p.Cout)
+                            atomicAdd(p.dw + size_t(row) * p.Npad + cc + i, v[i]);
+                }
+            }
+            tc::fence_before_sync();
+            __syncthreads();
+            if(tid < 32)
+                tc::tmem_dealloc(tmem, cols);
+        }
+
+        int num_sms()
+        {
+            static int n = 0;
+            if(n == 0)
+            {
+                int dev = 0;
+                cudaGetDevice(&dev);
+                cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+                if(n <= 0)
+                    n = 148;
+            }
+            return n;
+        }
+    } // namespace
+
+    size_t conv_gemm_smem(int Npad, int Kpad)
+    {
+        return size_t(Npad) * Kpad * 2 + size_t(kStages) * kStageBytesA + 128;
+    }
+    size_t conv_wgrad_smem(int Npad)
+    {
+        return size_t(kStages) * (kStageBytesA + size_t(Npad) * 128) + 128;
+    }
+
+    bool launch_conv_gemm(const ConvGemmParams& p, cudaStream_t s)
+    {
+        const size_t smem = conv_gemm_smem(p.Npad, p.Kpad);
+        if(smem > 227 * 1024)
+            return false;
+        cudaFuncSetAttribute(k_conv_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        const int P = p.B * p.Ho * p.Wo;
+        const int tiles = (P + kTileM - 1) / kTileM;
+        const int grid = tiles < num_sms() ? tiles : num_sms();
+        k_conv_gemm<<<grid, kThreads, smem, s>>>(p);
+        return true;
+    }
+
+    bool launch_conv_wgrad(WgradParams p, cudaStream_t s)
+    {
+        const size_t smem = conv_wgrad_smem(p.Npad);
+        if(smem > 227 * 1024)
+            return false;
+        cudaFuncSetAttribute(k_conv_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        const int P = p.B * p.Ho * p.Wo;
+        const int nChunks = (P + kChunkK - 1) / kChunkK;
+        const int mTiles = (p.Mtot + kTileM - 1) / kTileM;
+        // about two CTAs' worth of work per SM in total, at least 4 chunks each
+        int splits = (2 * num_sms() + mTiles - 1) / mTiles;
+        int per = (nChunks + splits - 1) / splits;
+        if(per < 4)
+            per = 4;
+        splits = (nChunks + per - 1) / per;
+        p.chunksPerSplit = per;
+        dim3 grid(mTiles, splits);
+        k_conv_wgrad<<<grid, kThreads, smem, s>>>(p);
+        return true;
+    }
+} // namespace isaacb
+
+using namespace isaacb;
+
+namespace
+{
+    int round_up(int v, int m)
+    {
+        return (v + m - 1) / m * m;
+    }
+
+    isaacb_status check_conv(const isaacb_conv_args* a, bool wgrad)
+    {
+        if(!a)
+            return ISAACB_INVALID_ARG;
+        if(a->batch == 0 || a->in_h == 0 || a->in_w == 0 || a->out_h == 0 || a->out_w == 0 || a->c_in == 0 || a->c_out == 0)
+            return ISAACB_INVALID_ARG;
+        if(a->c_in % 8 != 0 || a->c_out % 8 != 0 || a->c_out > 256 || a->ksize < 1 || a->ksize > 7 || a->stride < 1
+           || a->stride > 4)
+            return ISAACB_INVALID_ARG;
+        const uint64_t pin = uint64_t(a->batch) * a->in_h * a->in_w, pout = uint64_t(a->batch) * a->out_h * a->out_w;
+        if(pin * a->c_in >= (1ull << 31) || pout * a->c_out >= (1ull << 31))
+            return ISAACB_INVALID_ARG;
+        if(wgrad ? (!a->x || !a->dy || !a->dw) : (!a->x || !a->w || (!a->y && !a->y_f32)))
+            return ISAACB_INVALID_ARG;
+        return ISAACB_OK;
+    }
+} // namespace
+
+extern "C"
+{
+    isaacb_status isaacb_conv_forward(const isaacb_conv_args* a, void* stream)
+    {
+        if(check_conv(a, false) != ISAACB_OK)
+        {
+            set_global_error("isaacb_conv_forward: invalid arguments");
+            return ISAACB_INVALID_ARG;
+        }
+        ConvGemmParams p{};
+        p.x = static_cast<const __nv_bfloat16*>(a->x);
+        p.w = static_cast<const __nv_bfloat16*>(a->w);
+        p.bias = a->bias;
+        p.y = static_cast<__nv_bfloat16*>(a->y);
+        p.yf = a->y_f32;
+        p.mask = static_cast<const __nv_bfloat16*>(a->mask);
+        p.B = int(a->batch);
+        p.H = int(a->in_h);
+        p.W = int(a->in_w);
+        p.Cg = int(a->c_in);
+        p.Ho = int(a->out_h);
+        p.Wo = int(a->out_w);
+        p.Cout = int(a->c_out);
+        p.Npad = round_up(int(a->c_out), 16);
+        p.Kpad = round_up(int(a->ksize * a->ksize * a->c_in), 64);
+        p.ks = int(a->ksize);
+        p.stride = int(a->stride);
+        p.pad = int(a->pad);
+        p.transposed = a->transposed ? 1 : 0;
+        p.relu = a->relu ? 1 : 0;
+        p.accumulate = a->accumulate ? 1 : 0;
+        p.errorFlag = a->error_flag;
+        if(!launch_conv_gemm(p, (cudaStream_t) stream))
+        {
+            set_global_error("isaacb_conv_forward: weights do not fit in shared memory");
+            return ISAACB_INVALID_ARG;
+        }
+        const cudaError_t e = cudaGetLastError();
+        if(e != cudaSuccess)
+        {
+            set_global_error(std::string("isaacb_conv_forward: ") + cudaGetErrorString(e));
+            return ISAACB_CUDA_ERROR;
+        }
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_conv_wgrad(const isaacb_conv_args* a, void* stream)
+    {
+        if(check_conv(a, true) != ISAACB_OK)
+        {
+            set_global_error("isaacb_conv_wgrad: invalid arguments");
+            return ISAACB_INVALID_ARG;
+        }
+        WgradParams p{};
+        p.x = static_cast<const __nv_bfloat16*>(a->x);
+        p.dy = static_cast<const __nv_bfloat16*>(a->dy);
+        p.dw = a->dw;
+        p.B = int(a->batch);
+        p.H = int(a->in_h);
+        p.W = int(a->in_w);
+        p.Cin = int(a->c_in);
+        p.Ho = int(a->out_h);
+        p.Wo = int(a->out_w);
+        p.Cout = int(a->c_out);
+        p.Npad = round_up(int(a->c_out), 16);
+        p.ks = int(a->ksize);
+        p.stride = int(a->stride);
+        p.pad = int(a->pad);
+        p.Mtot = int(a->ksize * a->ksize * a->c_in);
+        p.errorFlag = a->error_flag;
+        if(!launch_conv_wgrad(p, (cudaStream_t) stream))
+        {
+            set_global_error("isaacb_conv_wgrad: tile does not fit in shared memory");
+            return ISAACB_INVALID_ARG;
+        }
+        const cudaError_t e = cudaGetLastError();
+        if(e != cudaSuccess)
+        {
+            set_global_error(std::string("isaacb_conv_wgrad: ") + cudaGetErrorString(e));
+            return ISAACB_CUDA_ERROR;
+        }
+        return ISAACB_OK;
+    }
+}

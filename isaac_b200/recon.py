@@ -1,0 +1,144 @@
+"""Learned frame reconstructor: Python side of ``isaacb_recon_*``.
+
+A 4-level convolutional U-Net rebuilds the full-size frame from a half-size
+render taken at twice the ray step.  The network trains and runs on the GPU
+in the library's own tcgen05 kernels; this module holds the weights file
+format, the training loop's host side and the judged renderer that falls back
+to the plain full-size render when the reconstruction's PSNR against it drops
+below a threshold.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+WEIGHTS = Path(__file__).resolve().parent / "data" / "recon_unet.f32"
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _stream():
+    return C.c_void_p(_torch().cuda.current_stream().cuda_stream)
+
+
+def psnr_from_sq(sq: float, nbytes: int) -> float:
+    mse = sq / max(nbytes, 1)
+    return float("inf") if mse == 0 else 10.0 * math.log10(255.0**2 / mse)
+
+
+class Reconstructor:
+    """The network with buffers for ``max_batch`` half-size inputs of max_h x max_w."""
+
+    def __init__(self, max_batch: int, max_h: int, max_w: int, seed: int = 1):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        check(self.lib.isaacb_recon_create(max_batch, max_h, max_w, seed, C.byref(h)))
+        self.handle = h
+        self.n_params = int(self.lib.isaacb_recon_param_count())
+        torch = _torch()
+        self._loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+        self._sq = torch.zeros(1, dtype=torch.int64, device="cuda")
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.isaacb_recon_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------ parameters
+    def params(self) -> np.ndarray:
+        out = np.empty(self.n_params, np.float32)
+        check(self.lib.isaacb_recon_get_params(self.handle, out.ctypes.data_as(_lib._fp)))
+        return out
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.n_params
+        check(self.lib.isaacb_recon_set_params(self.handle, p.ctypes.data_as(_lib._fp)))
+
+    def save(self, path: Path = WEIGHTS):
+        path = Path(path)
+        path.parent.mkdir(parents=True, exist_ok=True)
+        self.params().tofile(path)
+
+    def load(self, path: Path = WEIGHTS):
+        self.set_params(np.fromfile(path, dtype=np.float32))
+
+    # ------------------------------------------------------------------ training
+    def train_step(self, low, high, index, lr: float):
+        """One Adam step; ``low`` (N,h,w,4) and ``high`` (N,2h,2w,4) uint8 CUDA tensors,
+        ``index`` an int32 CUDA tensor of the batch's pairs.  Returns the loss as a CUDA tensor."""
+        n, h, w, _ = low.shape
+        check(
+            self.lib.isaacb_recon_train_step(
+                self.handle, C.c_void_p(low.data_ptr()), C.c_void_p(high.data_ptr()), C.c_void_p(index.data_ptr()),
+                int(index.numel()), h, w, float(lr), C.c_void_p(self._loss.data_ptr()), None, _stream(),
+            )
+        )
+        return self._loss
+
+    def gradients(self, low, high, index=None):
+        """Loss gradient with respect to the parameters (no update), as a numpy array."""
+        n, h, w, _ = low.shape
+        g = np.empty(self.n_params, np.float32)
+        check(
+            self.lib.isaacb_recon_train_step(
+                self.handle, C.c_void_p(low.data_ptr()), C.c_void_p(high.data_ptr()),
+                None if index is None else C.c_void_p(index.data_ptr()), n if index is None else int(index.numel()),
+                h, w, 0.0, C.c_void_p(self._loss.data_ptr()), g.ctypes.data_as(_lib._fp), _stream(),
+            )
+        )
+        return g, float(self._loss.item())
+
+    # ------------------------------------------------------------------ inference
+    def infer(self, low, out=None):
+        """Full-size RGBA8 frame (2h, 2w, 4) from a half-size (h, w, 4) CUDA tensor."""
+        torch = _torch()
+        h, w, _ = low.shape
+        if out is None:
+            out = torch.empty((2 * h, 2 * w, 4), dtype=torch.uint8, device="cuda")
+        check(self.lib.isaacb_recon_infer(self.handle, C.c_void_p(low.data_ptr()), h, w, C.c_void_p(out.data_ptr()), _stream()))
+        return out
+
+    def error_flag(self) -> int:
+        f = C.c_int32()
+        check(self.lib.isaacb_recon_error(self.handle, C.byref(f)))
+        return int(f.value)
+
+
+def bilinear2(low, out=None):
+    """The method without the network: bilinear x2 of a half-size (h, w, 4) CUDA frame."""
+    torch = _torch()
+    h, w, _ = low.shape
+    if out is None:
+        out = torch.empty((2 * h, 2 * w, 4), dtype=torch.uint8, device="cuda")
+    check(_lib.load().isaacb_upsample_bilinear2(C.c_void_p(low.data_ptr()), h, w, C.c_void_p(out.data_ptr()), _stream()))
+    return out
+
+
+def psnr(a, b, acc=None) -> float:
+    """PSNR (dB) of two RGBA8 CUDA images, reduced on the GPU."""
+    torch = _torch()
+    if acc is None:
+        acc = torch.zeros(1, dtype=torch.int64, device="cuda")
+    else:
+        acc.zero_()
+    check(_lib.load().isaacb_image_sq_error(C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()), a.numel(),
+                                            C.c_void_p(acc.data_ptr()), _stream()))
+    return psnr_from_sq(float(acc.item()), a.numel())

@@ -1,0 +1,111 @@
+"""The learned reconstructor on the GPU against the float64 CPU oracle:
+forward output, loss, every parameter's gradient, and a short training run.
+
+The oracle rounds to bf16 where the GPU stores bf16 (network input,
+activations, gradients), so the remaining differences are FP32-vs-FP64
+summation and the occasional rounding flip they cause.  Bars: loss within
+1e-3 relative; per layer, the GPU gradient within 3e-2 (relative L2) of the
+oracle's and a cosine above 0.999; reconstructed bytes within 1 LSB on 99 %
+of the values and 3 LSB everywhere."""
+
+import numpy as np
+import pytest
+import torch
+
+from isaac_b200.recon import Reconstructor, bilinear2, psnr
+from oracle import recon_oracle as R
+
+pytestmark = pytest.mark.gpu
+
+
+def _he_params(seed=0):
+    rng = np.random.default_rng(seed)
+    parts = []
+    for name, k, s, p, ci, co, relu, src in R.LAYERS:
+        fan = k * k * ci
+        parts.append(rng.standard_normal(co * fan) * np.sqrt(2.0 / fan))
+        parts.append(rng.standard_normal(co) * 0.05)
+    return np.concatenate(parts).astype(np.float32)
+
+
+def _smooth_pairs(n, h, w, seed):
+    """Smooth random RGBA pairs: a full-size image and its even-pixel subsample."""
+    rng = np.random.default_rng(seed)
+    H, W = 2 * h, 2 * w
+    yy, xx = np.meshgrid(np.arange(H), np.arange(W), indexing="ij")
+    high = np.zeros((n, H, W, 4), np.uint8)
+    for i in range(n):
+        img = np.zeros((H, W, 4))
+        for c in range(4):
+            f = rng.uniform(0.02, 0.15, 2)
+            ph = rng.uniform(0, 6.3, 2)
+            img[..., c] = 0.5 + 0.25 * np.sin(f[0] * xx + ph[0]) + 0.25 * np.cos(f[1] * yy + ph[1])
+        high[i] = np.clip(np.rint(img * 255), 0, 255)
+    low = high[:, ::2, ::2].copy()
+    return low, high
+
+
+def _layer_slices():
+    o = 0
+    for name, k, s, p, ci, co, relu, src in R.LAYERS:
+        n = co * k * k * ci + co
+        yield name, slice(o, o + n)
+        o += n
+
+
+def test_gradients_match_oracle():
+    params = _he_params(0)
+    rng = np.random.default_rng(2)
+    low = rng.integers(0, 256, (2, 12, 20, 4)).astype(np.uint8)
+    high = rng.integers(0, 256, (2, 24, 40, 4)).astype(np.uint8)
+    net = Reconstructor(2, 12, 20, seed=1)
+    net.set_params(params)
+    g, loss = net.gradients(torch.from_numpy(low).cuda(), torch.from_numpy(high).cuda())
+    assert net.error_flag() == 0
+    ref_loss, ref = R.UNet(params.astype(np.float64), bf16=True).loss_and_backward(low, high)
+    assert abs(loss - ref_loss) <= 1e-3 * ref_loss
+    for name, sl in _layer_slices():
+        a, b = g[sl].astype(np.float64), ref[sl]
+        nb = np.linalg.norm(b)
+        if nb == 0:
+            assert np.linalg.norm(a) == 0, name
+            continue
+        rel = np.linalg.norm(a - b) / nb
+        cos = float(a @ b / (np.linalg.norm(a) * nb))
+        assert rel < 3e-2 and cos > 0.999, (name, rel, cos)
+
+
+def test_inference_matches_oracle():
+    params = _he_params(3)
+    params[-528:] *= 0.1  # OUT weights and bias: a small residual, as after initialisation
+    low, _ = _smooth_pairs(1, 36, 52, 5)
+    net = Reconstructor(1, 36, 52, seed=1)
+    net.set_params(params)
+    got = net.infer(torch.from_numpy(low[0]).cuda()).cpu().numpy().astype(np.int32)
+    pred = R.UNet(params.astype(np.float64), bf16=True).predict(low)[0]
+    ref = np.clip(np.rint(pred * 255.0), 0, 255).astype(np.int32)
+    d = np.abs(got - ref)
+    assert (d <= 1).mean() >= 0.99 and d.max() <= 3, (float((d <= 1).mean()), int(d.max()))
+    # bilinear alone
+    bl = bilinear2(torch.from_numpy(low[0]).cuda()).cpu().numpy().astype(np.int32)
+    refb = np.clip(np.rint(R.upsample_bilinear2(low / 255.0)[0] * 255.0), 0, 255).astype(np.int32)
+    assert np.abs(bl - refb).max() <= 1
+
+
+def test_short_training_beats_bilinear():
+    low, high = _smooth_pairs(16, 32, 32, 7)
+    lt, ht = torch.from_numpy(low).cuda(), torch.from_numpy(high).cuda()
+    net = Reconstructor(8, 32, 32, seed=4)
+    rng = np.random.default_rng(0)
+    first = None
+    for step in range(300):
+        idx = torch.from_numpy(rng.integers(0, 16, 8).astype(np.int32)).cuda()
+        loss = float(net.train_step(lt, ht, idx, 1e-3).item())
+        first = first if first is not None else loss
+    assert net.error_flag() == 0
+    assert loss < 0.5 * first, (first, loss)
+    gains = []
+    for i in range(4):
+        rec = net.infer(lt[i])
+        gains.append(psnr(rec, ht[i]) - psnr(bilinear2(lt[i]), ht[i]))
+    assert min(gains) > 0.5, gains
