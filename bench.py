@@ -45,10 +45,11 @@ def parse_args():
     ap.add_argument(
         "--scene",
         default="precision",
-        choices=["precision", "gaussian", "full", "batch"],
+        choices=["precision", "gaussian", "full", "batch", "learned"],
         help="precision: N sources of size^3 (default); gaussian: 128^3 scalar + curl at 512x512; "
         "full: 3 x 256^3 + 1M particles, iso, 2 clipping planes, SSAO at 1080p; "
-        "batch: the precision sources over 4 timesteps, 16 views of uneven resolution in one launch",
+        "batch: the precision sources over 4 timesteps, 16 views of uneven resolution in one launch; "
+        "learned: BF16 bricks, half-size render at twice the step + U-Net vs the plain full-size render",
     )
     ap.add_argument("--timesteps", type=int, default=4, help="batch scene: timesteps (contexts)")
     ap.add_argument("--shift", type=float, default=0.05, help="batch scene: advection per timestep, fraction of the box")
@@ -74,6 +75,18 @@ def measured_peaks():
         except Exception:
             pass
     return FALLBACK_HBM_GBS, "fallback"
+
+
+def measured_peaks_all() -> dict:
+    """Every figure of MEASURED_PEAKS.json, with the fallbacks where it is absent."""
+    d = {"hbm_gbs": FALLBACK_HBM_GBS, "bf16_tflops": 1590.0}
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d.update({k: float(v) for k, v in json.loads(p.read_text()).items() if isinstance(v, (int, float))})
+        except Exception:
+            pass
+    return d
 
 
 class ClockSampler:
@@ -138,6 +151,8 @@ def apply_scene_defaults(args):
     """The gaussian and full scenes fix their own sizes."""
     if args.scene == "gaussian":
         args.size, args.width, args.height, args.sources = 128, 512, 512, 2
+    elif args.scene == "learned":
+        args.renderer, args.dtype, args.sources = "per_source", "bf16", 4
     elif args.scene == "full":
         args.size, args.sources = 256, 3
         args.width = args.width or 1920
@@ -165,7 +180,7 @@ def build_scene(args, device):
 
     n = args.size
     sc = Scene()
-    if args.scene == "precision":
+    if args.scene in ("precision", "learned"):
         seeds = (6, 7, 8, 9, 10, 11, 12, 13)[: args.sources]
         slopes = (-5.0 / 3.0, -2.0, -3.0, -11.0 / 3.0, -5.0 / 3.0, -2.0, -3.0, -11.0 / 3.0)[: args.sources]
         fields = scenes.precision_scene(n, seeds=seeds, slopes=slopes, device=device)
@@ -246,7 +261,14 @@ def oracle_for(args, sc):
     if npart:
         fds = fds + [int(sc.particles[2].shape[1])]
     o = O.Oracle((args.width, args.height), (n, n, n), (n, n, n), pcells, (0, 0, 0), (1, 1, 1), fds, [1] * len(fds), nv)
+    import torch
+
+    dt = {"f32": 0, "bf16": 1, "f16": 2}[args.dtype] if args.renderer == "per_source" else 0
     for i, (t, _) in enumerate(sc.volumes):
+        if dt:
+            # the per-source renderer samples the stored (rounded) values
+            t = t.to(torch.bfloat16 if dt == 1 else torch.float16).float()
+            o.set_storage(i, dt)
         o.set_source(i, t.cpu().numpy())
     if npart:
         off, pos, attr, radius, _ = sc.particles
@@ -337,6 +359,11 @@ def run_reference(args):
 
 
 def metric_name(args):
+    if args.scene == "learned":
+        return (
+            f"fps @{args.width}x{args.height}, {args.sources}x{args.size}^3 BF16 bricks: learned path "
+            f"({args.width // 2}x{args.height // 2} step 1.0 + U-Net, judged every 16th frame) vs plain step 0.5"
+        )
     if args.scene == "batch":
         return (
             f"batch frames/s: 16 views (4x256^2, 4x720p, 4x1080p, 4x2048x1152) over {args.timesteps} timesteps "
@@ -357,6 +384,20 @@ def config_of(args):
         "batch": f"batching scene: {args.timesteps} timesteps (advected {args.shift} box/step) of {args.sources} x "
         f"{args.size}^3 float32 spectral sources, 16 views of uneven resolution",
     }
+    if args.scene == "learned":
+        return {
+            "workload": f"learned reconstruction: {args.sources} x {args.size}^3 spectral sources as BF16 bricks "
+            f"(per-source renderer), {args.width // 2}x{args.height // 2} at step 1.0 + 4-level U-Net -> "
+            f"{args.width}x{args.height}; plain {args.width}x{args.height} step 0.5 every 16th frame as judge, "
+            "fallback below 40 dB; orbiting camera over one timestep",
+            "scene": "learned",
+            "sources": args.sources,
+            "volume": args.size,
+            "framebuffer": [args.width, args.height],
+            "renderer": "per_source (bf16 bricks)",
+            "parallelism": "replicas",
+            "l2": "inputs larger than L2 (sources and bricks are > 126 MB)",
+        }
     if args.scene == "batch":
         return {
             "workload": names["batch"] + ", trilinear, step 0.5, combined renderer, 4 merges + 1 persistent render per step",
@@ -671,6 +712,189 @@ def run_batch(args, world, rank, local, barrier, max_over_ranks):
     return 0
 
 
+# ---------------------------------------------------------------------------- learned reconstruction scene
+def run_learned(args, world, rank, local, barrier, max_over_ranks):
+    """Plain full-size frames against the judged learned path on the same
+    orbiting camera: every frame a half-size render at twice the step and the
+    U-Net; every 16th frame also the plain render as judge (fallback below 40 dB)."""
+    import numpy as np
+    import torch
+
+    from isaac_b200 import recon, scenes
+    from isaac_b200.recon_train import PairRenderer
+
+    W, H = args.width, args.height
+    pr = PairRenderer(args.size, W, H)
+    pr.set_timestep(0)
+    tfs = [scenes.transfer_4point(0.7 * i) for i in range(args.sources)]
+    n_frames = max(16, (args.steps + 15) // 16 * 16)
+    cams = [scenes.orbit_camera(W, H, yaw=2 * np.pi * k / 96.0, pitch=0.35, distance=2.4) for k in range(n_frames)]
+    pr.set_view(*cams[0], tfs)
+    pr.full.update()
+    pr.low.update()
+    net = recon.Reconstructor(1, H // 2, W // 2, seed=1)
+    if not recon.WEIGHTS.exists():
+        raise SystemExit(f"trained weights missing: {recon.WEIGHTS} (python -m isaac_b200.recon_train)")
+    net.load()
+    jr = recon.JudgedRenderer(pr.full, pr.low, net, judge_every=16, threshold=40.0)
+    full = torch.empty((H, W, 4), dtype=torch.uint8, device="cuda")
+
+    # samples per full-size and half-size frame (untimed)
+    pr.full.setCounting(True)
+    pr.low.setCounting(True)
+    pr.full.render(full)
+    pr.low.render(jr.half)
+    full_samples = pr.full.counters()[0]
+    half_samples = pr.low.counters()[0]
+    pr.full.setCounting(False)
+    pr.low.setCounting(False)
+
+    # quality over every frame of the orbit (untimed): reconstruction and bilinear x2 against plain
+    rec_psnr, bil_psnr = [], []
+    tmp = torch.empty_like(full)
+    for P, MV in cams:
+        jr.setCamera(P, MV)
+        pr.full.render(full)
+        pr.low.render(jr.half)
+        net.infer(jr.half, jr.rec)
+        rec_psnr.append(recon.psnr(jr.rec, full))
+        bil_psnr.append(recon.psnr(recon.bilinear2(jr.half, tmp), full))
+
+    def timed(fn):
+        for k in range(args.warmup):
+            fn(k)
+        torch.cuda.synchronize()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in range(n_frames):
+            fn(k)
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / n_frames)
+
+    def plain(k):
+        pr.full.setCamera(*cams[k % n_frames])
+        pr.full.render(full)
+
+    def learned(k):
+        jr.setCamera(*cams[k % n_frames])
+        jr.frame()
+
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.3)
+    plain_ms = timed(plain)
+    jr.count, jr.judged, jr.fallback, jr.fallback_frames = 0, [], False, 0
+    learned_ms = timed(learned)
+    clocks = clk.stop()
+    judged = [p for _, p in jr.judged[-(n_frames // 16):]]
+
+    # phases of one learned frame (events on the launch stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    nt = 8
+    half_ms = net_ms = 0.0
+    for k in range(nt):
+        pr.low.setCamera(*cams[k])
+        ev[0].record()
+        pr.low.render(jr.half)
+        ev[1].record()
+        net.infer(jr.half, jr.rec)
+        ev[2].record()
+        ev[2].synchronize()
+        half_ms += ev[0].elapsed_time(ev[1]) / nt
+        net_ms += ev[1].elapsed_time(ev[2]) / nt
+    flops = recon.inference_flops(H // 2, W // 2)
+    peaks = measured_peaks_all()
+    roofline = {
+        "bound": "tensor",
+        "kernel": "U-Net inference (k_conv_gemm tcgen05 layers + elementwise), one 960x540 frame",
+        "achieved": flops / (net_ms * 1e-3) / 1e12 if net_ms > 0 else None,
+        "peak": peaks.get("bf16_tflops"),
+        "peak_kind": "measured bf16 burst",
+        "unit": "TFLOP/s",
+        "frac": (flops / (net_ms * 1e-3) / 1e12 / peaks["bf16_tflops"]) if net_ms > 0 and peaks.get("bf16_tflops") else None,
+        "traffic": None,
+        "flops_per_launch": flops,
+        "kernel_ms": net_ms,
+        "half_render_ms": half_ms,
+        "half_render_samples": half_samples,
+        "half_render_gbs_bf16": half_samples * 64 / (half_ms * 1e-3) / 1e9 if half_ms > 0 else None,
+    }
+
+    # end to end through the public API: camera in, frame D2H to pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty((H, W, 4), dtype=torch.uint8).pin_memory()
+
+        def e2e_step(k):
+            jr.setCamera(*cams[k % n_frames])
+            host.copy_(jr.frame(), non_blocking=True)
+
+        jr.count, jr.fallback = 0, False
+        e2e_ms = timed(e2e_step)
+        e2e = {"value": world * 1000.0 / e2e_ms, "unit": "frames/s", "h2d_bytes_per_step": 2 * 16 * 8,
+               "d2h_bytes_per_step": H * W * 4, "ms_per_step": e2e_ms,
+               "note": "inputs per step are the two camera matrices; the sources stay one resident timestep"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            sc = build_scene(args, "cuda")
+            sc.P, sc.MV = cams[0]
+            o = oracle_for(args, sc)
+            frame_s, sps, rows, merge_s, band_s, cs, threads = cpu_sample(args, o, args.cpu_rows)
+            cpu = {"value": 1.0 / frame_s, "unit": "frames/s", "cores": threads, "kind": "port",
+                   "sample": f"plain per-source BF16 path: brick update ({merge_s:.2f} s) + {rows} of {H} rows "
+                   f"({band_s:.2f} s), extrapolated to a frame"}
+            del o, sc
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "frames/s", "cores": None, "kind": "port", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        fps = world * 1000.0 / learned_ms
+        plain_fps = world * 1000.0 / plain_ms
+        line = {
+            "metric": metric_name(args),
+            "value": fps,
+            "unit": "frames/s",
+            "n_gpus": world,
+            "steps": n_frames,
+            "warmup": args.warmup,
+            "ms_per_step": learned_ms,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "bf16",
+            "data": "synthetic (seeded spectral fields); network trained on renderer-made pairs",
+            "config": config_of(args),
+            "plain_fps": plain_fps,
+            "plain_ms": plain_ms,
+            "speedup_vs_plain": fps / plain_fps,
+            "psnr_db": {"reconstruction_mean": float(np.mean(rec_psnr)), "reconstruction_min": float(np.min(rec_psnr)),
+                        "bilinear_mean": float(np.mean(bil_psnr)), "bilinear_min": float(np.min(bil_psnr)),
+                        "frames_at_or_above_40db": float(np.mean(np.array(rec_psnr) >= 40.0)),
+                        "judged_in_timed_run": judged},
+            "fallback_frames": jr.fallback_frames,
+            "samples_per_frame": {"full": full_samples, "half": half_samples},
+            "phases_ms": {"half_render": half_ms, "unet": net_ms},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clocks,
+            "gpu_launches": None,
+        }
+        print(json.dumps(line), flush=True)
+    net.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse_args()
     apply_scene_defaults(args)
@@ -703,6 +927,8 @@ def main():
 
     if args.scene == "batch":
         return run_batch(args, world, rank, local, barrier, max_over_ranks)
+    if args.scene == "learned":
+        return run_learned(args, world, rank, local, barrier, max_over_ranks)
 
     sc = build_scene(args, "cuda")
     viz = make_viz(args, sc)

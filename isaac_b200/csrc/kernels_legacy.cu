@@ -292,9 +292,160 @@ namespace isaacb
             count_warp(p.counters, n);
     }
 
+    // 4 consecutive stored values (one x-quad of a slot) as floats
+    template<int DT>
+    __device__ __forceinline__ void load_quad(const void* base, size_t slot, float (&v)[4])
+    {
+        if constexpr(DT == 0)
+        {
+            const float4 q = __ldg(reinterpret_cast<const float4*>(base) + slot);
+            v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+        }
+        else
+        {
+            const uint2 q = __ldg(reinterpret_cast<const uint2*>(base) + slot);
+            if constexpr(DT == 1)
+            {
+                v[0] = __uint_as_float(q.x << 16);
+                v[1] = __uint_as_float(q.x & 0xFFFF0000u);
+                v[2] = __uint_as_float(q.y << 16);
+                v[3] = __uint_as_float(q.y & 0xFFFF0000u);
+            }
+            else
+            {
+                const __half2 a = *reinterpret_cast<const __half2*>(&q.x), b = *reinterpret_cast<const __half2*>(&q.y);
+                const float2 fa = __half22float2(a), fb = __half22float2(b);
+                v[0] = fa.x, v[1] = fa.y, v[2] = fb.x, v[3] = fb.y;
+            }
+        }
+    }
+
+    // The same march as k_shade_volume_per_source for the common case of scalar,
+    // persistent sources that share one storage type: the trilinear footprint (slot
+    // and fractions) is found once per sample for all sources, and each source's
+    // two x-quads come in two vector loads.  Arithmetic and order are unchanged,
+    // so the frame is bit-identical to the general kernel's.
+    template<int DT, bool LINEAR>
+    __global__ void __launch_bounds__(256) k_shade_volume_per_source_scalar(const __grid_constant__ FrameParams p)
+    {
+        int px, py;
+        thread_pixel(px, py);
+        unsigned long long n = 0;
+        if(px < p.v.W && py < p.v.H)
+        {
+            const size_t o = size_t(py) * p.v.W + px;
+            shade_pixel(p, px, py, o);
+            bool any = false;
+            for(int s = 0; s < p.nVol; ++s)
+                any |= p.ps[s].weight != 0.0f;
+            Ray ray = pixel_to_ray(p.v, p.g, px, py);
+            if(any && clip_ray(ray, p.v, p.g))
+            {
+                ray.endDepth = gmin(ray.endDepth, p.depth[o]);
+                if(!(ray.endDepth <= ray.startDepth))
+                {
+                    March m = march_setup(ray, p.g, p.v.scale, p.step);
+                    legacy_bounds(p.g, m);
+                    const Geom& g = p.g;
+                    float4 value = make_float4(0, 0, 0, 0);
+                    float4 color = make_float4(0, 0, 0, 0);
+                    for(int i = m.startSteps; i <= m.endSteps; i++)
+                    {
+                        ++n;
+                        const float3 pos = march_pos(m, i);
+                        size_t q0;
+                        float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+                        if(LINEAR)
+                        {
+                            const float cx = pos.x - 0.5f, cy = pos.y - 0.5f, cz = pos.z - 0.5f;
+                            fx = cx - floorf(cx);
+                            fy = cy - floorf(cy);
+                            fz = cz - floorf(cz);
+                            // persistent sources: isaac_int(offsetPos) truncates
+                            const int ix = iclamp(f2i(cx), -1, g.ls[0] - 1);
+                            const int iy = iclamp(f2i(cy), -1, g.ls[1] - 1);
+                            const int iz = iclamp(f2i(cz), -1, g.ls[2] - 1);
+                            q0 = brick_slot(g, ix, iy, iz);
+                        }
+                        else
+                        {
+                            const int ix = iclamp(f2i(pos.x), 0, g.ls[0] - 1);
+                            const int iy = iclamp(f2i(pos.y), 0, g.ls[1] - 1);
+                            const int iz = iclamp(f2i(pos.z), 0, g.ls[2] - 1);
+                            q0 = brick_slot(g, ix, iy, iz);
+                        }
+                        for(int s = 0; s < p.nVol; ++s)
+                        {
+                            const PerSourceSrc& S = p.ps[s];
+                            const float w = S.weight;
+                            if(w == 0.0f)
+                                continue;
+                            float a[4], b[4];
+                            load_quad<DT>(S.bricks, q0, a);
+                            float v[4] = {0, 0, 0, 0};
+                            if(LINEAR)
+                            {
+                                load_quad<DT>(S.bricks, q0 + 64, b);
+                                v[0] = tri_q(fx, fy, fz, a[0], a[1], a[2], a[3], b[0], b[1], b[2], b[3]);
+                            }
+                            else
+                                v[0] = a[0];
+                            const float result = apply_chain(v, S.fdim, S.chain);
+                            float4 c = __ldg(p.lut + size_t(s) * p.ts + lut_index(result, p.ts));
+                            c.w *= w;
+                            value.x += c.x * c.w;
+                            value.y += c.y * c.w;
+                            value.z += c.z * c.w;
+                            value.w += c.w;
+                        }
+                        const float oma = 1.0f - color.w;
+                        value = make_float4(value.x * m.factor, value.y * m.factor, value.z * m.factor, value.w * m.factor);
+                        color.x += oma * value.x;
+                        color.y += oma * value.y;
+                        color.z += oma * value.z;
+                        color.w += oma * value.w;
+                        if(color.w > 0.99f)
+                            break;
+                    }
+                    const float4 solid = from_byte4(p.color[o]);
+                    const float r = 1.0f - color.w;
+                    color = make_float4(color.x + r * solid.x, color.y + r * solid.y, color.z + r * solid.z, color.w + r * solid.w);
+                    p.color[o] = to_byte4(color);
+                }
+            }
+        }
+        if(p.counters)
+            count_warp(p.counters, n);
+    }
+
     void launch_shade_volume_per_source(const FrameParams& p, cudaStream_t s)
     {
         dim3 grid((p.v.W + 31) / 32, (p.v.H + 7) / 8);
+        // the scalar kernel serves frames whose weighted sources are all scalar, persistent and of one type
+        int dt = -1;
+        bool scalar = true;
+        for(int k = 0; k < p.nVol && scalar; ++k)
+        {
+            const PerSourceSrc& S = p.ps[k];
+            if(S.weight == 0.0f)
+                continue;
+            scalar = S.fdim == 1 && S.ncomp == 1 && S.persistent && (dt < 0 || dt == S.dtype);
+            dt = S.dtype;
+        }
+        if(scalar && dt >= 0)
+        {
+            const bool lin = p.interpolation != 0;
+            if(dt == 0)
+                lin ? k_shade_volume_per_source_scalar<0, true><<<grid, 256, 0, s>>>(p)
+                    : k_shade_volume_per_source_scalar<0, false><<<grid, 256, 0, s>>>(p);
+            else if(dt == 1)
+                lin ? k_shade_volume_per_source_scalar<1, true><<<grid, 256, 0, s>>>(p)
+                    : k_shade_volume_per_source_scalar<1, false><<<grid, 256, 0, s>>>(p);
+            else
+                lin ? k_shade_volume_per_source_scalar<2, true><<<grid, 256, 0, s>>>(p)
+                    : k_shade_volume_per_source_scalar<2, false><<<grid, 256, 0, s>>>(p);
+            return;
+        }
         k_shade_volume_per_source<<<grid, 256, 0, s>>>(p);
     }
 } // namespace isaacb

@@ -233,7 +233,8 @@ namespace
         int B,
         int h,
         int w,
-        float gradScale)
+        float gradScale,
+        float invCount)
     {
         float acc = 0.0f;
         const size_t n = size_t(B) * h * w;
@@ -290,7 +291,7 @@ namespace
             float s = 0.0f;
             for(int k = 0; k < int(blockDim.x >> 5); ++k)
                 s += red[k];
-            atomicAdd(lossSum, s);
+            atomicAdd(lossSum, s * invCount);
         }
     }
 
@@ -869,7 +870,7 @@ extern "C"
             return fail_r(ISAACB_INVALID_ARG, "isaacb_recon_train_step: layer does not fit");
         cudaMemsetAsync(R->lossSum, 0, sizeof(float), s);
         const float n = float(pix0) * 16.0f;
-        k_loss<<<grid_for(pix0), 256, 0, s>>>(low, high, index, R->r, R->dpre[kLayers - 1], R->lossSum, B, int(h), int(w), 2.0f / n);
+        k_loss<<<grid_for(pix0), 256, 0, s>>>(low, high, index, R->r, R->dpre[kLayers - 1], R->lossSum, B, int(h), int(w), 2.0f / n, 1.0f / n);
         if(!backward(R, B, s))
             return fail_r(ISAACB_INVALID_ARG, "isaacb_recon_train_step: layer does not fit");
         table_pointers(R, true);

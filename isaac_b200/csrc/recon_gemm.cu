@@ -522,7 +522,15 @@ namespace isaacb
         cudaFuncSetAttribute(k_conv_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         const int P = p.B * p.Ho * p.Wo;
         const int tiles = (P + kTileM - 1) / kTileM;
-        const int grid = tiles < num_sms() ? tiles : num_sms();
+        // as many persistent CTAs as fit on an SM (shared memory and TMEM permitting), so one
+        // CTA's epilogue and gathers overlap another's MMAs
+        int perSm = 1;
+        if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_conv_gemm, kThreads, smem) != cudaSuccess || perSm < 1)
+            perSm = 1;
+        while(perSm > 1 && perSm * int(tmem_columns(p.Npad)) > 512)
+            --perSm;
+        const int slots = num_sms() * perSm;
+        const int grid = tiles < slots ? tiles : slots;
         k_conv_gemm<<<grid, kThreads, smem, s>>>(p);
         return true;
     }

@@ -142,3 +142,92 @@ def psnr(a, b, acc=None) -> float:
     check(_lib.load().isaacb_image_sq_error(C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()), a.numel(),
                                             C.c_void_p(acc.data_ptr()), _stream()))
     return psnr_from_sq(float(acc.item()), a.numel())
+
+
+class JudgedRenderer:
+    """The learned path with the plain renderer as its judge and fallback.
+
+    Every frame renders the half-size view (``low_viz``, twice the ray step)
+    and reconstructs the full-size frame.  Every ``judge_every``-th frame,
+    the first included, the plain full-size frame (``full_viz``) is rendered
+    too and the reconstruction's PSNR against it measured on the GPU.  Below
+    ``threshold`` dB the plain frame is served, and plain frames keep being
+    served until a later judge frame measures the reconstruction at or above
+    the threshold again.  Both visualizations must show the same sources,
+    transfer functions and camera."""
+
+    def __init__(self, full_viz, low_viz, net, judge_every: int = 16, threshold: float = 40.0, measure=None, device="cuda"):
+        torch = _torch()
+        self.full_viz, self.low_viz, self.net = full_viz, low_viz, net
+        self.judge_every, self.threshold = judge_every, threshold
+        W, H = full_viz.framebufferSize
+        w, h = low_viz.framebufferSize
+        if (W, H) != (2 * w, 2 * h):
+            raise ValueError("the half-size view must be exactly half the full size")
+        self.half = torch.empty((h, w, 4), dtype=torch.uint8, device=device)
+        self.rec = torch.empty((H, W, 4), dtype=torch.uint8, device=device)
+        self.full = torch.empty((H, W, 4), dtype=torch.uint8, device=device)
+        self._acc = torch.zeros(1, dtype=torch.int64, device=device)
+        # PSNR (dB) of the reconstruction against the plain frame
+        self.measure = measure or (lambda a, b: psnr(a, b, self._acc))
+        self.count = 0
+        self.fallback = False
+        self.judged = []  # (frame number, PSNR dB)
+        self.fallback_frames = 0
+
+    def setCamera(self, projection, modelview):
+        self.full_viz.setCamera(projection, modelview)
+        self.low_viz.setCamera(projection, modelview)
+
+    def frame(self, update: bool = False):
+        """The frame to show, an (H, W, 4) uint8 CUDA tensor (row 0 = bottom)."""
+        k = self.count
+        self.count += 1
+        judge = k % self.judge_every == 0
+        if self.fallback and not judge:
+            self.fallback_frames += 1
+            if update:
+                self.full_viz.update()
+            self.full_viz.render(self.full)
+            return self.full
+        if update:
+            self.low_viz.update()
+        self.low_viz.render(self.half)
+        self.net.infer(self.half, self.rec)
+        if not judge:
+            return self.rec
+        if update:
+            self.full_viz.update()
+        self.full_viz.render(self.full)
+        p = self.measure(self.rec, self.full)
+        self.judged.append((k, p))
+        self.fallback = p < self.threshold
+        if self.fallback:
+            self.fallback_frames += 1
+            return self.full
+        return self.rec
+
+
+# (ksize, stride, pad, c_in, c_out, output level) of the network's convolutions
+LAYER_SHAPES = [
+    (3, 1, 1, 8, 32, 0), (3, 1, 1, 32, 32, 0), (3, 2, 1, 32, 64, 1), (3, 1, 1, 64, 64, 1), (3, 2, 1, 64, 96, 2),
+    (2, 2, 0, 96, 128, 3), (1, 1, 0, 224, 96, 2), (1, 1, 0, 160, 64, 1), (1, 1, 0, 96, 32, 0), (3, 1, 1, 32, 32, 0),
+    (1, 1, 0, 32, 16, 0),
+]
+
+
+def level_sizes(h: int, w: int):
+    def o(n, k, s, p):
+        return (n + 2 * p - k) // s + 1
+
+    hs, ws = [h], [w]
+    for k, s, p in ((3, 2, 1), (3, 2, 1), (2, 2, 0)):
+        hs.append(o(hs[-1], k, s, p))
+        ws.append(o(ws[-1], k, s, p))
+    return hs, ws
+
+
+def inference_flops(h: int, w: int) -> float:
+    """Multiply-adds x 2 of one inference on an h x w half-size frame (the convolutions)."""
+    hs, ws = level_sizes(h, w)
+    return float(sum(2 * k * k * ci * co * hs[l] * ws[l] for k, s, p, ci, co, l in LAYER_SHAPES))

@@ -184,6 +184,17 @@ def camera(width: int, height: int, seed: int = 1, distance: float = 2.5, fov_de
     return P, MV
 
 
+def orbit_camera(width: int, height: int, yaw: float, pitch: float = 0.3, distance: float = 2.5, fov_degrees: float = 45.0):
+    """Projection and modelview of a camera orbiting the volume centre (angles in radians)."""
+    P = perspective(math.radians(fov_degrees), width / height, 0.002, 100.0)
+    rot = _cm_mul(rotation_x(pitch), rotation_y(yaw))
+    R = np.eye(4)
+    R[0:3, 0:3] = rot
+    D = np.eye(4)
+    D[3][2] = -distance
+    return P, _cm_mul(D, R)
+
+
 def transfer_4point(hue: float = 0.0):
     """A 4-point piecewise-linear RGBA transfer function (keys in 0..1024)."""
     h = hue

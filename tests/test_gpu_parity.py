@@ -219,6 +219,21 @@ def test_per_source_renderer(dtype, persistent):
     assert_image_parity(got, ref)
 
 
+@pytest.mark.parametrize("dtype", [0, 1, 2])
+@pytest.mark.parametrize("interp", [True, False])
+def test_per_source_scalar_sources(dtype, interp):
+    """Scalar persistent sources of one storage type take the specialised kernel."""
+    fields = scenes.precision_scene(24)
+    s = Scene(n=(24, 24, 24), fb=(56, 40), volumes=[(f.numpy(), True) for f in fields], optimized=False)
+    s.transfer = [scenes.transfer_4point(0.7 * i) for i in range(4)]
+    s.storage = [dtype] * 4
+    s.interpolation = interp
+    s.weights = [2.0, 0.0, 1.5, 2.0]  # a disabled source in the middle
+    s.functions = ["idem", "idem", "mul(0.8)|add(0.1)", "idem"]
+    got, ref, _, _ = _frames(s)
+    assert_image_parity(got, ref)
+
+
 @pytest.mark.parametrize("interp", [True, False])
 def test_per_source_iso(interp):
     s = gaussian_pair(n=32, fb=(64, 48), optimized=False, interpolation=interp, iso=[0.3, 0.2])
