@@ -140,6 +140,16 @@ namespace isaacb
             return false;
         }
 
+        __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+        {
+            asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" ::"r"(smem_addr(bar)) : "memory");
+        }
+        // the barrier receives one arrival once all of this thread's earlier cp.async copies have landed
+        __device__ __forceinline__ void cp_async_arrive(uint64_t* bar)
+        {
+            asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+        }
+
         // ------------------------------------------------------------ cp.async
         // 16-byte gather; srcBytes = 0 writes zeros (the address is not read)
         __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t srcBytes)

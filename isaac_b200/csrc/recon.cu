@@ -101,7 +101,8 @@ namespace
         }
     }
 
-    // half-size RGBA8 frames (batch entry b is frame index[b]) -> network input
+    // half-size RGBA8 frames (batch entry b is frame index[b]) -> network input: RGBA / 255
+    // and zeros, 16 channels (the parameters see the first 8; the GEMM wants multiples of 16)
     __global__ void k_input(const uint8_t* __restrict__ low, const int32_t* __restrict__ index, int B, int h, int w, bf16* __restrict__ x)
     {
         const size_t n = size_t(B) * h * w;
@@ -113,7 +114,8 @@ namespace
             const int f = index ? __ldg(index + b) : b;
             const uchar4 c = __ldg(reinterpret_cast<const uchar4*>(low) + size_t(f) * hw + pp);
             float v[8] = {float(c.x) / 255.0f, float(c.y) / 255.0f, float(c.z) / 255.0f, float(c.w) / 255.0f, 0, 0, 0, 0};
-            reinterpret_cast<uint4*>(x)[i] = pack8(v);
+            reinterpret_cast<uint4*>(x)[2 * i] = pack8(v);
+            reinterpret_cast<uint4*>(x)[2 * i + 1] = make_uint4(0, 0, 0, 0);
         }
     }
 
@@ -379,6 +381,7 @@ namespace
     {
         int off[kLayers + 1]; // flat offsets of each layer's weights (then its bias)
         int ks[kLayers], cin[kLayers], cout[kLayers];
+        int cg[kLayers]; // input channels of the GEMM layout (cin rounded up to 16)
         int Npad[kLayers], Kpad[kLayers], NpadT[kLayers], KpadT[kLayers];
         bf16* wf[kLayers];
         bf16* wt[kLayers];
@@ -404,7 +407,7 @@ namespace
         int L = 0;
         while(L + 1 < kLayers && i >= T.off[L + 1])
             ++L;
-        const int ks = T.ks[L], cin = T.cin[L], cout = T.cout[L];
+        const int ks = T.ks[L], cin = T.cin[L], cout = T.cout[L], cg = T.cg[L];
         const int taps = ks * ks;
         const int o = i - T.off[L];
         const int nw = cout * taps * cin;
@@ -417,7 +420,7 @@ namespace
             t = r / cin;
             ci = r - t * cin;
             if(T.dw[L])
-                g = T.dw[L][size_t(t * cin + ci) * T.Npad[L] + co];
+                g = T.dw[L][size_t(t * cg + ci) * T.Npad[L] + co];
         }
         else
         {
@@ -443,7 +446,7 @@ namespace
         if(o < nw)
         {
             const bf16 pb = __float2bfloat16_rn(p);
-            T.wf[L][size_t(co) * T.Kpad[L] + t * cin + ci] = pb;
+            T.wf[L][size_t(co) * T.Kpad[L] + t * cg + ci] = pb;
             if(T.wt[L])
                 T.wt[L][size_t(ci) * T.KpadT[L] + t * cout + co] = pb;
         }
@@ -555,7 +558,7 @@ namespace
         p.B = B;
         p.H = R->lh[li];
         p.W = R->lw[li];
-        p.Cg = d.cin;
+        p.Cg = R->T.cg[L];
         p.Ho = R->lh[lo];
         p.Wo = R->lw[lo];
         p.Cout = d.cout;
@@ -601,7 +604,7 @@ namespace
         bool has[kLayers] = {};
         for(int L = 0; L < kLayers; ++L)
         {
-            cudaMemsetAsync(R->dw[L], 0, size_t(kDefs[L].ks * kDefs[L].ks * kDefs[L].cin) * R->T.Npad[L] * sizeof(float), s);
+            cudaMemsetAsync(R->dw[L], 0, size_t(kDefs[L].ks * kDefs[L].ks * R->T.cg[L]) * R->T.Npad[L] * sizeof(float), s);
             cudaMemsetAsync(R->db[L], 0, size_t(kDefs[L].cout) * sizeof(float), s);
         }
         for(int L = kLayers - 1; L >= 0; --L)
@@ -617,7 +620,7 @@ namespace
             wp.B = B;
             wp.H = R->lh[li];
             wp.W = R->lw[li];
-            wp.Cin = d.cin;
+            wp.Cin = R->T.cg[L];
             wp.Ho = R->lh[lo];
             wp.Wo = R->lw[lo];
             wp.Cout = d.cout;
@@ -625,7 +628,7 @@ namespace
             wp.ks = d.ks;
             wp.stride = d.stride;
             wp.pad = d.pad;
-            wp.Mtot = d.ks * d.ks * d.cin;
+            wp.Mtot = d.ks * d.ks * R->T.cg[L];
             wp.errorFlag = R->errorFlag;
             if(!launch_conv_wgrad(wp, s))
                 return false;
@@ -752,16 +755,18 @@ extern "C"
         for(int L = 0; L < kLayers && ok; ++L)
         {
             const LayerDef& d = kDefs[L];
-            const int K = d.ks * d.ks * d.cin, KT = d.ks * d.ks * d.cout;
+            const int cg = round_up(d.cin, 16);
+            const int K = d.ks * d.ks * cg, KT = d.ks * d.ks * d.cout;
             R->T.off[L] = off;
             R->T.ks[L] = d.ks;
             R->T.cin[L] = d.cin;
+            R->T.cg[L] = cg;
             R->T.cout[L] = d.cout;
             R->T.Npad[L] = round_up(d.cout, 16);
             R->T.Kpad[L] = round_up(K, 64);
             R->T.NpadT[L] = round_up(d.cin, 16);
             R->T.KpadT[L] = round_up(KT, 64);
-            off += d.cout * K + d.cout;
+            off += d.cout * d.ks * d.ks * d.cin + d.cout;
             const size_t pix = size_t(R->maxBatch) * mh[kLevel[L]] * mw[kLevel[L]];
             ok = ok && dalloc(R, R->wf[L], size_t(R->T.Npad[L]) * R->T.Kpad[L]);
             ok = ok && (d.src == SRC_X || dalloc(R, R->wt[L], size_t(R->T.NpadT[L]) * R->T.KpadT[L]));
@@ -782,7 +787,7 @@ extern "C"
         R->T.off[kLayers] = off;
         R->total = off;
         const size_t pix0 = size_t(R->maxBatch) * mh[0] * mw[0];
-        ok = ok && dalloc(R, R->dcat, maxCat) && dalloc(R, R->x, pix0 * 8) && dalloc(R, R->r, pix0 * 16);
+        ok = ok && dalloc(R, R->dcat, maxCat) && dalloc(R, R->x, pix0 * 16) && dalloc(R, R->r, pix0 * 16);
         ok = ok && dalloc(R, R->master, size_t(off)) && dalloc(R, R->adamM, size_t(off)) && dalloc(R, R->adamV, size_t(off));
         ok = ok && dalloc(R, R->lossSum, 1) && dalloc(R, R->gradHost, size_t(off)) && dalloc(R, R->sqErr, 1) && dalloc(R, R->errorFlag, 1);
         if(!ok)

@@ -29,6 +29,7 @@
 #include "isaacb_tc.cuh"
 
 #include <cuda_bf16.h>
+#include <algorithm>
 #include <string>
 
 namespace isaacb
@@ -327,6 +328,281 @@ namespace isaacb
                 tc::tmem_dealloc(tmem, cols);
         }
 
+        // ------------------------------------------------------------------ row tiles
+        // Convolutions of stride 1 (forward, or the input gradient with `transposed`) or
+        // stride 2 (forward) whose gathered channel count is a multiple of 16.  A tile is
+        // 128 consecutive output pixels of one image row.  Its input rows (ks of them)
+        // are loaded into shared memory once, channel chunks of 8 stored as separate
+        // runs of 16-byte pixels; for stride 2 each run is split into its even and odd
+        // input columns.  Every tap then reads the same halo through a descriptor whose
+        // start is shifted by the tap's column offset: the no-swizzle core matrix is 8
+        // consecutive 16-byte rows, and consecutive output pixels are consecutive
+        // entries of a run (of a parity plane for stride 2).  Warp roles:
+        //   warps 0-3  epilogue (TMEM lane = pixel), double-buffered accumulators
+        //   warps 4-7  producers: cp.async of the halo, arrival on the stage's mbarrier
+        //   warp 8     one thread issues the MMAs and commits them
+        constexpr int kRowThreads = 288;
+
+        struct RowGeom
+        {
+            int S; // stride: 1 or 2
+            int HWp; // entries per run (per parity plane for stride 2)
+            int stages; // halo buffers: 1 or 2
+        };
+
+        __host__ __device__ inline RowGeom row_geom(int stride, int ks, int pad, int stages)
+        {
+            RowGeom g;
+            g.S = stride;
+            g.HWp = stride == 1 ? kTileM + 2 * pad : kTileM + (ks - 1) / 2 + 1;
+            g.stages = stages;
+            return g;
+        }
+
+        __global__ void __launch_bounds__(kRowThreads, 1) k_conv_row(const __grid_constant__ ConvGemmParams p, const RowGeom rg)
+        {
+            extern __shared__ unsigned char dsm[];
+            __shared__ uint32_t sTmem;
+            __shared__ __align__(8) uint64_t sFull[2];
+            __shared__ __align__(8) uint64_t sEmpty[2];
+            __shared__ __align__(8) uint64_t sAccFull[2];
+            __shared__ __align__(8) uint64_t sAccEmpty[2];
+            __shared__ __align__(8) uint64_t sDrain;
+            unsigned char* base = dsm + ((128u - (tc::smem_addr(dsm) & 127u)) & 127u);
+            const uint32_t sB = tc::smem_addr(base);
+            const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+            const int pad = p.pad, ks = p.ks, S = rg.S, HWp = rg.HWp, NS = rg.stages;
+            const int nC = p.Cg / 8;
+            const uint32_t runBytes = uint32_t(HWp) * 16u;
+            const uint32_t haloBytes = uint32_t(ks * nC * S) * runBytes;
+            const uint32_t sH = sB + uint32_t(p.Npad) * uint32_t(p.Kpad) * 2u;
+            const uint32_t half = tmem_columns(p.Npad);
+            const uint32_t cols = 2 * half;
+            if(warp == 0)
+            {
+                tc::tmem_alloc(&sTmem, cols);
+                tc::tmem_relinquish();
+            }
+            if(tid == 0)
+            {
+                for(int s = 0; s < 2; ++s)
+                {
+                    tc::mbar_init(&sFull[s], 128);
+                    tc::mbar_init(&sEmpty[s], 1);
+                    tc::mbar_init(&sAccFull[s], 1);
+                    tc::mbar_init(&sAccEmpty[s], 128);
+                }
+                tc::mbar_init(&sDrain, 1);
+                tc::mbar_init_fence();
+            }
+            {
+                const int kb = p.Kpad / 8;
+                const int pieces = p.Npad * kb;
+                for(int i = tid; i < pieces; i += kRowThreads)
+                {
+                    const int n = i / kb, k8 = i - n * kb;
+                    const uint32_t dst = sB + uint32_t(n >> 3) * uint32_t(p.Kpad) * 16u + uint32_t(k8) * 128u + uint32_t(n & 7) * 16u;
+                    tc::cp_async16(dst, p.w + size_t(n) * p.Kpad + size_t(k8) * 8, 16);
+                }
+                tc::cp_async_commit();
+                tc::cp_async_wait<0>();
+                tc::fence_async_smem();
+            }
+            tc::fence_before_sync();
+            __syncthreads();
+            tc::fence_after_sync();
+            const uint32_t tmem = sTmem;
+            const int tilesPerRow = (p.Wo + kTileM - 1) / kTileM;
+            const int nTiles = p.B * p.Ho * tilesPerRow;
+
+            if(warp >= 4 && warp < 8)
+            {
+                // producers: entry (ty, chunk j, parity q, idx) holds input column S*x0 - pad + S*idx + q
+                const int pt = tid - 128;
+                const int dj = 128 % nC, dc = 128 / nC;
+                int i = 0;
+                for(int tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++i)
+                {
+                    const int s = i % NS, n = i / NS;
+                    if(n >= 1 && !tc::mbar_wait(&sEmpty[s], uint32_t(n - 1) & 1u))
+                    {
+                        if(p.errorFlag)
+                            atomicExch(p.errorFlag, 1);
+                        break;
+                    }
+                    const int xt = tile % tilesPerRow;
+                    const int row = tile / tilesPerRow;
+                    const int y = row % p.Ho, b = row / p.Ho;
+                    const int x0 = xt * kTileM;
+                    const uint32_t st = sH + uint32_t(s) * haloBytes;
+                    // flat index g = (c * nC + j) within one halo row, c = S*idx + q the input column
+                    // offset; consecutive threads take consecutive 16-byte pieces of global memory and
+                    // step by 128 pieces, so j and c advance by fixed amounts
+                    const int perRow = nC * S * HWp;
+                    for(int ty = 0; ty < ks; ++ty)
+                    {
+                        const int iy = p.transposed ? y + pad - ty : S * y - pad + ty;
+                        const bool rowOk = iy >= 0 && iy < p.H;
+                        const bf16* rowPtr = p.x + (size_t(b) * p.H + (rowOk ? iy : 0)) * p.W * p.Cg;
+                        const uint32_t rowBase = st + uint32_t(ty * nC * S) * runBytes;
+                        int j = pt % nC, c = pt / nC;
+                        for(int g = pt; g < perRow; g += 128)
+                        {
+                            const int ix = S * x0 - pad + c;
+                            const int q = c & (S - 1), idx = S == 1 ? c : (c >> 1);
+                            const bool ok = rowOk && ix >= 0 && ix < p.W;
+                            const bf16* src = ok ? rowPtr + size_t(ix) * p.Cg + j * 8 : p.x;
+                            tc::cp_async16(rowBase + uint32_t(j * S + q) * runBytes + uint32_t(idx) * 16u, src, ok ? 16u : 0u);
+                            j += dj;
+                            c += dc;
+                            if(j >= nC)
+                            {
+                                j -= nC;
+                                ++c;
+                            }
+                        }
+                    }
+                    tc::cp_async_arrive(&sFull[s]);
+                }
+                tc::cp_async_wait<0>();
+            }
+            else if(warp == 8)
+            {
+                if(lane == 0)
+                {
+                    const uint32_t idesc = tc::idesc_bf16(kTileM, p.Npad, false, false);
+                    const uint32_t lboA = uint32_t(S) * runBytes;
+                    const uint32_t sboB = uint32_t(p.Kpad) * 16u;
+                    int i = 0;
+                    for(int tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++i)
+                    {
+                        const int s = i % NS, n = i / NS;
+                        const int a = i & 1, na = i >> 1;
+                        if(!tc::mbar_wait(&sFull[s], uint32_t(n) & 1u)
+                           || (na >= 1 && !tc::mbar_wait(&sAccEmpty[a], uint32_t(na - 1) & 1u)))
+                        {
+                            if(p.errorFlag)
+                                atomicExch(p.errorFlag, 1);
+                            break;
+                        }
+                        tc::fence_async_smem();
+                        tc::fence_after_sync();
+                        const uint32_t st = sH + uint32_t(s) * haloBytes;
+                        const uint32_t d = tmem + uint32_t(a) * half;
+                        // descriptors differ only in their start field (16-byte units), so the
+                        // loop adds offsets to two base descriptors
+                        const uint64_t aBase = tc::smem_desc(st, lboA, 128u);
+                        const uint64_t bBase = tc::smem_desc(sB, 128u, sboB);
+                        uint32_t acc = 0;
+                        for(int ty = 0; ty < ks; ++ty)
+                            for(int tx = 0; tx < ks; ++tx)
+                            {
+                                const int col = p.transposed ? 2 * pad - tx : tx;
+                                const int q = col & (S - 1), idx0 = S == 1 ? col : (col >> 1);
+                                uint32_t aOff = uint32_t((ty * nC * S + q) * HWp + idx0);
+                                uint32_t bOff = uint32_t((ty * ks + tx) * p.Cg);
+                                for(int jp = 0; jp < nC / 2; ++jp)
+                                {
+                                    tc::mma_bf16(d, aBase + aOff, bBase + bOff, idesc, acc);
+                                    acc = 1;
+                                    aOff += uint32_t(2 * S * HWp);
+                                    bOff += 16u;
+                                }
+                            }
+                        tc::mma_commit(&sEmpty[s]);
+                        tc::mma_commit(&sAccFull[a]);
+                    }
+                    // every MMA of this CTA has completed before TMEM is released
+                    tc::mma_commit(&sDrain);
+                    tc::mbar_wait(&sDrain, 0);
+                }
+                __syncwarp();
+            }
+            else
+            {
+                // epilogue: thread = TMEM lane = pixel of the tile
+                const uint32_t lane0 = uint32_t(warp) * 32u;
+                int i = 0;
+                for(int tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++i)
+                {
+                    const int a = i & 1;
+                    if(!tc::mbar_wait(&sAccFull[a], uint32_t(i >> 1) & 1u))
+                    {
+                        if(p.errorFlag)
+                            atomicExch(p.errorFlag, 1);
+                        break;
+                    }
+                    tc::fence_after_sync();
+                    const int xt = tile % tilesPerRow;
+                    const int row = tile / tilesPerRow;
+                    const int x = xt * kTileM + tid;
+                    const bool valid = x < p.Wo;
+                    const size_t pix = size_t(row) * p.Wo + x;
+                    for(int c0 = 0; c0 < p.Npad; c0 += 8)
+                    {
+                        float v[8];
+                        tc::tmem_ld8(tmem + uint32_t(a) * half + (lane0 << 16) + uint32_t(c0), v);
+                        tc::tmem_wait_ld();
+                        if(!valid || c0 >= p.Cout)
+                            continue;
+                        const size_t o = pix * p.Cout + c0;
+                        if(p.bias)
+                        {
+#pragma unroll
+                            for(int k = 0; k < 8; ++k)
+                                v[k] += __ldg(p.bias + c0 + k);
+                        }
+                        if(p.relu)
+                        {
+#pragma unroll
+                            for(int k = 0; k < 8; ++k)
+                                v[k] = fmaxf(v[k], 0.0f);
+                        }
+                        if(p.mask)
+                        {
+                            float mk[8];
+                            unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(p.mask + o)), mk);
+#pragma unroll
+                            for(int k = 0; k < 8; ++k)
+                                v[k] = mk[k] > 0.0f ? v[k] : 0.0f;
+                        }
+                        if(p.yf)
+                        {
+                            float4* dst = reinterpret_cast<float4*>(p.yf + o);
+                            if(p.accumulate)
+                            {
+                                const float4 u = dst[0], w = dst[1];
+                                v[0] += u.x, v[1] += u.y, v[2] += u.z, v[3] += u.w;
+                                v[4] += w.x, v[5] += w.y, v[6] += w.z, v[7] += w.w;
+                            }
+                            dst[0] = make_float4(v[0], v[1], v[2], v[3]);
+                            dst[1] = make_float4(v[4], v[5], v[6], v[7]);
+                        }
+                        else
+                        {
+                            uint4* dst = reinterpret_cast<uint4*>(p.y + o);
+                            if(p.accumulate)
+                            {
+                                float u[8];
+                                unpack_bf16x8(*dst, u);
+#pragma unroll
+                                for(int k = 0; k < 8; ++k)
+                                    v[k] += u[k];
+                            }
+                            *dst = pack_bf16x8(v);
+                        }
+                    }
+                    tc::fence_before_sync();
+                    tc::mbar_arrive(&sAccEmpty[a]);
+                }
+            }
+            tc::fence_before_sync();
+            __syncthreads();
+            tc::fence_after_sync();
+            if(warp == 0)
+                tc::tmem_dealloc(tmem, cols);
+        }
+
         // ------------------------------------------------------------------ weight gradient
         __global__ void __launch_bounds__(kThreads, 1) k_conv_wgrad(const __grid_constant__ WgradParams p)
         {
@@ -514,19 +790,71 @@ namespace isaacb
         return size_t(kStages) * (kStageBytesA + size_t(Npad) * 128) + 128;
     }
 
+    // CTAs of `kernel` that fit on one SM with `threads` threads and `dynSmem` bytes of
+    // dynamic shared memory (registers, threads, shared memory; at most 4)
+    template<class K>
+    int ctas_per_sm(K kernel, int threads, size_t dynSmem)
+    {
+        cudaFuncAttributes fa{};
+        int dev = 0, smemSm = 0, reserved = 0, regsSm = 0, thrSm = 0;
+        if(cudaFuncGetAttributes(&fa, kernel) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess)
+            return 1;
+        cudaDeviceGetAttribute(&smemSm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+        cudaDeviceGetAttribute(&regsSm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&thrSm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+        const size_t perCta = dynSmem + fa.sharedSizeBytes + size_t(reserved);
+        int n = perCta ? int(size_t(smemSm) / perCta) : 4;
+        const int warps = (threads + 31) / 32;
+        const int regsPerWarp = ((fa.numRegs * 32 + 255) / 256) * 256;
+        if(regsPerWarp > 0)
+            n = std::min(n, regsSm / (regsPerWarp * warps));
+        n = std::min(n, thrSm / (warps * 32));
+        return std::max(1, std::min(n, 4));
+    }
+
+    bool row_tiles_apply(const ConvGemmParams& p)
+    {
+        return p.Cg % 16 == 0 && p.Npad <= 256
+            && ((p.stride == 1 && 2 * p.pad == p.ks - 1) || (p.stride == 2 && !p.transposed && p.ks <= 3 && p.pad <= 1));
+    }
+    size_t conv_row_smem(const ConvGemmParams& p, int stages)
+    {
+        const RowGeom g = row_geom(p.stride, p.ks, p.pad, stages);
+        return size_t(p.Npad) * p.Kpad * 2 + size_t(stages) * p.ks * (p.Cg / 8) * g.S * g.HWp * 16 + 128;
+    }
+
     bool launch_conv_gemm(const ConvGemmParams& p, cudaStream_t s)
     {
+        if(row_tiles_apply(p))
+        {
+            int stages = 2;
+            if(conv_row_smem(p, 2) > 227 * 1024)
+                stages = 1;
+            if(conv_row_smem(p, stages) <= 227 * 1024)
+            {
+                const size_t smem = conv_row_smem(p, stages);
+                cudaFuncSetAttribute(k_conv_row, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+                cudaFuncSetAttribute(k_conv_row, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+                const int tiles = p.B * p.Ho * ((p.Wo + kTileM - 1) / kTileM);
+                int perSm = ctas_per_sm(k_conv_row, kRowThreads, smem);
+                while(perSm > 1 && perSm * 2 * int(tmem_columns(p.Npad)) > 512)
+                    --perSm;
+                const int slots = num_sms() * perSm;
+                k_conv_row<<<tiles < slots ? tiles : slots, kRowThreads, smem, s>>>(p, row_geom(p.stride, p.ks, p.pad, stages));
+                return true;
+            }
+        }
         const size_t smem = conv_gemm_smem(p.Npad, p.Kpad);
         if(smem > 227 * 1024)
             return false;
         cudaFuncSetAttribute(k_conv_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaFuncSetAttribute(k_conv_gemm, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         const int P = p.B * p.Ho * p.Wo;
         const int tiles = (P + kTileM - 1) / kTileM;
         // as many persistent CTAs as fit on an SM (shared memory and TMEM permitting), so one
         // CTA's epilogue and gathers overlap another's MMAs
-        int perSm = 1;
-        if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_conv_gemm, kThreads, smem) != cudaSuccess || perSm < 1)
-            perSm = 1;
+        int perSm = ctas_per_sm(k_conv_gemm, kThreads, smem);
         while(perSm > 1 && perSm * int(tmem_columns(p.Npad)) > 512)
             --perSm;
         const int slots = num_sms() * perSm;
@@ -541,6 +869,7 @@ namespace isaacb
         if(smem > 227 * 1024)
             return false;
         cudaFuncSetAttribute(k_conv_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaFuncSetAttribute(k_conv_wgrad, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         const int P = p.B * p.Ho * p.Wo;
         const int nChunks = (P + kChunkK - 1) / kChunkK;
         const int mTiles = (p.Mtot + kTileM - 1) / kTileM;

@@ -49,6 +49,9 @@ CASES = [
     (2, 14, 13, 224, 96, 1, 1, 0),
     (1, 16, 16, 32, 16, 1, 1, 0),
     (2, 120, 90, 32, 32, 3, 1, 1),  # more tiles than SMs: several tiles per CTA
+    (1, 40, 300, 16, 32, 3, 1, 1),  # rows of 2 full and 1 ragged 128-pixel tiles
+    (1, 33, 290, 32, 64, 3, 2, 1),  # stride 2 on row tiles, ragged
+    (2, 31, 260, 64, 64, 3, 1, 1),
 ]
 
 
