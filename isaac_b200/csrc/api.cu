@@ -570,6 +570,10 @@ namespace
         }
         p.tileBytes = bytes;
         p.txBytes = tx;
+        p.scalarIdem = 1;
+        for(int s = 0; s < c->nVol; ++s)
+            if(c->weight[s] + c->iso[s] > 0.0f && !(p.fdim[s] == 1 && p.chainIdem[s]))
+                p.scalarIdem = 0;
         if(bytes == 0 || bytes > 160 * 1024)
             p.useTma = 0;
     }

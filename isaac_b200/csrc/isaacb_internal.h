@@ -2,6 +2,8 @@
 // kernel translation units.  Not installed; not part of the C ABI.
 #pragma once
 
+#include <algorithm>
+
 #include "isaacb_device.cuh"
 
 #include <cstdint>
@@ -28,6 +30,7 @@ namespace isaacb
         float totalWeight;
         float invTotalWeight; // 2^-k when totalWeight == 2^k exactly, else 0
         int32_t nonNegative; // every colour sum is finite and >= 0 (tables and weights >= 0, total > 0)
+        int32_t scalarIdem; // every active source is scalar with an all-idem chain
         uint4* volQ; // combined volume, quad bricks
         uint32_t* isoAQ; // combined iso alpha, quad bricks
         uint32_t* isoLin; // combined iso RGBA8, linear
@@ -43,6 +46,29 @@ namespace isaacb
         int32_t txBytes; // bytes the TMA boxes deliver (the mbarrier's transaction count)
         alignas(64) CUtensorMap tmap[kMaxSources];
     };
+    // CTAs of `kernel` that fit on one SM with `threads` threads and `dynSmem` bytes of
+    // dynamic shared memory (registers, threads, shared memory; at most 4)
+    template<class K>
+    inline int ctas_per_sm(K kernel, int threads, size_t dynSmem)
+    {
+        cudaFuncAttributes fa{};
+        int dev = 0, smemSm = 0, reserved = 0, regsSm = 0, thrSm = 0;
+        if(cudaFuncGetAttributes(&fa, kernel) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess)
+            return 1;
+        cudaDeviceGetAttribute(&smemSm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+        cudaDeviceGetAttribute(&regsSm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&thrSm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+        const size_t perCta = dynSmem + fa.sharedSizeBytes + size_t(reserved);
+        int n = perCta ? int(size_t(smemSm) / perCta) : 4;
+        const int warps = (threads + 31) / 32;
+        const int regsPerWarp = ((fa.numRegs * 32 + 255) / 256) * 256;
+        if(regsPerWarp > 0)
+            n = std::min(n, regsSm / (regsPerWarp * warps));
+        n = std::min(n, thrSm / (warps * 32));
+        return std::max(1, std::min(n, 4));
+    }
+
     void launch_merge(const MergeParams& p, cudaStream_t s);
 
     // per-source renderer bricks: persistent sources keep their raw components,

@@ -127,15 +127,38 @@ namespace isaacb
                 : "memory");
             return done != 0;
         }
-        // bounded wait for the phase with the given parity to complete: false after about 0.5 s
+        // one potentially blocking probe: the thread is suspended until the phase completes
+        // or a hardware time limit passes, so waiting warps take no issue slots
+        __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity)
+        {
+            uint32_t done;
+            asm volatile(
+                "{\n\t.reg .pred P;\n\tmbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\tselp.u32 %0, 1, 0, P;\n\t}\n"
+                : "=r"(done)
+                : "r"(smem_addr(bar)), "r"(parity)
+                : "memory");
+            return done != 0;
+        }
+        __device__ __forceinline__ uint64_t global_ns()
+        {
+            uint64_t t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            return t;
+        }
+        // bounded wait for the phase with the given parity to complete: false once about one
+        // second of wall time has passed (checked between probes, whatever each probe's own
+        // suspension limit is) or after 2^26 probes, whichever comes first
         __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
         {
-            for(int it = 0; it < (1 << 22); ++it)
+            if(mbar_try(bar, parity))
+                return true;
+            const uint64_t t0 = global_ns();
+            for(int it = 0; it < (1 << 26); ++it)
             {
-                if(mbar_test(bar, parity))
+                if(mbar_try(bar, parity))
                     return true;
-                if(it > 64)
-                    __nanosleep(64);
+                if(global_ns() - t0 > 1000000000ull)
+                    return false;
             }
             return false;
         }

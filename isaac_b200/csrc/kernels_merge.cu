@@ -243,6 +243,102 @@ namespace isaacb
         }
     }
 
+    // merge_brick for the common case of scalar sources with all-idem chains staged by
+    // TMA: one tile offset per texel serves every source, the value is one shared-memory
+    // load, and the source loop has no per-source layout arithmetic.  Same operations in
+    // the same order as merge_brick, so the bytes are identical.
+    template<bool ISO>
+    __device__ __forceinline__ void merge_brick_scalar(
+        const MergeParams& p,
+        int bx,
+        int by,
+        int bz,
+        uint32_t* volS,
+        uint32_t* isoS,
+        int& anyVol,
+        int& myIsoMax,
+        const uint8_t* mask,
+        const unsigned char* tiles,
+        int x0,
+        int y0,
+        int z0)
+    {
+        constexpr int kPer = 3;
+        constexpr int kTex = kApron * kApron * kApron;
+        const Geom& g = p.g;
+        int xs[kPer], ys[kPer], zs[kPer], off[kPer];
+        float4 vc[kPer], ic[kPer];
+#pragma unroll
+        for(int j = 0; j < kPer; ++j)
+        {
+            const int t = min(int(threadIdx.x) + 256 * j, kTex - 1);
+            const int lz = t / (kApron * kApron);
+            const int r = t - lz * (kApron * kApron);
+            const int ly = r / kApron, lx = r - ly * kApron;
+            xs[j] = iclamp(bx * 8 - 1 + lx, 0, g.ls[0] - 1);
+            ys[j] = iclamp(by * 8 - 1 + ly, 0, g.ls[1] - 1);
+            zs[j] = iclamp(bz * 8 - 1 + lz, 0, g.ls[2] - 1);
+            off[j] = ((zs[j] - z0) * kApron + (ys[j] - y0)) * 16 + (xs[j] - x0);
+            vc[j] = make_float4(0, 0, 0, 0);
+            ic[j] = make_float4(0, 0, 0, 0);
+        }
+        const int nMine = int(threadIdx.x) + 512 < kTex ? 3 : 2;
+        const int ts = p.ts;
+        for(int s = 0; s < p.nVol; ++s)
+        {
+            const float vw = p.weight[s];
+            const float it = p.iso[s];
+            if(!(vw + it > 0.0f))
+                continue;
+            const float* tile = reinterpret_cast<const float*>(tiles + p.tileOffset[s]);
+            const float4* lut = p.lut + size_t(s) * ts;
+#pragma unroll
+            for(int j = 0; j < kPer; ++j)
+            {
+                if(j >= nMine)
+                    break;
+                const float4 c = __ldg(lut + lut_index_fast(tile[off[j]], ts));
+                if(vw > 0.0f)
+                {
+                    const float a = c.w * vw;
+                    vc[j].x += c.x * a;
+                    vc[j].y += c.y * a;
+                    vc[j].z += c.z * a;
+                    vc[j].w += a;
+                }
+                if(ISO && it > 0.0f)
+                {
+                    const float a = c.w / it * 0.5f;
+                    if(ic[j].w < a)
+                        ic[j] = make_float4(c.x, c.y, c.z, a);
+                }
+            }
+        }
+#pragma unroll
+        for(int j = 0; j < kPer; ++j)
+        {
+            if(j >= nMine)
+                break;
+            const int t = int(threadIdx.x) + 256 * j;
+            float4 c = vc[j];
+            if(p.invTotalWeight != 0.0f)
+                c = make_float4(c.x * p.invTotalWeight, c.y * p.invTotalWeight, c.z * p.invTotalWeight, c.w * p.invTotalWeight);
+            else
+                c = make_float4(c.x / p.totalWeight, c.y / p.totalWeight, c.z / p.totalWeight, c.w / p.totalWeight);
+            const uint32_t vb = p.nonNegative ? dither_rgba_nonneg(p.ditherMode, mask, xs[j], ys[j], zs[j], c)
+                                              : dither_rgba(p.ditherMode, mask, xs[j], ys[j], zs[j], c);
+            volS[t] = vb;
+            anyVol |= vb != 0u;
+            if(ISO)
+            {
+                const float4 q = ic[j];
+                const uint32_t ib = round_byte(q.x) | (round_byte(q.y) << 8) | (round_byte(q.z) << 16) | (round_byte(q.w) << 24);
+                isoS[t] = ib;
+                myIsoMax = max(myIsoMax, int(ib >> 24));
+            }
+        }
+    }
+
     // voxel readers of merge_brick: the TMA-staged tile in shared memory, or global memory
     struct TileFetch
     {
@@ -348,7 +444,10 @@ namespace isaacb
         int myIsoMax = 0;
         if(TMA)
         {
-            merge_brick<ISO>(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, sMask, TileFetch{p, tiles, x0, y0, z0});
+            if(p.scalarIdem)
+                merge_brick_scalar<ISO>(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, sMask, tiles, x0, y0, z0);
+            else
+                merge_brick<ISO>(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, sMask, TileFetch{p, tiles, x0, y0, z0});
         }
         else
         {

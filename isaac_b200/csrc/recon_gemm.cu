@@ -790,29 +790,6 @@ namespace isaacb
         return size_t(kStages) * (kStageBytesA + size_t(Npad) * 128) + 128;
     }
 
-    // CTAs of `kernel` that fit on one SM with `threads` threads and `dynSmem` bytes of
-    // dynamic shared memory (registers, threads, shared memory; at most 4)
-    template<class K>
-    int ctas_per_sm(K kernel, int threads, size_t dynSmem)
-    {
-        cudaFuncAttributes fa{};
-        int dev = 0, smemSm = 0, reserved = 0, regsSm = 0, thrSm = 0;
-        if(cudaFuncGetAttributes(&fa, kernel) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess)
-            return 1;
-        cudaDeviceGetAttribute(&smemSm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
-        cudaDeviceGetAttribute(&regsSm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
-        cudaDeviceGetAttribute(&thrSm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
-        const size_t perCta = dynSmem + fa.sharedSizeBytes + size_t(reserved);
-        int n = perCta ? int(size_t(smemSm) / perCta) : 4;
-        const int warps = (threads + 31) / 32;
-        const int regsPerWarp = ((fa.numRegs * 32 + 255) / 256) * 256;
-        if(regsPerWarp > 0)
-            n = std::min(n, regsSm / (regsPerWarp * warps));
-        n = std::min(n, thrSm / (warps * 32));
-        return std::max(1, std::min(n, 4));
-    }
-
     bool row_tiles_apply(const ConvGemmParams& p)
     {
         return p.Cg % 16 == 0 && p.Npad <= 256

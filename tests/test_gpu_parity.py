@@ -47,6 +47,27 @@ def test_merge_textures_bit_exact(dither, iso):
     assert np.array_equal(gi, ri)
 
 
+@pytest.mark.parametrize("dither", [0, 1, 2])
+@pytest.mark.parametrize("iso", [False, True])
+@pytest.mark.parametrize("weights", [(2.0, 2.0, 2.0, 2.0), (1.0, 0.0, 3.5, 0.25)])
+def test_merge_scalar_sources_bit_exact(dither, iso, weights):
+    """Scalar sources with all-idem chains take the specialised merge."""
+    fields = scenes.precision_scene(27)
+    s = Scene(n=(27, 27, 27), volumes=[(f.numpy(), True) for f in fields], dither_mode=dither)
+    s.transfer = [scenes.transfer_4point(0.7 * i) for i in range(4)]
+    s.weights = list(weights)
+    if iso:
+        s.iso = [0.0, 0.45, 0.0, 0.3]
+    o = build_oracle(s)
+    o.update()
+    rv, ri = o.combined()
+    viz = build_gpu(s)
+    viz.update()
+    gv, gi = viz.combinedTextures()
+    assert np.array_equal(gv, rv)
+    assert np.array_equal(gi, ri)
+
+
 def test_merge_weights_and_zero_total():
     s = gaussian_pair(n=16, weights=[0.0, 3.5])
     o = build_oracle(s)
