@@ -418,6 +418,177 @@ namespace isaacb
             count_warp(p.counters, n);
     }
 
+    // Weighted sources of a frame, in source order (zero weights dropped): the
+    // specialised kernel below keeps their pointers and weights in registers.
+    struct ActiveSources
+    {
+        int n;
+        int idx[kMaxSources];
+        const void* bricks[kMaxSources];
+        float weight[kMaxSources];
+    };
+
+    // a*(1-o) + b*o on two lanes (two sources), each lane rounded exactly like lin()
+    __device__ __forceinline__ f2p lin2(f2p omo, f2p o, f2p a, f2p b)
+    {
+        return f2p_add(f2p_mul(a, omo), f2p_mul(b, o));
+    }
+
+    // k_shade_volume_per_source_scalar for 1..4 weighted sources known at compile time:
+    // the sources' quads are all loaded before any is used, pairs of sources share packed
+    // FP32 trilinear arithmetic (two lanes, the scalar roundings), and with IDEM the
+    // functor chain is skipped.  Same operations in the same order per source, so the
+    // frame is bit-identical to the general kernels'.
+    template<int DT, bool LINEAR, int NS, bool IDEM>
+    __global__ void __launch_bounds__(256) k_shade_volume_per_source_n(
+        const __grid_constant__ FrameParams p,
+        const __grid_constant__ ActiveSources act)
+    {
+        int px, py;
+        thread_pixel(px, py);
+        unsigned long long n = 0;
+        if(px < p.v.W && py < p.v.H)
+        {
+            const size_t o = size_t(py) * p.v.W + px;
+            shade_pixel(p, px, py, o);
+            Ray ray = pixel_to_ray(p.v, p.g, px, py);
+            if(clip_ray(ray, p.v, p.g))
+            {
+                ray.endDepth = gmin(ray.endDepth, p.depth[o]);
+                if(!(ray.endDepth <= ray.startDepth))
+                {
+                    March m = march_setup(ray, p.g, p.v.scale, p.step);
+                    legacy_bounds(p.g, m);
+                    const Geom& g = p.g;
+                    const void* br[NS];
+                    float wt[NS];
+                    const float4* lut[NS];
+#pragma unroll
+                    for(int k = 0; k < NS; ++k)
+                    {
+                        br[k] = act.bricks[k];
+                        wt[k] = act.weight[k];
+                        lut[k] = p.lut + size_t(act.idx[k]) * p.ts;
+                    }
+                    float4 value = make_float4(0, 0, 0, 0);
+                    float4 color = make_float4(0, 0, 0, 0);
+                    for(int i = m.startSteps; i <= m.endSteps; i++)
+                    {
+                        ++n;
+                        const float3 pos = march_pos(m, i);
+                        uint32_t q0;
+                        float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+                        if(LINEAR)
+                        {
+                            const float cx = pos.x - 0.5f, cy = pos.y - 0.5f, cz = pos.z - 0.5f;
+                            fx = cx - floorf(cx);
+                            fy = cy - floorf(cy);
+                            fz = cz - floorf(cz);
+                            const int ix = iclamp(f2i(cx), -1, g.ls[0] - 1);
+                            const int iy = iclamp(f2i(cy), -1, g.ls[1] - 1);
+                            const int iz = iclamp(f2i(cz), -1, g.ls[2] - 1);
+                            q0 = uint32_t(brick_slot(g, ix, iy, iz));
+                        }
+                        else
+                        {
+                            const int ix = iclamp(f2i(pos.x), 0, g.ls[0] - 1);
+                            const int iy = iclamp(f2i(pos.y), 0, g.ls[1] - 1);
+                            const int iz = iclamp(f2i(pos.z), 0, g.ls[2] - 1);
+                            q0 = uint32_t(brick_slot(g, ix, iy, iz));
+                        }
+                        float a[NS][4], b[NS][4], val[NS];
+#pragma unroll
+                        for(int k = 0; k < NS; ++k)
+                        {
+                            load_quad<DT>(br[k], q0, a[k]);
+                            if(LINEAR)
+                                load_quad<DT>(br[k], q0 + 64u, b[k]);
+                        }
+                        if(LINEAR)
+                        {
+                            const f2p omz = f2p_make(1.0f - fz, 1.0f - fz), vz = f2p_make(fz, fz);
+                            const f2p omy = f2p_make(1.0f - fy, 1.0f - fy), vy = f2p_make(fy, fy);
+                            const f2p omx = f2p_make(1.0f - fx, 1.0f - fx), vx = f2p_make(fx, fx);
+#pragma unroll
+                            for(int k = 0; k + 1 < NS; k += 2)
+                            {
+                                // quad order (x0,y0),(x0+1,y0),(x0,y0+1),(x0+1,y0+1); tri_q's lerp tree
+                                const f2p z00 = lin2(omz, vz, f2p_make(a[k][0], a[k + 1][0]), f2p_make(b[k][0], b[k + 1][0]));
+                                const f2p z01 = lin2(omz, vz, f2p_make(a[k][2], a[k + 1][2]), f2p_make(b[k][2], b[k + 1][2]));
+                                const f2p z10 = lin2(omz, vz, f2p_make(a[k][1], a[k + 1][1]), f2p_make(b[k][1], b[k + 1][1]));
+                                const f2p z11 = lin2(omz, vz, f2p_make(a[k][3], a[k + 1][3]), f2p_make(b[k][3], b[k + 1][3]));
+                                const f2p A = lin2(omy, vy, z00, z01);
+                                const f2p B = lin2(omy, vy, z10, z11);
+                                f2p_split(lin2(omx, vx, A, B), val[k], val[k + 1]);
+                            }
+                            if(NS & 1)
+                            {
+                                const int k = NS - 1;
+                                val[k] = tri_q(fx, fy, fz, a[k][0], a[k][1], a[k][2], a[k][3], b[k][0], b[k][1], b[k][2], b[k][3]);
+                            }
+                        }
+                        else
+                        {
+#pragma unroll
+                            for(int k = 0; k < NS; ++k)
+                                val[k] = a[k][0];
+                        }
+#pragma unroll
+                        for(int k = 0; k < NS; ++k)
+                        {
+                            float result = val[k];
+                            if(!IDEM)
+                            {
+                                float v[4] = {val[k], 0.0f, 0.0f, 0.0f};
+                                result = apply_chain(v, 1, p.ps[act.idx[k]].chain);
+                            }
+                            float4 c = __ldg(lut[k] + lut_index_fast(result, p.ts));
+                            c.w *= wt[k];
+                            value.x += c.x * c.w;
+                            value.y += c.y * c.w;
+                            value.z += c.z * c.w;
+                            value.w += c.w;
+                        }
+                        const float oma = 1.0f - color.w;
+                        value = make_float4(value.x * m.factor, value.y * m.factor, value.z * m.factor, value.w * m.factor);
+                        color.x += oma * value.x;
+                        color.y += oma * value.y;
+                        color.z += oma * value.z;
+                        color.w += oma * value.w;
+                        if(color.w > 0.99f)
+                            break;
+                    }
+                    const float4 solid = from_byte4(p.color[o]);
+                    const float r = 1.0f - color.w;
+                    color = make_float4(color.x + r * solid.x, color.y + r * solid.y, color.z + r * solid.z, color.w + r * solid.w);
+                    p.color[o] = to_byte4(color);
+                }
+            }
+        }
+        if(p.counters)
+            count_warp(p.counters, n);
+    }
+
+    template<int DT, bool LINEAR, bool IDEM>
+    void launch_ps_n(const FrameParams& p, const ActiveSources& act, dim3 grid, cudaStream_t s)
+    {
+        switch(act.n)
+        {
+        case 1: k_shade_volume_per_source_n<DT, LINEAR, 1, IDEM><<<grid, 256, 0, s>>>(p, act); break;
+        case 2: k_shade_volume_per_source_n<DT, LINEAR, 2, IDEM><<<grid, 256, 0, s>>>(p, act); break;
+        case 3: k_shade_volume_per_source_n<DT, LINEAR, 3, IDEM><<<grid, 256, 0, s>>>(p, act); break;
+        default: k_shade_volume_per_source_n<DT, LINEAR, 4, IDEM><<<grid, 256, 0, s>>>(p, act); break;
+        }
+    }
+    template<int DT>
+    void launch_ps_dt(const FrameParams& p, const ActiveSources& act, bool lin, bool idem, dim3 grid, cudaStream_t s)
+    {
+        if(lin)
+            idem ? launch_ps_n<DT, true, true>(p, act, grid, s) : launch_ps_n<DT, true, false>(p, act, grid, s);
+        else
+            idem ? launch_ps_n<DT, false, true>(p, act, grid, s) : launch_ps_n<DT, false, false>(p, act, grid, s);
+    }
+
     void launch_shade_volume_per_source(const FrameParams& p, cudaStream_t s)
     {
         dim3 grid((p.v.W + 31) / 32, (p.v.H + 7) / 8);
@@ -435,6 +606,31 @@ namespace isaacb
         if(scalar && dt >= 0)
         {
             const bool lin = p.interpolation != 0;
+            ActiveSources act{};
+            bool idem = true;
+            for(int k = 0; k < p.nVol; ++k)
+            {
+                const PerSourceSrc& S = p.ps[k];
+                if(S.weight == 0.0f)
+                    continue;
+                act.idx[act.n] = k;
+                act.bricks[act.n] = S.bricks;
+                act.weight[act.n] = S.weight;
+                act.n++;
+                idem = idem && S.chain.op[0] == OP_IDEM && S.chain.op[1] == OP_IDEM && S.chain.op[2] == OP_IDEM;
+            }
+            // slot indices of the specialised kernel are 32-bit
+            const bool fits = size_t(p.g.nb[0]) * p.g.nb[1] * p.g.nb[2] * kSlotsPerBrick < (1ull << 31);
+            if(act.n >= 1 && act.n <= 4 && fits)
+            {
+                if(dt == 0)
+                    launch_ps_dt<0>(p, act, lin, idem, grid, s);
+                else if(dt == 1)
+                    launch_ps_dt<1>(p, act, lin, idem, grid, s);
+                else
+                    launch_ps_dt<2>(p, act, lin, idem, grid, s);
+                return;
+            }
             if(dt == 0)
                 lin ? k_shade_volume_per_source_scalar<0, true><<<grid, 256, 0, s>>>(p)
                     : k_shade_volume_per_source_scalar<0, false><<<grid, 256, 0, s>>>(p);

@@ -231,3 +231,31 @@ def inference_flops(h: int, w: int) -> float:
     """Multiply-adds x 2 of one inference on an h x w half-size frame (the convolutions)."""
     hs, ws = level_sizes(h, w)
     return float(sum(2 * k * k * ci * co * hs[l] * ws[l] for k, s, p, ci, co, l in LAYER_SHAPES))
+
+
+def _main(argv=None):
+    """``python -m isaac_b200.recon [--height H --width W --repeat N --weights F]``:
+    inference on a seeded random half-size frame, N times (used for profiling)."""
+    import argparse
+
+    torch = _torch()
+    ap = argparse.ArgumentParser(description=_main.__doc__)
+    ap.add_argument("--height", type=int, default=540)
+    ap.add_argument("--width", type=int, default=960)
+    ap.add_argument("--repeat", type=int, default=3)
+    ap.add_argument("--weights", default=str(WEIGHTS))
+    a = ap.parse_args(argv)
+    net = Reconstructor(1, a.height, a.width, seed=1)
+    if Path(a.weights).exists():
+        net.load(Path(a.weights))
+    g = torch.Generator(device="cuda").manual_seed(1)
+    low = torch.randint(0, 256, (a.height, a.width, 4), dtype=torch.uint8, device="cuda", generator=g)
+    for _ in range(a.repeat):
+        net.infer(low)
+    torch.cuda.synchronize()
+    print("ok", net.error_flag())
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(_main())
