@@ -136,7 +136,7 @@ isaacb_status isaacb_get_transfer(isaacb_ctx* ctx, uint32_t src, float* lut_rgba
 /* Steering setters: "weight" (lib/isaac.hpp:1700-1706), "iso threshold"
  * (:1684-1690), "step" (:1626-1635, raised to 0.01), "interpolation"
  * (:1613-1618), "render optimization" (:1619-1625), "ao" (:1768-1778),
- * "render mode" (:1780-1786), "dither mode" (:1788-1795; modes 0, 1, 2). */
+ * "render mode" (:1780-1786), "dither mode" (:1788-1795; 0 round, 1 ordered 4^3, 2 / 3 / >= 4 blue noise 4^3 / 8^3 / 16^3). */
 isaacb_status isaacb_set_weight(isaacb_ctx* ctx, uint32_t src, float weight);
 isaacb_status isaacb_set_iso_threshold(isaacb_ctx* ctx, uint32_t src, float iso);
 isaacb_status isaacb_set_step(isaacb_ctx* ctx, float step);
@@ -364,6 +364,47 @@ isaacb_status isaacb_recon_error(isaacb_recon* recon, int32_t* flag);
 isaacb_status isaacb_upsample_bilinear2(const uint8_t* low, uint32_t h, uint32_t w, uint8_t* out, void* stream);
 /* Adds the sum of squared byte differences of two RGBA8 images to *sum_dev. */
 isaacb_status isaacb_image_sq_error(const uint8_t* a, const uint8_t* b, uint64_t bytes, unsigned long long* sum_dev, void* stream);
+
+/* ---- Field sources and advection (lib/isaac.hpp:292-370, 499-562, 1819-1850;
+ * lib/isaac/isaac_common_kernel.hpp:334-430, 500-550, 618-686).  The reference
+ * keeps vector fields in a separate source list, merged after the volume sources;
+ * here they are the LAST volume sources (feature_dim 3), flagged with
+ * isaacb_set_field_source.  Each update then swaps the field's two advection
+ * textures, counts the step, advects the texture along the field (noise blended in
+ * by the seeding period / duration) and the merge multiplies the field source's
+ * alpha by the advection texture / 255.  The reference leaves the advection
+ * textures uninitialised; here they start at zero.  Combined renderer only. */
+isaacb_status isaacb_set_field_source(isaacb_ctx* ctx, uint32_t source, int32_t enabled);
+/* "advection step" (factor of the 3-cell maximum step), "advection weight"
+ * (history weight), "advection seeding period", "advection seeding duration",
+ * "seed points" (isaac.hpp:1636-1662); defaults 1, 0.95, 1, 1, 1000. */
+isaacb_status isaacb_set_advection(
+    isaacb_ctx* ctx,
+    float step_factor,
+    float history_weight,
+    int32_t seeding_period,
+    int32_t seeding_duration,
+    int32_t seed_points);
+/* Read back the current advection texture of a field source (local size, x fastest)
+ * and the noise texture (floats); synchronous on `stream`. */
+isaacb_status isaacb_get_advection(isaacb_ctx* ctx, void* stream, uint32_t source, uint8_t* host);
+isaacb_status isaacb_get_noise(isaacb_ctx* ctx, void* stream, float* host);
+
+/* ---- Stereo compositing (lib/isaac/isaac_compositors.hpp:37-116, done on the GPU).
+ * mode 0: out = left (width x height); mode 1: left and right side by side
+ * (2*width x height); mode 2: per pixel (left & left_filter) | (right & right_filter)
+ * on the 32-bit RGBA8 word (bytes R, G, B, A from the low end).  Device frames,
+ * asynchronous on `stream`. */
+isaacb_status isaacb_composite(
+    int32_t mode,
+    const uint8_t* left,
+    const uint8_t* right,
+    uint32_t width,
+    uint32_t height,
+    uint32_t left_filter,
+    uint32_t right_filter,
+    uint8_t* out,
+    void* stream);
 
 /* Number of kernels the last isaacb_update / isaacb_render enqueued. */
 isaacb_status isaacb_get_launch_count(isaacb_ctx* ctx, uint32_t* update_launches, uint32_t* render_launches);

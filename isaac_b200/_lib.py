@@ -183,6 +183,11 @@ SIGNATURES = {
     "isaacb_recon_error": (_i32, [_P, _i32p]),
     "isaacb_upsample_bilinear2": (_i32, [_P, _u32, _u32, _P, _P]),
     "isaacb_image_sq_error": (_i32, [_P, _P, C.c_uint64, _P, _P]),
+    "isaacb_composite": (_i32, [_i32, _P, _P, _u32, _u32, _u32, _u32, _P, _P]),
+    "isaacb_set_field_source": (_i32, [_P, _u32, _i32]),
+    "isaacb_set_advection": (_i32, [_P, _f, _f, _i32, _i32, _i32]),
+    "isaacb_get_advection": (_i32, [_P, _P, _u32, _P]),
+    "isaacb_get_noise": (_i32, [_P, _P, _fp]),
 }
 
 

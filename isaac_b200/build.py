@@ -44,6 +44,7 @@ SOURCES = [
     "kernels_batch.cu",
     "recon_gemm.cu",
     "recon.cu",
+    "composite.cu",
 ]
 
 

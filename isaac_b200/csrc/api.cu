@@ -303,6 +303,16 @@ struct isaacb_ctx
     // TMA tensor maps of the sources, re-encoded when a pointer changes
     CUtensorMap tmap[kMaxSources]{};
     const float* tmapPtr[kMaxSources]{};
+    // field-source advection (defaults of lib/isaac.hpp:606-643); the textures start at zero
+    bool field[kMaxSources]{};
+    uint8_t* adv[kMaxSources]{};
+    uint8_t* advBack[kMaxSources]{};
+    float* noise = nullptr;
+    float* noiseTmp = nullptr;
+    bool noiseDirty = true;
+    float advStepFactor = 1.0f, advHistoryWeight = 0.95f;
+    int advSeedPeriod = 1, advSeedTime = 1, seedPoints = 1000;
+    long long timeStep = 0;
     uint32_t updateLaunches = 0, renderLaunches = 0;
     bool timing = false;
     cudaEvent_t ev[2 * ISAACB_TIMING_SLOTS]{};
@@ -498,6 +508,77 @@ namespace
         return true;
     }
 
+    size_t voxel_count(const isaacb_ctx* c)
+    {
+        return size_t(c->desc.local_size[0]) * c->desc.local_size[1] * c->desc.local_size[2];
+    }
+
+    // Per update with field sources (lib/isaac.hpp:1819-1850): the noise texture when its
+    // seed count changed, the swap of every field source's front and back advection
+    // texture, the step counter, and the advection of each enabled field source.
+    isaacb_status advect_fields(isaacb_ctx* c, cudaStream_t st)
+    {
+        bool any = false;
+        for(int s = 0; s < c->nVol; ++s)
+            any = any || c->field[s];
+        if(!any)
+            return ISAACB_OK;
+        const size_t n = voxel_count(c);
+        if(!c->noise)
+        {
+            ISAACB_CUDA(c, cudaMalloc(&c->noise, n * sizeof(float)), "noise texture");
+            ISAACB_CUDA(c, cudaMalloc(&c->noiseTmp, n * sizeof(float)), "noise texture");
+            c->noiseDirty = true;
+        }
+        NoiseParams np{};
+        np.LX = int(c->desc.local_size[0]);
+        np.LY = int(c->desc.local_size[1]);
+        np.LZ = int(c->desc.local_size[2]);
+        for(int i = 0; i < 3; ++i)
+            np.scale[i] = c->desc.scale[i];
+        np.seedPoints = c->seedPoints;
+        if(c->noiseDirty)
+        {
+            launch_noise(np, c->noise, c->noiseTmp, st);
+            c->noiseDirty = false;
+        }
+        for(int s = 0; s < c->nVol; ++s)
+        {
+            if(!c->field[s])
+                continue;
+            if(!c->adv[s])
+            {
+                ISAACB_CUDA(c, cudaMalloc(&c->adv[s], n), "advection texture");
+                ISAACB_CUDA(c, cudaMalloc(&c->advBack[s], n), "advection texture");
+                ISAACB_CUDA(c, cudaMemsetAsync(c->adv[s], 0, n, st), "advection texture");
+                ISAACB_CUDA(c, cudaMemsetAsync(c->advBack[s], 0, n, st), "advection texture");
+            }
+            std::swap(c->adv[s], c->advBack[s]);
+        }
+        c->timeStep++;
+        for(int s = 0; s < c->nVol; ++s)
+        {
+            if(!c->field[s] || !(c->weight[s] != 0.0f || c->iso[s] != 0.0f))
+                continue;
+            AdvectParams ap{};
+            ap.field = c->src[s];
+            ap.back = c->advBack[s];
+            ap.out = c->adv[s];
+            ap.noise = c->noise;
+            ap.LX = np.LX;
+            ap.LY = np.LY;
+            ap.LZ = np.LZ;
+            for(int i = 0; i < 3; ++i)
+                ap.scale[i] = np.scale[i];
+            ap.stepSize = c->advStepFactor * 3.0f; // ISAAC_MAX_ADVECTION_STEP_SIZE (isaac_defines.hpp:21)
+            ap.historyWeight = c->advHistoryWeight;
+            ap.seedNoise = (c->timeStep % c->advSeedPeriod) >= c->advSeedTime ? 0 : 1;
+            launch_advect(ap, st);
+        }
+        ISAACB_CUDA(c, cudaGetLastError(), "advection");
+        return ISAACB_OK;
+    }
+
     // the merge's launch parameters from a context's state (no launch, no stream work)
     void prepare_merge(isaacb_ctx* c, MergeParams& p)
     {
@@ -572,8 +653,11 @@ namespace
         p.txBytes = tx;
         p.scalarIdem = 1;
         for(int s = 0; s < c->nVol; ++s)
-            if(c->weight[s] + c->iso[s] > 0.0f && !(p.fdim[s] == 1 && p.chainIdem[s]))
+        {
+            p.adv[s] = c->field[s] ? c->adv[s] : nullptr;
+            if(c->weight[s] + c->iso[s] > 0.0f && (!(p.fdim[s] == 1 && p.chainIdem[s]) || c->field[s]))
                 p.scalarIdem = 0;
+        }
         if(bytes == 0 || bytes > 160 * 1024)
             p.useTma = 0;
     }
@@ -742,6 +826,13 @@ extern "C"
         cudaFree(c->mmResult);
         cudaFree(c->mmKeys);
         cudaFree(c->errorFlag);
+        for(int s = 0; s < kMaxSources; ++s)
+        {
+            cudaFree(c->adv[s]);
+            cudaFree(c->advBack[s]);
+        }
+        cudaFree(c->noise);
+        cudaFree(c->noiseTmp);
         cudaFree(c->emptyDev);
         if(c->emptyPinned)
             cudaFreeHost(c->emptyPinned);
@@ -874,11 +965,93 @@ extern "C"
     }
     isaacb_status isaacb_set_dither_mode(isaacb_ctx* c, int32_t m)
     {
-        if(!c || m < 0 || m > 2)
-            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_dither_mode: modes 0, 1 and 2 are supported");
+        // 0 rounding, 1 ordered 4^3, 2 blue noise 4^3, 3 blue noise 8^3, any larger value blue noise 16^3
+        if(!c || m < 0)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_dither_mode: mode must be >= 0");
         c->ditherMode = m;
         return ISAACB_OK;
     }
+    isaacb_status isaacb_set_field_source(isaacb_ctx* c, uint32_t s, int32_t enabled)
+    {
+        if(!c || s >= uint32_t(c->nVol))
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_field_source: bad source");
+        if(enabled && c->desc.feature_dim[s] != 3)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_field_source: a field source is a float3 vector field");
+        bool f[kMaxSources];
+        for(int k = 0; k < c->nVol; ++k)
+            f[k] = c->field[k];
+        f[s] = enabled != 0;
+        // the reference merges the volume sources, then the field sources: field sources
+        // must follow every other volume source
+        for(int k = 0; k + 1 < c->nVol; ++k)
+            if(f[k] && !f[k + 1])
+                return fail(c, ISAACB_INVALID_ARG, "isaacb_set_field_source: field sources must be the last volume sources");
+        c->field[s] = f[s];
+        return ISAACB_OK;
+    }
+    isaacb_status isaacb_set_advection(
+        isaacb_ctx* c,
+        float step_factor,
+        float history_weight,
+        int32_t seeding_period,
+        int32_t seeding_duration,
+        int32_t seed_points)
+    {
+        if(!c || seeding_period < 1 || seed_points < 0)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_advection: seeding period >= 1 and seed points >= 0");
+        c->advStepFactor = step_factor;
+        c->advHistoryWeight = history_weight;
+        c->advSeedPeriod = seeding_period;
+        c->advSeedTime = seeding_duration;
+        if(seed_points != c->seedPoints)
+            c->noiseDirty = true;
+        c->seedPoints = seed_points;
+        return ISAACB_OK;
+    }
+    isaacb_status isaacb_get_advection(isaacb_ctx* c, void* stream, uint32_t s, uint8_t* host)
+    {
+        if(!c || !host || s >= uint32_t(c->nVol))
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_get_advection: bad arguments");
+        cudaStream_t st = (cudaStream_t) stream;
+        const size_t n = voxel_count(c);
+        if(!c->adv[s])
+        {
+            std::memset(host, 0, n);
+            return ISAACB_OK;
+        }
+        ISAACB_CUDA(c, cudaMemcpyAsync(host, c->adv[s], n, cudaMemcpyDeviceToHost, st), "advection readback");
+        ISAACB_CUDA(c, cudaStreamSynchronize(st), "advection readback");
+        return ISAACB_OK;
+    }
+    isaacb_status isaacb_get_noise(isaacb_ctx* c, void* stream, float* host)
+    {
+        if(!c || !host)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_get_noise: bad arguments");
+        cudaStream_t st = (cudaStream_t) stream;
+        const size_t n = voxel_count(c);
+        if(!c->noise)
+        {
+            ISAACB_CUDA(c, cudaMalloc(&c->noise, n * sizeof(float)), "noise texture");
+            ISAACB_CUDA(c, cudaMalloc(&c->noiseTmp, n * sizeof(float)), "noise texture");
+            c->noiseDirty = true;
+        }
+        if(c->noiseDirty)
+        {
+            NoiseParams np{};
+            np.LX = int(c->desc.local_size[0]);
+            np.LY = int(c->desc.local_size[1]);
+            np.LZ = int(c->desc.local_size[2]);
+            for(int i = 0; i < 3; ++i)
+                np.scale[i] = c->desc.scale[i];
+            np.seedPoints = c->seedPoints;
+            launch_noise(np, c->noise, c->noiseTmp, st);
+            c->noiseDirty = false;
+        }
+        ISAACB_CUDA(c, cudaMemcpyAsync(host, c->noise, n * sizeof(float), cudaMemcpyDeviceToHost, st), "noise readback");
+        ISAACB_CUDA(c, cudaStreamSynchronize(st), "noise readback");
+        return ISAACB_OK;
+    }
+
     isaacb_status isaacb_set_background(isaacb_ctx* c, const float* rgba)
     {
         if(!c || !rgba)
@@ -959,6 +1132,9 @@ extern "C"
         c->updateLaunches = 0;
         if(c->renderer == ISAACB_RENDERER_COMBINED)
         {
+            r = advect_fields(c, st);
+            if(r != ISAACB_OK)
+                return r;
             MergeParams p{};
             prepare_merge(c, p);
             ISAACB_CUDA(c, cudaMemsetAsync(c->emptyDev, 0, sizeof(unsigned int), st), "empty brick counter");
@@ -991,6 +1167,9 @@ extern "C"
         }
         else
         {
+            for(int k = 0; k < c->nVol; ++k)
+                if(c->field[k] && (c->weight[k] != 0.0f || c->iso[k] != 0.0f))
+                    return fail(c, ISAACB_INVALID_ARG, "isaacb_update: field sources are merged by the combined renderer only");
             for(int k = 0; k < ISAACB_TIMING_SLOTS; ++k)
                 c->evUsed[k] = false;
             if(c->timing)
@@ -1376,6 +1555,13 @@ namespace
             why = "iso threshold set";
         else if(c->aoEnabled && c->aoWeight > 0.0f)
             why = "SSAO enabled";
+        else if([&] {
+                    for(int k = 0; k < c->nVol; ++k)
+                        if(c->field[k])
+                            return true;
+                    return false;
+                }())
+            why = "advected field source";
         else
         {
             for(int s = 0; s < c->nPart; ++s)

@@ -31,6 +31,7 @@ namespace isaacb
         float invTotalWeight; // 2^-k when totalWeight == 2^k exactly, else 0
         int32_t nonNegative; // every colour sum is finite and >= 0 (tables and weights >= 0, total > 0)
         int32_t scalarIdem; // every active source is scalar with an all-idem chain
+        const uint8_t* adv[kMaxSources]; // field sources: advection texture (localSize, x fastest), else null
         uint4* volQ; // combined volume, quad bricks
         uint32_t* isoAQ; // combined iso alpha, quad bricks
         uint32_t* isoLin; // combined iso RGBA8, linear
@@ -70,6 +71,29 @@ namespace isaacb
     }
 
     void launch_merge(const MergeParams& p, cudaStream_t s);
+
+    // field-source advection (kernels_merge.cu)
+    struct NoiseParams
+    {
+        int LX, LY, LZ;
+        float scale[3];
+        int seedPoints;
+    };
+    // noise texture: Halton seeds, three 7-tap blur passes, x30 clamped (tmp: scratch of the same size)
+    void launch_noise(const NoiseParams& p, float* noise, float* tmp, cudaStream_t s);
+    struct AdvectParams
+    {
+        const float* field; // float3 per voxel, x fastest
+        const uint8_t* back; // last frame's advection texture
+        uint8_t* out;
+        const float* noise;
+        int LX, LY, LZ;
+        float scale[3];
+        float stepSize; // step factor * ISAAC_MAX_ADVECTION_STEP_SIZE
+        float historyWeight;
+        int seedNoise; // 1: this step adds the noise (timeStep % period < seeding time)
+    };
+    void launch_advect(const AdvectParams& p, cudaStream_t s);
 
     // per-source renderer bricks: persistent sources keep their raw components,
     // non-persistent sources their functor-chain value (UpdatePersistendTextureKernel)

@@ -8,10 +8,13 @@
 // the brick (its 8^3 voxels plus the apron on the low side, clamped at the
 // volume border) once into shared memory, then writes the 576 slots as
 // coalesced 16-byte stores.  The per-brick flags feed empty-space skipping.
+#include "isaacb_blue_noise.h"
 #include "isaacb_internal.h"
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+
+#include <algorithm>
 
 namespace isaacb
 {
@@ -25,7 +28,21 @@ namespace isaacb
            31, 0,  54, 21, 58, 24, 17, 5,  28, 38, 56, 41, 11, 63, 14, 47, 37, 48, 42, 62, 12, 18,
            3,  35, 50, 44, 19, 1,  20, 34, 29, 25, 57, 4,  22, 8,  33, 53, 30, 55, 27, 7};
 
-    // applyDither3D (lib/isaac/isaac_dither_kernel.hpp:7-329), modes 0, 1, 2, bit-exact,
+    // 8^3 and 16^3 blue-noise masks of dither modes 3 and >= 4 (lib/isaac/isaac_dither_kernel.hpp:42-310)
+    __device__ const uint16_t g_blue8[512] = {ISAACB_BLUE_NOISE8_VALUES};
+    __device__ const uint16_t g_blue16[4096] = {ISAACB_BLUE_NOISE16_VALUES};
+
+    // the mode's threshold for voxel (x, y, z >= 0); mask: the 64-entry table of modes 1 and 2
+    __device__ __forceinline__ float dither_threshold(int mode, const uint8_t* mask, int x, int y, int z)
+    {
+        if(mode == 1 || mode == 2)
+            return float(mask[(x & 3) + (y & 3) * 4 + (z & 3) * 16]) / 64.0f;
+        if(mode == 3)
+            return float(__ldg(&g_blue8[(x & 7) + (y & 7) * 8 + (z & 7) * 64])) / 512.0f;
+        return float(__ldg(&g_blue16[(x & 15) + (y & 15) * 16 + (z & 15) * 256])) / 4096.0f;
+    }
+
+    // applyDither3D (lib/isaac/isaac_dither_kernel.hpp:7-329), every mode, bit-exact,
     // with truncation, floor and rounding done by exact magic-number adds on the FMA pipe
     __device__ __forceinline__ uint32_t round_byte(float v)
     {
@@ -46,7 +63,7 @@ namespace isaacb
                 out |= uint32_t(min(round_nonneg(fminf(v[i], 1.0f) * 255.0f), 255)) << (8 * i);
             return out;
         }
-        const float d = float(mask[(x & 3) + (y & 3) * 4 + (z & 3) * 16]) / 64.0f;
+        const float d = dither_threshold(mode, mask, x, y, z);
 #pragma unroll
         for(int i = 0; i < 4; ++i)
         {
@@ -75,7 +92,7 @@ namespace isaacb
             }
             return out;
         }
-        const float d = float(mask[(x & 3) + (y & 3) * 4 + (z & 3) * 16]) / 64.0f; // x, y, z >= 0
+        const float d = dither_threshold(mode, mask, x, y, z); // x, y, z >= 0
 #pragma unroll
         for(int i = 0; i < 4; ++i)
         {
@@ -172,8 +189,16 @@ namespace isaacb
             if(!(vw + it > 0.0f))
                 continue;
             const float4* lut = p.lut + size_t(s) * p.ts;
+            const uint8_t* adv = p.adv[s];
             auto accumulate = [&](int j, float val) {
-                const float4 c = __ldg(lut + lut_index_fast(val, p.ts));
+                float4 c = __ldg(lut + lut_index_fast(val, p.ts));
+                if(adv)
+                {
+                    // field source: alpha blended with the advection texture
+                    // (MergeAdvectionToCombinedTextureIterator, isaac_common_kernel.hpp:664-665)
+                    const size_t vox = (size_t(zs[j]) * g.ls[1] + ys[j]) * g.ls[0] + xs[j];
+                    c.w *= float(__ldg(adv + vox)) / 255.0f;
+                }
                 if(vw > 0.0f)
                 {
                     const float a = c.w * vw;
@@ -512,6 +537,157 @@ namespace isaacb
             k_merge<false, true><<<grid, 256, 0, s>>>(p);
         else
             k_merge<false, false><<<grid, 256, 0, s>>>(p);
+    }
+
+    // ---------------------------------------------------------------- field-source advection
+    // updateNoiseTexture (lib/isaac.hpp:499-562) with HaltonSeedingKernel, GaussBlur7Kernel
+    // and MultiplyClampKernel (lib/isaac/isaac_common_kernel.hpp:334-430), and
+    // GenerateAdvectionTextureKernel (:500-550).  The reference leaves the advection
+    // textures (and their guard cells) uninitialised; here they start at zero, so a
+    // sample outside the local volume reads 0 like its VALUE border.
+
+    // trilinear sample of a scalar texture through Sampler<LINEAR, ...>::interpolate
+    // (isaac_texture.hpp:237-257): fetch(ix, iy, iz) returns the bordered texel
+    template<class F>
+    __device__ __forceinline__ float sample_linear(float cx, float cy, float cz, F fetch)
+    {
+        cx -= 0.5f;
+        cy -= 0.5f;
+        cz -= 0.5f;
+        const float flx = floorf(cx), fly = floorf(cy), flz = floorf(cz);
+        const int ix = int(flx), iy = int(fly), iz = int(flz);
+        const float ox = cx - flx, oy = cy - fly, oz = cz - flz;
+        return tri_q(
+            ox,
+            oy,
+            oz,
+            fetch(ix, iy, iz),
+            fetch(ix + 1, iy, iz),
+            fetch(ix, iy + 1, iz),
+            fetch(ix + 1, iy + 1, iz),
+            fetch(ix, iy, iz + 1),
+            fetch(ix + 1, iy, iz + 1),
+            fetch(ix, iy + 1, iz + 1),
+            fetch(ix + 1, iy + 1, iz + 1));
+    }
+
+    __device__ __forceinline__ float halton_f(uint32_t index, uint32_t base)
+    {
+        // isaac_helper.hpp:57-69
+        float result = 0.0f, f = 1.0f;
+        while(index > 0)
+        {
+            f /= float(base);
+            result += f * float(index % base);
+            index /= base;
+        }
+        return result;
+    }
+
+    __global__ void k_noise_seed(NoiseParams p, float* __restrict__ noise)
+    {
+        // every seed writes 1, so the serial reference loop and this one agree in any order
+        const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+        if(i > p.seedPoints)
+            return;
+        const int x = int(float(p.LX) * halton_f(uint32_t(i), 3));
+        const int y = int(float(p.LY) * halton_f(uint32_t(i), 5));
+        const int z = int(float(p.LZ) * halton_f(uint32_t(i), 7));
+        noise[(size_t(z) * p.LY + y) * p.LX + x] = 1.0f;
+    }
+
+    __global__ void k_noise_blur(NoiseParams p, const float* __restrict__ src, float* __restrict__ dst, int axis)
+    {
+        const size_t n = size_t(p.LX) * p.LY * p.LZ;
+        const float g7[4] = {64.0f, 40.5f, 10.0f, 1.0f};
+        const float mx = axis == 0 ? 1.0f : 0.0f, my = axis == 1 ? 1.0f : 0.0f, mz = axis == 2 ? 1.0f : 0.0f;
+        auto fetch = [&](int x, int y, int z) {
+            // REPEAT border, no guard
+            x = (p.LX + (x % p.LX)) % p.LX;
+            y = (p.LY + (y % p.LY)) % p.LY;
+            z = (p.LZ + (z % p.LZ)) % p.LZ;
+            return __ldg(src + (size_t(z) * p.LY + y) * p.LX + x);
+        };
+        for(size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        {
+            const int x = int(i % p.LX);
+            const size_t t = i / p.LX;
+            const int y = int(t % p.LY), z = int(t / p.LY);
+            float r = 0.0f;
+            for(int k = -3; k < 4; ++k)
+            {
+                const float cx = float(x) + mx * float(k) / p.scale[0];
+                const float cy = float(y) + my * float(k) / p.scale[1];
+                const float cz = float(z) + mz * float(k) / p.scale[2];
+                r += sample_linear(cx, cy, cz, fetch) * g7[k < 0 ? -k : k];
+            }
+            dst[i] = r / 167.0f;
+        }
+    }
+
+    __global__ void k_noise_clamp(size_t n, const float* __restrict__ src, float* __restrict__ dst)
+    {
+        for(size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+            dst[i] = gclamp(src[i] * 30.0f, 0.0f, 1.0f);
+    }
+
+    void launch_noise(const NoiseParams& p, float* noise, float* tmp, cudaStream_t s)
+    {
+        const size_t n = size_t(p.LX) * p.LY * p.LZ;
+        cudaMemsetAsync(noise, 0, n * sizeof(float), s);
+        if(p.seedPoints > 0)
+            k_noise_seed<<<(p.seedPoints + 255) / 256, 256, 0, s>>>(p, noise);
+        const int blocks = int(std::min<size_t>((n + 255) / 256, 148 * 16));
+        k_noise_blur<<<blocks, 256, 0, s>>>(p, noise, tmp, 0);
+        k_noise_blur<<<blocks, 256, 0, s>>>(p, tmp, noise, 1);
+        k_noise_blur<<<blocks, 256, 0, s>>>(p, noise, tmp, 2);
+        k_noise_clamp<<<blocks, 256, 0, s>>>(n, tmp, noise);
+    }
+
+    __global__ void k_advect(const __grid_constant__ AdvectParams p)
+    {
+        const size_t n = size_t(p.LX) * p.LY * p.LZ;
+        auto fetch = [&](int x, int y, int z) {
+            // VALUE border 0 (the guard cells are zero too)
+            if(x < 0 || y < 0 || z < 0 || x >= p.LX || y >= p.LY || z >= p.LZ)
+                return 0.0f;
+            return float(__ldg(p.back + (size_t(z) * p.LY + y) * p.LX + x));
+        };
+        for(size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        {
+            const int x = int(i % p.LX);
+            const size_t t = i / p.LX;
+            const int y = int(t % p.LY), z = int(t / p.LY);
+            float vx = __ldg(p.field + 3 * i), vy = __ldg(p.field + 3 * i + 1), vz = __ldg(p.field + 3 * i + 2);
+            // glm::length: sqrt((x*x + y*y) + z*z); at least FLT_MIN
+            const float len = gmax(sqrtf((vx * vx + vy * vy) + vz * vz), 1.17549435e-38f);
+            vx = vx / len;
+            vy = vy / len;
+            vz = vz / len;
+            const float cx = (float(x) + 0.5f) - vx * p.stepSize / p.scale[0];
+            const float cy = (float(y) + 0.5f) - vy * p.stepSize / p.scale[1];
+            const float cz = (float(z) + 0.5f) - vz * p.stepSize / p.scale[2];
+            const float history = sample_linear(cx, cy, cz, fetch) / 255.0f;
+            const float nv = p.seedNoise ? __ldg(p.noise + i) : 0.0f;
+            const float v = nv + history * p.historyWeight * (1.0f - nv);
+            // applyDither3D(5, coord, v): the 16^3 blue-noise mask, int(s) + (fract(s) > d), clamped
+            const float d = dither_threshold(5, nullptr, x, y, z);
+            const float sv = fminf(fmaxf(v * 255.0f, -2.0f), 257.0f);
+            float tr;
+            int ti = trunc_nonneg(fabsf(sv), tr);
+            if(sv < 0.0f)
+                ti = -ti;
+            float fl;
+            int fi;
+            floor_split(sv, fl, fi);
+            p.out[i] = uint8_t(min(max(ti + ((sv - fl) > d ? 1 : 0), 0), 255));
+        }
+    }
+
+    void launch_advect(const AdvectParams& p, cudaStream_t s)
+    {
+        const size_t n = size_t(p.LX) * p.LY * p.LZ;
+        k_advect<<<int(std::min<size_t>((n + 255) / 256, 148 * 16)), 256, 0, s>>>(p);
     }
 
     // ---------------------------------------------------------------- per-source bricks

@@ -22,26 +22,13 @@ import numpy as np
 from . import _lib
 from ._lib import check
 
-Z_NEAR = 0.002  # ISAAC_Z_NEAR, lib/isaac/isaac_defines.hpp:53
-Z_FAR = 100.0  # ISAAC_Z_FAR, lib/isaac/isaac_defines.hpp:54
+from .controllers import Z_FAR, Z_NEAR, DefaultCompositor, DefaultController, perspective  # noqa: F401
 
 
 def _torch():
     import torch
 
     return torch
-
-
-def perspective(fovy: float, aspect: float, znear: float, zfar: float) -> np.ndarray:
-    """glm::perspective (right handed, clip depth -1..1), column major 4x4 double."""
-    t = math.tan(fovy / 2.0)
-    m = np.zeros((4, 4), dtype=np.float64)  # m[col][row]
-    m[0][0] = 1.0 / (aspect * t)
-    m[1][1] = 1.0 / t
-    m[2][2] = -(zfar + znear) / (zfar - znear)
-    m[2][3] = -1.0
-    m[3][2] = -(2.0 * zfar * znear) / (zfar - znear)
-    return m
 
 
 def modelview(look_at=(0.0, 0.0, 0.0), rotation=None, distance=-4.5) -> np.ndarray:
@@ -60,17 +47,6 @@ def modelview(look_at=(0.0, 0.0, 0.0), rotation=None, distance=-4.5) -> np.ndarr
 def _cm_mul(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     """Product of two column-major [col][row] matrices, returned column-major."""
     return (a.T @ b.T).T
-
-
-class DefaultController:
-    """isaac_controllers.hpp:23-43: perspective(45.0, w/h, Z_NEAR, Z_FAR), with 45.0 in radians as glm reads it."""
-
-    passCount = 1
-
-    @staticmethod
-    def updateProjection(framebuffer_size) -> np.ndarray:
-        w, h = framebuffer_size
-        return perspective(45.0, float(w) / float(h), Z_NEAR, Z_FAR)
 
 
 class VolumeSource:
@@ -135,6 +111,7 @@ class IsaacVisualization:
         scale: Sequence[float] = (1.0, 1.0, 1.0),
         transfer_size: int = 1024,
         controller=DefaultController,
+        compositor=None,
     ):
         self.lib = _lib.load()
         self.name = name
@@ -179,7 +156,10 @@ class IsaacVisualization:
         self.backgroundColor = [0.0, 0.0, 0.0, 0.0]
         self.clipping: list[tuple] = []
         self.controller = controller
-        self.projection = controller.updateProjection(self.framebufferSize)
+        self.compositor = compositor if compositor is not None else DefaultCompositor()
+        # one projection per render pass (two for a stereo controller)
+        self.projections = [np.asarray(m, dtype=np.float64) for m in controller.projections(self.framebufferSize)]
+        self.projection = self.projections[0]
         self.lookAt = (0.0, 0.0, 0.0)
         self.rotation = np.eye(3)
         self.distance = -4.5
@@ -291,6 +271,32 @@ class IsaacVisualization:
         self.ditherMode = int(mode)
         check(self.lib.isaacb_set_dither_mode(self.ctx, int(mode)), self.ctx)
 
+    # ------------------------------------------------------------------ field sources and advection
+    def setFieldSource(self, src: int, enabled: bool = True):
+        """Make volume source ``src`` (a float3 vector field, after every plain volume
+        source) an advected field source (the reference's FieldSourceList)."""
+        check(self.lib.isaacb_set_field_source(self.ctx, int(src), int(enabled)), self.ctx)
+
+    def setAdvection(self, step_factor=1.0, history_weight=0.95, seeding_period=1, seeding_duration=1, seed_points=1000):
+        """The "advection step", "advection weight", "advection seeding period",
+        "advection seeding duration" and "seed points" settings (lib/isaac.hpp:1636-1662)."""
+        self.advection = dict(step=step_factor, weight=history_weight, period=seeding_period,
+                              duration=seeding_duration, seeds=seed_points)
+        check(self.lib.isaacb_set_advection(self.ctx, float(step_factor), float(history_weight), int(seeding_period),
+                                             int(seeding_duration), int(seed_points)), self.ctx)
+
+    def advectionTexture(self, src: int) -> np.ndarray:
+        lx, ly, lz = (int(v) for v in self.desc.local_size)
+        out = np.empty((lz, ly, lx), dtype=np.uint8)
+        check(self.lib.isaacb_get_advection(self.ctx, self._stream(), int(src), C.c_void_p(out.ctypes.data)), self.ctx)
+        return out
+
+    def noiseTexture(self) -> np.ndarray:
+        lx, ly, lz = (int(v) for v in self.desc.local_size)
+        out = np.empty((lz, ly, lx), dtype=np.float32)
+        check(self.lib.isaacb_get_noise(self.ctx, self._stream(), out.ctypes.data_as(_lib._fp)), self.ctx)
+        return out
+
     def setBackgroundColor(self, rgba: Sequence[float]):
         self.backgroundColor = [float(v) for v in rgba]
         check(self.lib.isaacb_set_background(self.ctx, _fa(self.backgroundColor)), self.ctx)
@@ -316,6 +322,7 @@ class IsaacVisualization:
     def setCamera(self, projection: np.ndarray, modelview_m: np.ndarray):
         """Explicit projection and modelview, column-major [col][row] doubles."""
         self.projection = np.asarray(projection, dtype=np.float64)
+        self.projections = [self.projection] + self.projections[1:]
         self.modelview = np.asarray(modelview_m, dtype=np.float64)
         self._push_camera()
 
@@ -375,6 +382,16 @@ class IsaacVisualization:
             self.addClipping(*c["position"], *c["normal"])
         if "clipping remove" in message:
             self.removeClipping(int(message["clipping remove"]))
+        keys = {"advection step": "step", "advection weight": "weight", "advection seeding period": "period",
+                "advection seeding duration": "duration", "seed points": "seeds"}
+        if any(k in message for k in keys):
+            a = dict(getattr(self, "advection", dict(step=1.0, weight=0.95, period=1, duration=1, seeds=1000)))
+            for k, name in keys.items():
+                if k in message:
+                    a[name] = message[k]
+            if "seed points" in message:
+                a["seeds"] = max(int(a["seeds"]), 0)
+            self.setAdvection(a["step"], a["weight"], a["period"], a["duration"], a["seeds"])
         if "clipping edit" in message:
             c = message["clipping edit"]
             self.editClipping(int(c["nr"]), *c["position"], *c["normal"])
@@ -408,6 +425,8 @@ class IsaacVisualization:
             return self._frame
         w, h = self.framebufferSize
         st = self._stream()
+        if len(self.projections) > 1 or not isinstance(self.compositor, DefaultCompositor):
+            return self._multi_pass(host, st)
         if host and not timing:
             if out is None:
                 out = np.empty((h, w, 4), dtype=np.uint8)
@@ -429,6 +448,26 @@ class IsaacVisualization:
             self.mergeTime = e0.elapsed_time(e1)
             self.kernelTime = e1.elapsed_time(e2)
         result = dev.cpu().numpy() if host else dev
+        self._frame = result
+        return result
+
+    def _multi_pass(self, host: bool, st):
+        """One render per controller pass (lib/isaac.hpp:2008-2061) with the pass's
+        projection and the common modelview, then the compositor on the GPU."""
+        torch = _torch()
+        w, h = self.framebufferSize
+        check(self.lib.isaacb_update(self.ctx, st), self.ctx)
+        m = np.ascontiguousarray(self.modelview, dtype=np.float64).reshape(16)
+        images = []
+        for proj in self.projections:
+            pp = np.ascontiguousarray(proj, dtype=np.float64).reshape(16)
+            check(self.lib.isaacb_set_camera(self.ctx, pp.ctypes.data_as(_lib._dp), m.ctypes.data_as(_lib._dp)), self.ctx)
+            img = torch.empty((h, w, 4), dtype=torch.uint8, device="cuda")
+            check(self.lib.isaacb_render(self.ctx, st, C.c_void_p(img.data_ptr())), self.ctx)
+            images.append(img)
+        self._push_camera()
+        frame = self.compositor.compose(images)
+        result = frame.cpu().numpy() if host else frame
         self._frame = result
         return result
 

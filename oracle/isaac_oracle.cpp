@@ -28,6 +28,7 @@
 //
 // Reference files cited below are paths inside the ISAAC repository.
 
+#include "../isaac_b200/csrc/isaacb_blue_noise.h"
 #include <algorithm>
 #include <cerrno>
 #include <cmath>
@@ -621,8 +622,16 @@ namespace orc
             }
             return;
         }
-        const uint8_t* mask = (mode == 2) ? kDitherMask2 : kDitherMask1;
-        T d = T(mask[x % 4 + (y % 4) * 4 + (z % 4) * 16]) / T(64);
+        T d;
+        if(mode == 1 || mode == 2)
+        {
+            const uint8_t* mask = (mode == 2) ? kDitherMask2 : kDitherMask1;
+            d = T(mask[x % 4 + (y % 4) * 4 + (z % 4) * 16]) / T(64);
+        }
+        else if(mode == 3)
+            d = T(kBlueNoise8[x % 8 + (y % 8) * 8 + (z % 8) * 64]) / T(512);
+        else
+            d = T(kBlueNoise16[x % 16 + (y % 16) * 16 + (z % 16) * 256]) / T(4096);
         for(int i = 0; i < 4; ++i)
         {
             T s = c[i] * T(255);
@@ -748,6 +757,17 @@ namespace orc
         float bg[4] = {0, 0, 0, 0};
         double proj[16], mv[16];
 
+        // field-source advection (lib/isaac.hpp:292-370, 499-562, 1819-1850); defaults of
+        // isaac.hpp:606-643.  The reference leaves the advection textures and their guard
+        // cells uninitialised; here they start at zero.
+        bool field[MAX_SOURCES] = {};
+        std::vector<uint8_t> adv[MAX_SOURCES], advBack[MAX_SOURCES]; // localSize, x fastest
+        std::vector<T> noise; // localSize
+        float advStepFactor = 1.0f, advHistoryWeight = 0.95f;
+        int advSeedPeriod = 1, advSeedTime = 1, seedPoints = 1000;
+        int64_t timeStep = 0;
+        bool noiseDirty = true;
+
         // buffers
         std::vector<uint8_t> volTex, isoTex; // localSize, RGBA8, x fastest
         std::vector<T> npTex[MAX_SOURCES]; // non-persistent textures (local+2g)^3
@@ -828,6 +848,31 @@ namespace orc
             gDepth.assign(size_t(W) * H, 0);
             gAo.assign(size_t(W) * H, 0);
             gNormal.assign(size_t(W) * H, V3<T>{0, 0, 0});
+        }
+
+        void setAdvection(float stepFactor, float historyWeight, int period, int seedTime, int seeds)
+        {
+            advStepFactor = stepFactor;
+            advHistoryWeight = historyWeight;
+            advSeedPeriod = period;
+            advSeedTime = seedTime;
+            if(seeds != seedPoints)
+                noiseDirty = true;
+            seedPoints = seeds;
+        }
+        void getAdvection(int s, uint8_t* out) const
+        {
+            const size_t n = size_t(localSize[0] * localSize[1] * localSize[2]);
+            for(size_t i = 0; i < n; ++i)
+                out[i] = adv[s].size() == n ? adv[s][i] : 0;
+        }
+        void getNoise(float* out)
+        {
+            const size_t n = size_t(localSize[0] * localSize[1] * localSize[2]);
+            if(noiseDirty || noise.size() != n)
+                updateNoise();
+            for(size_t i = 0; i < n; ++i)
+                out[i] = float(noise[i]);
         }
 
         void setFramebuffer(int w, int h)
@@ -936,10 +981,142 @@ namespace orc
             return lut[s][lut_index(v, ts)];
         }
 
+        // ----- trilinear sample of a scalar texture (Sampler<LINEAR, ...>::interpolate,
+        // lib/isaac/isaac_texture.hpp:237-257, trilinear of isaac_helper.hpp:138-144); fetch(ix, iy, iz)
+        // returns the bordered texel
+        template<class F>
+        T sampleLinear(V3<T> c, F fetch) const
+        {
+            c = {c.x - T(0.5), c.y - T(0.5), c.z - T(0.5)};
+            const int64_t fx = (int64_t) std::floor(c.x), fy = (int64_t) std::floor(c.y), fz = (int64_t) std::floor(c.z);
+            T d[2][2][2];
+            for(int z = 0; z < 2; ++z)
+                for(int y = 0; y < 2; ++y)
+                    for(int x = 0; x < 2; ++x)
+                        d[x][y][z] = fetch(fx + x, fy + y, fz + z);
+            const T ox = gfract(c.x), oy = gfract(c.y), oz = gfract(c.z);
+            auto lin = [](T o, T a, T b) { return a * (T(1) - o) + b * o; };
+            T a = lin(oy, lin(oz, d[0][0][0], d[0][0][1]), lin(oz, d[0][1][0], d[0][1][1]));
+            T b = lin(oy, lin(oz, d[1][0][0], d[1][0][1]), lin(oz, d[1][1][0], d[1][1][1]));
+            return lin(ox, a, b);
+        }
+
+        // ----- noise texture: HaltonSeedingKernel, three GaussBlur7Kernel passes and
+        // MultiplyClampKernel (isaac_common_kernel.hpp:334-430; updateNoiseTexture, isaac.hpp:499-562)
+        void updateNoise()
+        {
+            const int64_t LX = localSize[0], LY = localSize[1], LZ = localSize[2];
+            const size_t n = size_t(LX * LY * LZ);
+            noise.assign(n, T(0));
+            for(uint32_t i = 1; i <= uint32_t(seedPoints); ++i)
+            {
+                const float ux = halton(i, 3), uy = halton(i, 5), uz = halton(i, 7);
+                const int64_t x = (int64_t) (int32_t) (float(LX) * ux), y = (int64_t) (int32_t) (float(LY) * uy),
+                              z = (int64_t) (int32_t) (float(LZ) * uz);
+                noise[size_t(x + y * LX + z * LX * LY)] = T(1);
+            }
+            std::vector<T> tmp(n);
+            auto blur = [&](const std::vector<T>& src, std::vector<T>& dst, int axis) {
+                const T g7[4] = {T(64), T(40.5), T(10), T(1)};
+                auto fetch = [&](int64_t x, int64_t y, int64_t z) {
+                    // REPEAT border without guard
+                    x = (LX + (x % LX)) % LX;
+                    y = (LY + (y % LY)) % LY;
+                    z = (LZ + (z % LZ)) % LZ;
+                    return src[size_t(x + y * LX + z * LX * LY)];
+                };
+#pragma omp parallel for schedule(static)
+                for(int64_t z = 0; z < LZ; ++z)
+                    for(int64_t y = 0; y < LY; ++y)
+                        for(int64_t x = 0; x < LX; ++x)
+                        {
+                            T r = T(0);
+                            for(int i = -3; i < 4; ++i)
+                            {
+                                const T mx = axis == 0 ? T(1) : T(0), my = axis == 1 ? T(1) : T(0), mz = axis == 2 ? T(1) : T(0);
+                                V3<T> c{T(x) + mx * T(i) / T(scale[0]), T(y) + my * T(i) / T(scale[1]), T(z) + mz * T(i) / T(scale[2])};
+                                r += sampleLinear(c, fetch) * g7[i < 0 ? -i : i];
+                            }
+                            dst[size_t(x + y * LX + z * LX * LY)] = r / T(167);
+                        }
+            };
+            blur(noise, tmp, 0);
+            blur(tmp, noise, 1);
+            blur(noise, tmp, 2);
+            for(size_t i = 0; i < n; ++i)
+                noise[i] = gclamp(tmp[i] * T(30), T(0), T(1));
+            noiseDirty = false;
+        }
+
+        // ----- GenerateAdvectionTextureKernel (isaac_common_kernel.hpp:500-550) for one field source
+        void advect(int s)
+        {
+            const int64_t LX = localSize[0], LY = localSize[1], LZ = localSize[2];
+            const T stepSize = T(advStepFactor * float(3)); // ISAAC_MAX_ADVECTION_STEP_SIZE
+            const std::vector<uint8_t>& back = advBack[s];
+            auto fetch = [&](int64_t x, int64_t y, int64_t z) {
+                // VALUE border (0); the guard cells are zero as well
+                if(x < 0 || y < 0 || z < 0 || x >= LX || y >= LY || z >= LZ)
+                    return T(0);
+                return T(back[size_t(x + y * LX + z * LX * LY)]);
+            };
+#pragma omp parallel for schedule(static)
+            for(int64_t z = 0; z < LZ; ++z)
+                for(int64_t y = 0; y < LY; ++y)
+                    for(int64_t x = 0; x < LX; ++x)
+                    {
+                        T v[4];
+                        readSource(s, x, y, z, v);
+                        V3<T> vec{v[0], v[1], v[2]};
+                        const T len = gmax(length(vec), T(std::numeric_limits<float>::min()));
+                        vec = {vec.x / len, vec.y / len, vec.z / len};
+                        const V3<T> off{vec.x * stepSize / T(scale[0]), vec.y * stepSize / T(scale[1]), vec.z * stepSize / T(scale[2])};
+                        const V3<T> oc{(T(x) + T(0.5)) - off.x, (T(y) + T(0.5)) - off.y, (T(z) + T(0.5)) - off.z};
+                        const T history = sampleLinear(oc, fetch) / T(255);
+                        T nv = noise[size_t(x + y * LX + z * LX * LY)];
+                        if(timeStep % advSeedPeriod >= advSeedTime)
+                            nv = T(0);
+                        V4<T> c{nv + history * T(advHistoryWeight) * (T(1) - nv), T(0), T(0), T(0)};
+                        uint8_t out[4];
+                        dither(5, x, y, z, c, out);
+                        adv[s][size_t(x + y * LX + z * LX * LY)] = out[0];
+                    }
+        }
+
+        // ----- per frame: swap the advection buffers, count the step, advect the enabled field sources
+        // (isaac.hpp:1819-1850)
+        void updateAdvection()
+        {
+            bool anyField = false;
+            for(int s = 0; s < nVol; ++s)
+                anyField = anyField || field[s];
+            if(!anyField)
+                return;
+            const size_t n = size_t(localSize[0] * localSize[1] * localSize[2]);
+            if(noiseDirty || noise.size() != n)
+                updateNoise();
+            for(int s = 0; s < nVol; ++s)
+            {
+                if(!field[s])
+                    continue;
+                if(adv[s].size() != n)
+                {
+                    adv[s].assign(n, 0);
+                    advBack[s].assign(n, 0);
+                }
+                std::swap(adv[s], advBack[s]);
+            }
+            timeStep++;
+            for(int s = 0; s < nVol; ++s)
+                if(field[s] && (weight[s] != 0.0f || iso[s] != 0.0f))
+                    advect(s);
+        }
+
         // ----- buffer update: UpdatePersistendTextureKernel (lib/isaac/isaac_common_kernel.hpp:432-451)
         // and MergeToCombinedTextureKernel (lib/isaac/isaac_common_kernel.hpp:690-759).
         void update()
         {
+            updateAdvection();
             for(int s = 0; s < nVol; ++s)
             {
                 bool enabled = weight[s] != 0.0f || iso[s] != 0.0f;
@@ -981,6 +1158,10 @@ namespace orc
                                 continue;
                             T texValue = chainAt(s, x, y, z);
                             V4<T> color = lutAt(s, texValue);
+                            // field sources: alpha blended with the advection texture
+                            // (MergeAdvectionToCombinedTextureIterator, isaac_common_kernel.hpp:664-665)
+                            if(field[s])
+                                color.w *= (T(adv[s][size_t(x + y * LX + z * LX * LY)]) / T(255));
                             if(vw > T(0))
                             {
                                 V4<T> c = color;
@@ -2103,6 +2284,23 @@ extern "C"
     }
     // a new framebuffer size (the reference fixes it at construction; this
     // lets one oracle stand in for views of several sizes of the same scene)
+    // field sources must be scalar-indexed after every other volume source
+    void or_set_field(void* p, int s, int enabled)
+    {
+        OR_DISPATCH((OrHandle*) p, c->field[s] = enabled != 0);
+    }
+    void or_set_advection(void* p, float stepFactor, float historyWeight, int period, int seedTime, int seeds)
+    {
+        OR_DISPATCH((OrHandle*) p, c->setAdvection(stepFactor, historyWeight, period, seedTime, seeds));
+    }
+    void or_get_advection(void* p, int s, uint8_t* out)
+    {
+        OR_DISPATCH((OrHandle*) p, c->getAdvection(s, out));
+    }
+    void or_get_noise(void* p, float* out)
+    {
+        OR_DISPATCH((OrHandle*) p, c->getNoise(out));
+    }
     void or_set_framebuffer(void* p, int w, int h)
     {
         OR_DISPATCH((OrHandle*) p, c->setFramebuffer(w, h));

@@ -47,6 +47,10 @@ SIG = {
     "or_set_background": (None, [_P, _fp]),
     "or_set_camera": (None, [_P, _dp, _dp]),
     "or_set_framebuffer": (None, [_P, C.c_int, C.c_int]),
+    "or_set_field": (None, [_P, C.c_int, C.c_int]),
+    "or_set_advection": (None, [_P, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int]),
+    "or_get_advection": (None, [_P, C.c_int, _u8p]),
+    "or_get_noise": (None, [_P, _fp]),
     "or_update": (None, [_P]),
     "or_render": (None, [_P, _u8p, C.c_int, C.c_int]),
     "or_minmax": (None, [_P, _fp, _fp]),
@@ -222,6 +226,26 @@ class Oracle:
         p = np.ascontiguousarray(P, dtype=np.float64).reshape(16)
         m = np.ascontiguousarray(MV, dtype=np.float64).reshape(16)
         self.lib.or_set_camera(self.ctx, _ptr(p, _dp), _ptr(m, _dp))
+
+    def set_field(self, src: int, enabled: bool = True):
+        """Mark volume source ``src`` (featureDim 3, after every plain volume source) as an advected field."""
+        self.lib.or_set_field(self.ctx, int(src), int(enabled))
+
+    def set_advection(self, step_factor=1.0, history_weight=0.95, seeding_period=1, seeding_time=1, seed_points=1000):
+        self.lib.or_set_advection(self.ctx, float(step_factor), float(history_weight), int(seeding_period),
+                                  int(seeding_time), int(seed_points))
+
+    def advection(self, src: int) -> np.ndarray:
+        lx, ly, lz = self.local_size
+        out = np.zeros((lz, ly, lx), dtype=np.uint8)
+        self.lib.or_get_advection(self.ctx, int(src), _ptr(out, _u8p))
+        return out
+
+    def noise(self) -> np.ndarray:
+        lx, ly, lz = self.local_size
+        out = np.zeros((lz, ly, lx), dtype=np.float32)
+        self.lib.or_get_noise(self.ctx, _ptr(out, _fp))
+        return out
 
     def set_framebuffer(self, w: int, h: int):
         self.lib.or_set_framebuffer(self.ctx, int(w), int(h))

@@ -31,7 +31,7 @@ def _frames(s: Scene):
 
 
 # --------------------------------------------------------------------- merge
-@pytest.mark.parametrize("dither", [0, 1, 2])
+@pytest.mark.parametrize("dither", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("iso", [False, True])
 def test_merge_textures_bit_exact(dither, iso):
     s = gaussian_pair(n=29, dither_mode=dither)
@@ -47,7 +47,7 @@ def test_merge_textures_bit_exact(dither, iso):
     assert np.array_equal(gi, ri)
 
 
-@pytest.mark.parametrize("dither", [0, 1, 2])
+@pytest.mark.parametrize("dither", [0, 1, 2, 3, 5])
 @pytest.mark.parametrize("iso", [False, True])
 @pytest.mark.parametrize("weights", [(2.0, 2.0, 2.0, 2.0), (1.0, 0.0, 3.5, 0.25)])
 def test_merge_scalar_sources_bit_exact(dither, iso, weights):

@@ -213,3 +213,14 @@ def test_fp64_oracle_close_to_fp32():
     b = build_oracle(s, f64=True).frame()
     st = image_diff(a, b)
     assert st["max"] <= 3 and st["frac_le1"] > 0.99
+
+
+def test_dither_blue_noise_modes():
+    # mode 3: 8^3 mask (isaac_dither_kernel.hpp:42-74), value/512; first entries 140, 428
+    assert O.dither(3, 0, 0, 0, [0.5] * 4) == [128] * 4  # .5 > 140/512
+    assert O.dither(3, 1, 0, 0, [0.5] * 4) == [127] * 4  # .5 < 428/512
+    assert O.dither(3, 8, 8, 8, [0.5] * 4) == [128] * 4  # wraps every 8
+    # modes >= 4: 16^3 mask (:76-310), value/4096; entries 0 and 4 are 1940 and 2568
+    assert O.dither(4, 0, 0, 0, [0.5] * 4) == [128] * 4  # .5 > 1940/4096
+    assert O.dither(4, 4, 0, 0, [0.5] * 4) == [127] * 4  # .5 < 2568/4096
+    assert O.dither(7, 4, 16, 32, [0.5] * 4) == [127] * 4  # any larger mode, wraps every 16
