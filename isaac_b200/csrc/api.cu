@@ -5,7 +5,6 @@
 #include "../../include/isaac_b200.h"
 #include "isaacb_internal.h"
 
-#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cctype>
@@ -278,6 +277,7 @@ struct isaacb_ctx
     float4* lutDev = nullptr;
     float* lutPinned = nullptr;
     cudaEvent_t lutEvent = nullptr;
+    uint32_t* volLin = nullptr; // merge scratch: the combined volume, linear RGBA8
     uint4* volQ = nullptr;
     uint32_t* isoAQ = nullptr;
     uint32_t* isoLin = nullptr;
@@ -300,9 +300,6 @@ struct isaacb_ctx
     unsigned int* emptyPinned = nullptr;
     cudaEvent_t emptyEvent = nullptr;
     long long lastEmpty = -1;
-    // TMA tensor maps of the sources, re-encoded when a pointer changes
-    CUtensorMap tmap[kMaxSources]{};
-    const float* tmapPtr[kMaxSources]{};
     // field-source advection (defaults of lib/isaac.hpp:606-643); the textures start at zero
     bool field[kMaxSources]{};
     uint8_t* adv[kMaxSources]{};
@@ -394,25 +391,9 @@ namespace
         return ISAACB_OK;
     }
 
-    PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
-    {
-        static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-        static bool tried = false;
-        if(!tried)
-        {
-            tried = true;
-            void* f = nullptr;
-            cudaDriverEntryPointQueryResult q{};
-            if(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess
-               && q == cudaDriverEntryPointSuccess)
-                fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
-        }
-        return fn;
-    }
 
     // 3-D tensor map over a source seen as (X*featureDim, Y, Z) floats with box
     // (16*featureDim, 9, 9): the region a merge brick needs, x start on a 16-byte boundary
-    bool encode_source_map(isaacb_ctx* c, int s);
 
     size_t brick_count(const Geom& g)
     {
@@ -473,40 +454,6 @@ namespace
 
 namespace
 {
-    bool encode_source_map(isaacb_ctx* c, int s)
-    {
-        auto enc = tensor_map_encoder();
-        const float* src = c->src[s];
-        if(!enc || !src)
-            return false;
-        const uint64_t fd = c->desc.feature_dim[s];
-        const uint64_t X = uint64_t(c->g.ls[0]), Y = uint64_t(c->g.ls[1]), Z = uint64_t(c->g.ls[2]);
-        if((reinterpret_cast<uintptr_t>(src) & 15u) != 0 || ((X * fd) & 3u) != 0)
-            return false;
-        if(c->tmapPtr[s] == src)
-            return true;
-        cuuint64_t dims[3] = {X * fd, Y, Z};
-        cuuint64_t strides[2] = {X * fd * 4, X * Y * fd * 4};
-        cuuint32_t box[3] = {cuuint32_t(16 * fd), 9, 9};
-        cuuint32_t estr[3] = {1, 1, 1};
-        const CUresult r = enc(
-            &c->tmap[s],
-            CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-            3,
-            const_cast<float*>(src),
-            dims,
-            strides,
-            box,
-            estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE,
-            CU_TENSOR_MAP_SWIZZLE_NONE,
-            CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if(r != CUDA_SUCCESS)
-            return false;
-        c->tmapPtr[s] = src;
-        return true;
-    }
 
     size_t voxel_count(const isaacb_ctx* c)
     {
@@ -622,44 +569,15 @@ namespace
             // an exact power of two whose reciprocal is a normal float
             p.invTotalWeight = (m == 0.5f && e2 > -120 && e2 < 120) ? std::ldexp(1.0f, 1 - e2) : 0.0f;
         }
+        p.volLin = c->volLin;
         p.volQ = c->volQ;
         p.isoAQ = c->isoAQ;
         p.isoLin = c->isoLin;
         p.volFlag = c->volFlag;
         p.isoFlag = c->isoFlag;
-        p.errorFlag = c->errorFlag;
         p.emptyBricks = c->emptyDev;
-        // stage sources with TMA when every active one is 16-byte aligned with
-        // rows of a multiple of 16 bytes and the tiles fit in shared memory
-        p.useTma = 1;
-        int bytes = 0, tx = 0;
         for(int s = 0; s < c->nVol; ++s)
-        {
-            p.tileOffset[s] = -1;
-            if(!(c->weight[s] + c->iso[s] > 0.0f))
-                continue;
-            if(!encode_source_map(c, s))
-            {
-                p.useTma = 0;
-                break;
-            }
-            p.tmap[s] = c->tmap[s];
-            p.tileOffset[s] = bytes;
-            const int tile = 16 * int(c->desc.feature_dim[s]) * kApron * kApron * 4;
-            bytes += (tile + 127) & ~127;
-            tx += tile;
-        }
-        p.tileBytes = bytes;
-        p.txBytes = tx;
-        p.scalarIdem = 1;
-        for(int s = 0; s < c->nVol; ++s)
-        {
             p.adv[s] = c->field[s] ? c->adv[s] : nullptr;
-            if(c->weight[s] + c->iso[s] > 0.0f && (!(p.fdim[s] == 1 && p.chainIdem[s]) || c->field[s]))
-                p.scalarIdem = 0;
-        }
-        if(bytes == 0 || bytes > 160 * 1024)
-            p.useTma = 0;
     }
 } // namespace
 
@@ -766,6 +684,7 @@ extern "C"
         alloc((void**) &c->volQ, nbr * kSlotsPerBrick * sizeof(uint4));
         alloc((void**) &c->isoAQ, nbr * kSlotsPerBrick * sizeof(uint32_t));
         alloc((void**) &c->isoLin, size_t(g.ls[0]) * g.ls[1] * g.ls[2] * sizeof(uint32_t));
+        alloc((void**) &c->volLin, size_t(g.ls[0]) * g.ls[1] * g.ls[2] * sizeof(uint32_t));
         alloc((void**) &c->volFlag, nbr);
         alloc((void**) &c->isoFlag, nbr);
         alloc((void**) &c->color, npix * sizeof(uchar4));
@@ -813,6 +732,7 @@ extern "C"
         cudaFree(c->volQ);
         cudaFree(c->isoAQ);
         cudaFree(c->isoLin);
+        cudaFree(c->volLin);
         cudaFree(c->volFlag);
         cudaFree(c->isoFlag);
         for(int s = 0; s < kMaxSources; ++s)

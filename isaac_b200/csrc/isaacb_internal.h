@@ -7,7 +7,6 @@
 #include "isaacb_device.cuh"
 
 #include <cstdint>
-#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace isaacb
@@ -30,22 +29,14 @@ namespace isaacb
         float totalWeight;
         float invTotalWeight; // 2^-k when totalWeight == 2^k exactly, else 0
         int32_t nonNegative; // every colour sum is finite and >= 0 (tables and weights >= 0, total > 0)
-        int32_t scalarIdem; // every active source is scalar with an all-idem chain
         const uint8_t* adv[kMaxSources]; // field sources: advection texture (localSize, x fastest), else null
+        uint32_t* volLin; // combined volume RGBA8, linear (merge scratch between the two passes)
         uint4* volQ; // combined volume, quad bricks
         uint32_t* isoAQ; // combined iso alpha, quad bricks
         uint32_t* isoLin; // combined iso RGBA8, linear
         uint8_t* volFlag; // per brick: 1 if any texel (apron included) is non-zero
         uint8_t* isoFlag; // per brick: max alpha byte (apron included)
-        int32_t* errorFlag; // set when a bounded wait gives up
         unsigned int* emptyBricks; // count of all-zero bricks (zeroed by the host before the merge)
-        // TMA staging: one 3-D tensor map per source over (X*featureDim, Y, Z) floats,
-        // box (16*featureDim, 9, 9); useTma = 0 selects plain loads
-        int32_t useTma;
-        int32_t tileOffset[kMaxSources]; // byte offset of each source tile in dynamic smem (-1 = not loaded)
-        int32_t tileBytes; // dynamic smem bytes of all tiles (each padded to 128 bytes)
-        int32_t txBytes; // bytes the TMA boxes deliver (the mbarrier's transaction count)
-        alignas(64) CUtensorMap tmap[kMaxSources];
     };
     // CTAs of `kernel` that fit on one SM with `threads` threads and `dynSmem` bytes of
     // dynamic shared memory (registers, threads, shared memory; at most 4)

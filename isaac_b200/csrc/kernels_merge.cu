@@ -4,10 +4,11 @@
 // per-source renderer (UpdatePersistendTextureKernel,
 // lib/isaac/isaac_common_kernel.hpp:432-451).
 //
-// One CTA builds one quad-packed apron brick.  It evaluates the 9^3 texels of
-// the brick (its 8^3 voxels plus the apron on the low side, clamped at the
-// volume border) once into shared memory, then writes the 576 slots as
-// coalesced 16-byte stores.  The per-brick flags feed empty-space skipping.
+// The merge runs in two passes: every voxel is evaluated once, in x-rows, into
+// linear RGBA8 textures; then one CTA per row of quad-packed apron bricks gathers
+// their texels (each brick's 8^3 voxels plus the apron on the low side, clamped at
+// the volume border) and writes the bricks' slots as coalesced 16-byte stores.  The per-brick
+// flags feed empty-space skipping.
 #include "isaacb_blue_noise.h"
 #include "isaacb_internal.h"
 
@@ -121,422 +122,295 @@ namespace isaacb
         v[3] = fdim > 3 ? __ldg(p + 3) : 0.0f;
     }
 
-    // ---------------------------------------------------------------- TMA / mbarrier helpers
-    __device__ __forceinline__ uint32_t smem_u32(const void* p)
+    // ---------------------------------------------------------------- merge, pass 1: per voxel
+    // One thread per voxel (rows of x, so every source read and texture write is
+    // coalesced): the functor chain, the transfer lookup, the field alpha of advected
+    // sources, the weighted sum and the dither, in the reference's source order.  The
+    // results go to two linear RGBA8 textures, the volume (a scratch buffer) and the iso
+    // texture (the iso output).
+
+    // the weighted or iso sources of a merge, in source order
+    struct MergeActive
     {
-        return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-    }
-    __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t phase)
+        int n;
+        const float* src[kMaxSources];
+        const float4* lut[kMaxSources];
+        float weight[kMaxSources];
+        float iso[kMaxSources];
+    };
+
+    // the voxel's volume texel (weighted sum / total weight, dithered) and iso texel
+    __device__ __forceinline__ uint32_t merge_volume_texel(const MergeParams& p, const uint8_t* mask, int x, int y, int z, float4 vc)
     {
-        uint32_t done;
-        asm volatile(
-            "{\n .reg .pred P;\n mbarrier.test_wait.parity.shared::cta.b64 P, [%1], %2;\n selp.u32 %0, 1, 0, P;\n}\n"
-            : "=r"(done)
-            : "r"(bar), "r"(phase)
-            : "memory");
-        return done != 0;
-    }
-    // bounded wait: about 0.5 s at most, then false
-    __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t phase)
-    {
-        for(int it = 0; it < (1 << 22); ++it)
+        if(p.invTotalWeight != 0.0f)
         {
-            if(mbar_test(bar, phase))
-                return true;
-            __nanosleep(100);
+            // totalWeight is a power of two: x * 2^-k is the correctly rounded x / 2^k
+            vc = make_float4(vc.x * p.invTotalWeight, vc.y * p.invTotalWeight, vc.z * p.invTotalWeight, vc.w * p.invTotalWeight);
         }
-        return false;
+        else
+            vc = make_float4(vc.x / p.totalWeight, vc.y / p.totalWeight, vc.z / p.totalWeight, vc.w / p.totalWeight);
+        return p.nonNegative ? dither_rgba_nonneg(p.ditherMode, mask, x, y, z, vc) : dither_rgba(p.ditherMode, mask, x, y, z, vc);
+    }
+    __device__ __forceinline__ uint32_t merge_iso_texel(float4 ic)
+    {
+        return round_byte(ic.x) | (round_byte(ic.y) << 8) | (round_byte(ic.z) << 16) | (round_byte(ic.w) << 24);
     }
 
-    // The 9^3 texels of one brick.  Each thread owns up to three texels (t, t+256,
-    // t+512) and keeps their colour sums in registers while the sources are visited
-    // in the outer loop, so per-source state (chain, table, weights) is uniform and
-    // loaded once.  fetch(s, x, y, z, v) reads a clamped voxel.
-    template<bool ISO, class Fetch>
-    __device__ __forceinline__ void merge_brick(
-        const MergeParams& p,
-        int bx,
-        int by,
-        int bz,
-        uint32_t* volS,
-        uint32_t* isoS,
-        int& anyVol,
-        int& myIsoMax,
-        const uint8_t* mask,
-        Fetch fetch)
-    {
-        constexpr int kPer = 3;
-        constexpr int kTex = kApron * kApron * kApron;
-        const Geom& g = p.g;
-        int xs[kPer], ys[kPer], zs[kPer];
-        float4 vc[kPer], ic[kPer];
-#pragma unroll
-        for(int j = 0; j < kPer; ++j)
-        {
-            const int t = min(int(threadIdx.x) + 256 * j, kTex - 1);
-            const int lx = t % kApron, ly = (t / kApron) % kApron, lz = t / (kApron * kApron);
-            xs[j] = iclamp(bx * 8 - 1 + lx, 0, g.ls[0] - 1);
-            ys[j] = iclamp(by * 8 - 1 + ly, 0, g.ls[1] - 1);
-            zs[j] = iclamp(bz * 8 - 1 + lz, 0, g.ls[2] - 1);
-            vc[j] = make_float4(0, 0, 0, 0);
-            ic[j] = make_float4(0, 0, 0, 0);
-        }
-        const int nMine = int(threadIdx.x) + 512 < kTex ? 3 : 2; // 729 texels over 256 threads
-        for(int s = 0; s < p.nVol; ++s)
-        {
-            const float vw = p.weight[s];
-            const float it = p.iso[s];
-            if(!(vw + it > 0.0f))
-                continue;
-            const float4* lut = p.lut + size_t(s) * p.ts;
-            const uint8_t* adv = p.adv[s];
-            auto accumulate = [&](int j, float val) {
-                float4 c = __ldg(lut + lut_index_fast(val, p.ts));
-                if(adv)
-                {
-                    // field source: alpha blended with the advection texture
-                    // (MergeAdvectionToCombinedTextureIterator, isaac_common_kernel.hpp:664-665)
-                    const size_t vox = (size_t(zs[j]) * g.ls[1] + ys[j]) * g.ls[0] + xs[j];
-                    c.w *= float(__ldg(adv + vox)) / 255.0f;
-                }
-                if(vw > 0.0f)
-                {
-                    const float a = c.w * vw;
-                    vc[j].x += c.x * a;
-                    vc[j].y += c.y * a;
-                    vc[j].z += c.z * a;
-                    vc[j].w += a;
-                }
-                if(ISO && it > 0.0f)
-                {
-                    const float a = c.w / it * 0.5f;
-                    if(ic[j].w < a)
-                        ic[j] = make_float4(c.x, c.y, c.z, a);
-                }
-            };
-            if(p.chainIdem[s] != 0)
-            {
-                // all functors idem: the value is the first component
-#pragma unroll
-                for(int j = 0; j < kPer; ++j)
-                {
-                    if(j < nMine)
-                        accumulate(j, fetch.first(s, xs[j], ys[j], zs[j]));
-                }
-            }
-            else
-            {
-#pragma unroll
-                for(int j = 0; j < kPer; ++j)
-                {
-                    if(j < nMine)
-                    {
-                        float v[4];
-                        fetch(s, xs[j], ys[j], zs[j], v);
-                        accumulate(j, apply_chain(v, p.fdim[s], p.chain[s]));
-                    }
-                }
-            }
-        }
-#pragma unroll
-        for(int j = 0; j < kPer; ++j)
-        {
-            if(j >= nMine)
-                break;
-            const int t = int(threadIdx.x) + 256 * j;
-            float4 c = vc[j];
-            if(p.invTotalWeight != 0.0f)
-            {
-                // totalWeight is a power of two: x * 2^-k is the correctly rounded x / 2^k
-                c = make_float4(c.x * p.invTotalWeight, c.y * p.invTotalWeight, c.z * p.invTotalWeight, c.w * p.invTotalWeight);
-            }
-            else
-            {
-                c = make_float4(c.x / p.totalWeight, c.y / p.totalWeight, c.z / p.totalWeight, c.w / p.totalWeight);
-            }
-            const uint32_t vb = p.nonNegative ? dither_rgba_nonneg(p.ditherMode, mask, xs[j], ys[j], zs[j], c)
-                                              : dither_rgba(p.ditherMode, mask, xs[j], ys[j], zs[j], c);
-            volS[t] = vb;
-            anyVol |= vb != 0u;
-            if(ISO)
-            {
-                const float4 q = ic[j];
-                const uint32_t ib = round_byte(q.x) | (round_byte(q.y) << 8) | (round_byte(q.z) << 16) | (round_byte(q.w) << 24);
-                isoS[t] = ib;
-                myIsoMax = max(myIsoMax, int(ib >> 24));
-            }
-        }
-    }
-
-    // merge_brick for the common case of scalar sources with all-idem chains staged by
-    // TMA: one tile offset per texel serves every source, the value is one shared-memory
-    // load, and the source loop has no per-source layout arithmetic.  Same operations in
-    // the same order as merge_brick, so the bytes are identical.
     template<bool ISO>
-    __device__ __forceinline__ void merge_brick_scalar(
-        const MergeParams& p,
-        int bx,
-        int by,
-        int bz,
-        uint32_t* volS,
-        uint32_t* isoS,
-        int& anyVol,
-        int& myIsoMax,
-        const uint8_t* mask,
-        const unsigned char* tiles,
-        int x0,
-        int y0,
-        int z0)
+    __device__ __forceinline__ void merge_store(const MergeParams& p, const uint8_t* mask, size_t i, int x, int y, int z, float4 vc, float4 ic)
     {
-        constexpr int kPer = 3;
-        constexpr int kTex = kApron * kApron * kApron;
-        const Geom& g = p.g;
-        int xs[kPer], ys[kPer], zs[kPer], off[kPer];
-        float4 vc[kPer], ic[kPer];
-#pragma unroll
-        for(int j = 0; j < kPer; ++j)
+        p.volLin[i] = merge_volume_texel(p, mask, x, y, z, vc);
+        if(ISO)
+            p.isoLin[i] = merge_iso_texel(ic);
+    }
+
+    __device__ __forceinline__ void merge_accumulate(float4 c, float vw, float it, bool iso, float4& vc, float4& ic)
+    {
+        if(vw > 0.0f)
         {
-            const int t = min(int(threadIdx.x) + 256 * j, kTex - 1);
-            const int lz = t / (kApron * kApron);
-            const int r = t - lz * (kApron * kApron);
-            const int ly = r / kApron, lx = r - ly * kApron;
-            xs[j] = iclamp(bx * 8 - 1 + lx, 0, g.ls[0] - 1);
-            ys[j] = iclamp(by * 8 - 1 + ly, 0, g.ls[1] - 1);
-            zs[j] = iclamp(bz * 8 - 1 + lz, 0, g.ls[2] - 1);
-            off[j] = ((zs[j] - z0) * kApron + (ys[j] - y0)) * 16 + (xs[j] - x0);
-            vc[j] = make_float4(0, 0, 0, 0);
-            ic[j] = make_float4(0, 0, 0, 0);
+            const float a = c.w * vw;
+            vc.x += c.x * a;
+            vc.y += c.y * a;
+            vc.z += c.z * a;
+            vc.w += a;
         }
-        const int nMine = int(threadIdx.x) + 512 < kTex ? 3 : 2;
-        const int ts = p.ts;
-        for(int s = 0; s < p.nVol; ++s)
+        if(iso && it > 0.0f)
         {
-            const float vw = p.weight[s];
-            const float it = p.iso[s];
-            if(!(vw + it > 0.0f))
-                continue;
-            const float* tile = reinterpret_cast<const float*>(tiles + p.tileOffset[s]);
-            const float4* lut = p.lut + size_t(s) * ts;
-#pragma unroll
-            for(int j = 0; j < kPer; ++j)
-            {
-                if(j >= nMine)
-                    break;
-                const float4 c = __ldg(lut + lut_index_fast(tile[off[j]], ts));
-                if(vw > 0.0f)
-                {
-                    const float a = c.w * vw;
-                    vc[j].x += c.x * a;
-                    vc[j].y += c.y * a;
-                    vc[j].z += c.z * a;
-                    vc[j].w += a;
-                }
-                if(ISO && it > 0.0f)
-                {
-                    const float a = c.w / it * 0.5f;
-                    if(ic[j].w < a)
-                        ic[j] = make_float4(c.x, c.y, c.z, a);
-                }
-            }
-        }
-#pragma unroll
-        for(int j = 0; j < kPer; ++j)
-        {
-            if(j >= nMine)
-                break;
-            const int t = int(threadIdx.x) + 256 * j;
-            float4 c = vc[j];
-            if(p.invTotalWeight != 0.0f)
-                c = make_float4(c.x * p.invTotalWeight, c.y * p.invTotalWeight, c.z * p.invTotalWeight, c.w * p.invTotalWeight);
-            else
-                c = make_float4(c.x / p.totalWeight, c.y / p.totalWeight, c.z / p.totalWeight, c.w / p.totalWeight);
-            const uint32_t vb = p.nonNegative ? dither_rgba_nonneg(p.ditherMode, mask, xs[j], ys[j], zs[j], c)
-                                              : dither_rgba(p.ditherMode, mask, xs[j], ys[j], zs[j], c);
-            volS[t] = vb;
-            anyVol |= vb != 0u;
-            if(ISO)
-            {
-                const float4 q = ic[j];
-                const uint32_t ib = round_byte(q.x) | (round_byte(q.y) << 8) | (round_byte(q.z) << 16) | (round_byte(q.w) << 24);
-                isoS[t] = ib;
-                myIsoMax = max(myIsoMax, int(ib >> 24));
-            }
+            const float a = c.w / it * 0.5f;
+            if(ic.w < a)
+                ic = make_float4(c.x, c.y, c.z, a);
         }
     }
 
-    // voxel readers of merge_brick: the TMA-staged tile in shared memory, or global memory
-    struct TileFetch
+    // NS (1..4) scalar sources whose chains are all idem, none advected: the sources'
+    // pointers, tables and weights live in registers and all values load up front
+    template<bool ISO, int NS>
+    __global__ void __launch_bounds__(256) k_merge_voxels_n(const __grid_constant__ MergeParams p, const __grid_constant__ MergeActive act)
     {
-        const MergeParams& p;
-        const unsigned char* tiles;
-        int x0, y0, z0;
-        __device__ __forceinline__ const float* at(int s, int x, int y, int z) const
-        {
-            const int fd = p.fdim[s];
-            const float* tile = reinterpret_cast<const float*>(tiles + p.tileOffset[s]);
-            return tile + ((z - z0) * kApron + (y - y0)) * (16 * fd) + (x - x0) * fd;
-        }
-        __device__ __forceinline__ float first(int s, int x, int y, int z) const
-        {
-            return *at(s, x, y, z);
-        }
-        __device__ __forceinline__ void operator()(int s, int x, int y, int z, float (&v)[4]) const
-        {
-            const int fd = p.fdim[s];
-            const float* q = at(s, x, y, z);
-            v[0] = q[0];
-            v[1] = fd > 1 ? q[1] : 0.0f;
-            v[2] = fd > 2 ? q[2] : 0.0f;
-            v[3] = fd > 3 ? q[3] : 0.0f;
-        }
-    };
-    struct GlobalFetch
-    {
-        const MergeParams& p;
-        __device__ __forceinline__ size_t idx(int x, int y, int z) const
-        {
-            return (size_t(z) * p.g.ls[1] + y) * p.g.ls[0] + x;
-        }
-        __device__ __forceinline__ float first(int s, int x, int y, int z) const
-        {
-            return __ldg(p.src[s] + idx(x, y, z) * p.fdim[s]);
-        }
-        __device__ __forceinline__ void operator()(int s, int x, int y, int z, float (&v)[4]) const
-        {
-            read_voxel(p.src[s], p.fdim[s], idx(x, y, z), v);
-        }
-    };
-
-    // One CTA per brick.  With TMA, thread 0 stages each active source's region
-    // [8b-4, 8b+12) x [8b-1, 8b+8) x [8b-1, 8b+8) (the x start rounded down to a
-    // 16-byte boundary; out-of-volume elements are never read) into shared memory
-    // with one cp.async.bulk.tensor per source, completing on an mbarrier.
-    template<bool TMA, bool ISO>
-    __global__ void __launch_bounds__(256, 5) k_merge(const __grid_constant__ MergeParams p)
-    {
-        extern __shared__ __align__(128) unsigned char dsm[];
-        __shared__ uint32_t volS[kApron * kApron * kApron];
-        __shared__ uint32_t isoS[kApron * kApron * kApron];
-        __shared__ int isoMax;
-        __shared__ __align__(8) unsigned long long mbar;
         __shared__ uint8_t sMask[64];
         if(threadIdx.x < 64)
             sMask[threadIdx.x] = p.ditherMode == 2 ? c_dither2[threadIdx.x] : c_dither1[threadIdx.x];
+        __syncthreads();
         const Geom& g = p.g;
-        const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
-        const int x0 = bx * 8 - 4, y0 = by * 8 - 1, z0 = bz * 8 - 1;
-        const uint32_t bar = smem_u32(&mbar);
-        // tiles start on a 128-byte boundary of the dynamic shared memory (128 spare bytes requested)
-        unsigned char* tiles = dsm + ((128u - (smem_u32(dsm) & 127u)) & 127u);
-        if(threadIdx.x == 0)
+        const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
+        if(x >= g.ls[0])
+            return;
+        const size_t i = (size_t(z) * g.ls[1] + y) * g.ls[0] + x;
+        float val[NS];
+#pragma unroll
+        for(int k = 0; k < NS; ++k)
+            val[k] = __ldg(act.src[k] + i);
+        float4 vc = make_float4(0, 0, 0, 0), ic = make_float4(0, 0, 0, 0);
+#pragma unroll
+        for(int k = 0; k < NS; ++k)
+            merge_accumulate(__ldg(act.lut[k] + lut_index_fast(val[k], p.ts)), act.weight[k], act.iso[k], ISO, vc, ic);
+        merge_store<ISO>(p, sMask, i, x, y, z, vc, ic);
+    }
+
+    // As k_merge_voxels_n, four x-adjacent voxels per thread: one 16-byte load per source
+    // and one 16-byte store per texture (rows a multiple of 4 voxels, 16-byte aligned
+    // sources, fewer than 2^32 groups of four)
+    template<bool ISO, int NS>
+    __global__ void __launch_bounds__(256) k_merge_voxels_x4(const __grid_constant__ MergeParams p, const __grid_constant__ MergeActive act)
+    {
+        __shared__ uint8_t sMask[64];
+        if(threadIdx.x < 64)
+            sMask[threadIdx.x] = p.ditherMode == 2 ? c_dither2[threadIdx.x] : c_dither1[threadIdx.x];
+        __syncthreads();
+        const Geom& g = p.g;
+        const uint32_t rowQuads = uint32_t(g.ls[0]) >> 2;
+        const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+        if(q >= rowQuads * uint32_t(g.ls[1]) * uint32_t(g.ls[2]))
+            return;
+        const uint32_t row = q / rowQuads;
+        const int x = int(q - row * rowQuads) * 4;
+        const int y = int(row % uint32_t(g.ls[1])), z = int(row / uint32_t(g.ls[1]));
+        float4 val[NS];
+#pragma unroll
+        for(int k = 0; k < NS; ++k)
+            val[k] = __ldg(reinterpret_cast<const float4*>(act.src[k]) + q);
+        uint32_t vo[4], io[4];
+#pragma unroll
+        for(int j = 0; j < 4; ++j)
         {
-            isoMax = 0;
-            if(TMA)
+            float4 vc = make_float4(0, 0, 0, 0), ic = make_float4(0, 0, 0, 0);
+#pragma unroll
+            for(int k = 0; k < NS; ++k)
             {
-                asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1) : "memory");
-                asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+                const float v = j == 0 ? val[k].x : j == 1 ? val[k].y : j == 2 ? val[k].z : val[k].w;
+                merge_accumulate(__ldg(act.lut[k] + lut_index_fast(v, p.ts)), act.weight[k], act.iso[k], ISO, vc, ic);
             }
+            vo[j] = merge_volume_texel(p, sMask, x + j, y, z, vc);
+            io[j] = ISO ? merge_iso_texel(ic) : 0u;
+        }
+        reinterpret_cast<uint4*>(p.volLin)[q] = make_uint4(vo[0], vo[1], vo[2], vo[3]);
+        if(ISO)
+            reinterpret_cast<uint4*>(p.isoLin)[q] = make_uint4(io[0], io[1], io[2], io[3]);
+    }
+
+    template<bool ISO>
+    __global__ void __launch_bounds__(256) k_merge_voxels(const __grid_constant__ MergeParams p)
+    {
+        __shared__ uint8_t sMask[64];
+        if(threadIdx.x < 64)
+            sMask[threadIdx.x] = p.ditherMode == 2 ? c_dither2[threadIdx.x] : c_dither1[threadIdx.x];
+        __syncthreads();
+        const Geom& g = p.g;
+        const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
+        if(x >= g.ls[0])
+            return;
+        const size_t i = (size_t(z) * g.ls[1] + y) * g.ls[0] + x;
+        float4 vc = make_float4(0, 0, 0, 0), ic = make_float4(0, 0, 0, 0);
+        for(int s = 0; s < p.nVol; ++s)
+        {
+            const float vw = p.weight[s];
+            const float it = p.iso[s];
+            if(!(vw + it > 0.0f))
+                continue;
+            float val;
+            if(p.chainIdem[s] != 0)
+                val = __ldg(p.src[s] + i * p.fdim[s]); // every functor idem: the x component
+            else
+            {
+                float v[4];
+                read_voxel(p.src[s], p.fdim[s], i, v);
+                val = apply_chain(v, p.fdim[s], p.chain[s]);
+            }
+            float4 c = __ldg(p.lut + size_t(s) * p.ts + lut_index_fast(val, p.ts));
+            if(p.adv[s])
+            {
+                // field source: alpha blended with the advection texture
+                // (MergeAdvectionToCombinedTextureIterator, isaac_common_kernel.hpp:664-665)
+                c.w *= float(__ldg(p.adv[s] + i)) / 255.0f;
+            }
+            merge_accumulate(c, vw, it, ISO, vc, ic);
+        }
+        merge_store<ISO>(p, sMask, i, x, y, z, vc, ic);
+    }
+
+    // ---------------------------------------------------------------- merge, pass 2: bricks
+    // One CTA per row of kPackRow bricks along x: the row's (8 kPackRow + 1) x 9 x 9
+    // texels (the bricks' voxels plus the apron on the low side, clamped at the volume
+    // border) from the linear textures into shared memory as rows of 33 texels, then
+    // the bricks' 576-slot quad blocks, contiguous in memory, as coalesced 16-byte
+    // stores.  Warp j scans brick j's 9^3 texels for the flags that drive empty-space
+    // skipping.  Every texel is a copy of a voxel pass 1 computed once.
+    constexpr int kPackRow = 4;
+    constexpr int kPackW = 8 * kPackRow + 1;
+    constexpr int kPackTexels = kPackW * kApron * kApron;
+
+    template<bool ISO>
+    __global__ void __launch_bounds__(256) k_merge_pack(const __grid_constant__ MergeParams p)
+    {
+        __shared__ uint32_t volS[kPackTexels];
+        __shared__ uint32_t isoS[ISO ? kPackTexels : 1];
+        const Geom& g = p.g;
+        const int bx0 = blockIdx.x * kPackRow, by = blockIdx.y, bz = blockIdx.z;
+        const int nRow = min(kPackRow, g.nb[0] - bx0);
+        for(int t = threadIdx.x; t < kPackTexels; t += blockDim.x)
+        {
+            const int lx = t % kPackW;
+            const int r = t / kPackW;
+            const int ly = r % kApron, lz = r / kApron;
+            const int x = iclamp(bx0 * 8 - 1 + lx, 0, g.ls[0] - 1);
+            const int y = iclamp(by * 8 - 1 + ly, 0, g.ls[1] - 1);
+            const int z = iclamp(bz * 8 - 1 + lz, 0, g.ls[2] - 1);
+            const size_t i = (size_t(z) * g.ls[1] + y) * g.ls[0] + x;
+            volS[t] = __ldg(p.volLin + i);
+            if(ISO)
+                isoS[t] = __ldg(p.isoLin + i);
         }
         __syncthreads();
-        if(TMA)
+        const size_t brick0 = (size_t(bz) * g.nb[1] + by) * g.nb[0] + bx0;
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if(warp < nRow)
         {
-            if(threadIdx.x == 0)
+            int anyVol = 0, isoMax = 0;
+            for(int t = lane; t < kApron * kApron * kApron; t += 32)
             {
-                asm volatile(
-                    "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(p.txBytes) : "memory");
-                for(int s = 0; s < p.nVol; ++s)
-                {
-                    if(p.tileOffset[s] < 0)
-                        continue;
-                    const uint32_t dst = smem_u32(tiles + p.tileOffset[s]);
-                    const uint64_t map = reinterpret_cast<uint64_t>(&p.tmap[s]);
-                    asm volatile(
-                        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-                        :
-                        : "r"(dst), "l"(map), "r"(x0 * p.fdim[s]), "r"(y0), "r"(z0), "r"(bar)
-                        : "memory");
-                }
+                const int lx = t % kApron, r = t / kApron;
+                const int o = r * kPackW + warp * 8 + lx; // r = lz * 9 + ly
+                anyVol |= volS[o] != 0u;
+                if(ISO)
+                    isoMax = max(isoMax, int(isoS[o] >> 24));
             }
-            if(!mbar_wait_bounded(bar, 0))
+            anyVol = __any_sync(0xFFFFFFFFu, anyVol);
+            if(ISO)
+                isoMax = int(__reduce_max_sync(0xFFFFFFFFu, unsigned(isoMax)));
+            if(lane == 0)
             {
-                atomicOr(p.errorFlag, 1);
-                // let the copies land before the block's shared memory is released
-                mbar_wait_bounded(bar, 0);
-                return;
+                p.volFlag[brick0 + warp] = anyVol ? 1 : 0;
+                if(!anyVol)
+                    atomicAdd(p.emptyBricks, 1u);
+                if(ISO)
+                    p.isoFlag[brick0 + warp] = uint8_t(isoMax);
             }
         }
-        int anyVol = 0;
-        int myIsoMax = 0;
-        if(TMA)
+        for(int s = threadIdx.x; s < nRow * kSlotsPerBrick; s += blockDim.x)
         {
-            if(p.scalarIdem)
-                merge_brick_scalar<ISO>(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, sMask, tiles, x0, y0, z0);
-            else
-                merge_brick<ISO>(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, sMask, TileFetch{p, tiles, x0, y0, z0});
+            const int j = s / kSlotsPerBrick, sl = s - j * kSlotsPerBrick;
+            const int lx = sl & 7, ly = (sl >> 3) & 7, lz = sl >> 6;
+            const int t = (lz * kApron + ly) * kPackW + j * 8 + lx;
+            p.volQ[brick0 * kSlotsPerBrick + s] = make_uint4(volS[t], volS[t + 1], volS[t + kPackW], volS[t + kPackW + 1]);
+            if(ISO)
+                p.isoAQ[brick0 * kSlotsPerBrick + s] = (isoS[t] >> 24) | ((isoS[t + 1] >> 24) << 8)
+                    | ((isoS[t + kPackW] >> 24) << 16) | ((isoS[t + kPackW + 1] >> 24) << 24);
+        }
+    }
+
+    template<bool ISO>
+    void launch_merge_iso(const MergeParams& p, cudaStream_t s)
+    {
+        const dim3 vgrid((p.g.ls[0] + 255) / 256, p.g.ls[1], p.g.ls[2]);
+        MergeActive act{};
+        bool scalar = true;
+        for(int k = 0; k < p.nVol; ++k)
+        {
+            if(!(p.weight[k] + p.iso[k] > 0.0f))
+                continue;
+            scalar = scalar && p.chainIdem[k] && p.fdim[k] == 1 && !p.adv[k];
+            act.src[act.n] = p.src[k];
+            act.lut[act.n] = p.lut + size_t(k) * p.ts;
+            act.weight[act.n] = p.weight[k];
+            act.iso[act.n] = p.iso[k];
+            act.n++;
+        }
+        bool x4 = (p.g.ls[0] & 3) == 0 && size_t(p.g.ls[0] / 4) * p.g.ls[1] * p.g.ls[2] < (size_t(1) << 32);
+        for(int k = 0; k < act.n; ++k)
+            x4 = x4 && (reinterpret_cast<uintptr_t>(act.src[k]) & 15u) == 0;
+        if(scalar && x4 && act.n >= 1 && act.n <= 4)
+        {
+            const size_t quads = size_t(p.g.ls[0] / 4) * p.g.ls[1] * p.g.ls[2];
+            const unsigned blocks = unsigned((quads + 255) / 256);
+            switch(act.n)
+            {
+            case 1: k_merge_voxels_x4<ISO, 1><<<blocks, 256, 0, s>>>(p, act); break;
+            case 2: k_merge_voxels_x4<ISO, 2><<<blocks, 256, 0, s>>>(p, act); break;
+            case 3: k_merge_voxels_x4<ISO, 3><<<blocks, 256, 0, s>>>(p, act); break;
+            default: k_merge_voxels_x4<ISO, 4><<<blocks, 256, 0, s>>>(p, act); break;
+            }
+        }
+        else if(scalar && act.n >= 1 && act.n <= 4)
+        {
+            switch(act.n)
+            {
+            case 1: k_merge_voxels_n<ISO, 1><<<vgrid, 256, 0, s>>>(p, act); break;
+            case 2: k_merge_voxels_n<ISO, 2><<<vgrid, 256, 0, s>>>(p, act); break;
+            case 3: k_merge_voxels_n<ISO, 3><<<vgrid, 256, 0, s>>>(p, act); break;
+            default: k_merge_voxels_n<ISO, 4><<<vgrid, 256, 0, s>>>(p, act); break;
+            }
         }
         else
-        {
-            merge_brick<ISO>(p, bx, by, bz, volS, isoS, anyVol, myIsoMax, sMask, GlobalFetch{p});
-        }
-        if(ISO)
-            atomicMax(&isoMax, myIsoMax);
-        anyVol = __syncthreads_or(anyVol);
-        const size_t brick = (size_t(bz) * g.nb[1] + by) * g.nb[0] + bx;
-        if(threadIdx.x == 0)
-        {
-            p.volFlag[brick] = anyVol ? 1 : 0;
-            if(!anyVol)
-                atomicAdd(p.emptyBricks, 1u);
-            if(ISO)
-                p.isoFlag[brick] = uint8_t(isoMax);
-        }
-        for(int s = threadIdx.x; s < kSlotsPerBrick; s += blockDim.x)
-        {
-            const int lx = s & 7, ly = (s >> 3) & 7, lz = s >> 6;
-            const int t = (lz * kApron + ly) * kApron + lx;
-            uint4 q = make_uint4(volS[t], volS[t + 1], volS[t + kApron], volS[t + kApron + 1]);
-            p.volQ[brick * kSlotsPerBrick + s] = q;
-            if(ISO)
-            {
-                uint32_t a = (isoS[t] >> 24) | ((isoS[t + 1] >> 24) << 8) | ((isoS[t + kApron] >> 24) << 16)
-                    | ((isoS[t + kApron + 1] >> 24) << 24);
-                p.isoAQ[brick * kSlotsPerBrick + s] = a;
-            }
-        }
-        if(ISO)
-        {
-            // interior voxels 8b..8b+7 of this brick in the linear iso texture
-            for(int t = threadIdx.x; t < 512; t += blockDim.x)
-            {
-                const int lx = t & 7, ly = (t >> 3) & 7, lz = t >> 6;
-                const int x = bx * 8 + lx, y = by * 8 + ly, z = bz * 8 + lz;
-                if(x < g.ls[0] && y < g.ls[1] && z < g.ls[2])
-                    p.isoLin[(size_t(z) * g.ls[1] + y) * g.ls[0] + x]
-                        = isoS[((lz + 1) * kApron + (ly + 1)) * kApron + (lx + 1)];
-            }
-        }
+            k_merge_voxels<ISO><<<vgrid, 256, 0, s>>>(p);
+        k_merge_pack<ISO><<<dim3((p.g.nb[0] + kPackRow - 1) / kPackRow, p.g.nb[1], p.g.nb[2]), 256, 0, s>>>(p);
     }
 
     void launch_merge(const MergeParams& p, cudaStream_t s)
     {
-        dim3 grid(p.g.nb[0], p.g.nb[1], p.g.nb[2]);
-        if(p.useTma)
-        {
-            if(p.writeIso)
-            {
-                cudaFuncSetAttribute(k_merge<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, p.tileBytes + 128);
-                k_merge<true, true><<<grid, 256, p.tileBytes + 128, s>>>(p);
-            }
-            else
-            {
-                cudaFuncSetAttribute(k_merge<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, p.tileBytes + 128);
-                k_merge<true, false><<<grid, 256, p.tileBytes + 128, s>>>(p);
-            }
-        }
-        else if(p.writeIso)
-            k_merge<false, true><<<grid, 256, 0, s>>>(p);
+        if(p.writeIso)
+            launch_merge_iso<true>(p, s);
         else
-            k_merge<false, false><<<grid, 256, 0, s>>>(p);
+            launch_merge_iso<false>(p, s);
     }
 
     // ---------------------------------------------------------------- field-source advection

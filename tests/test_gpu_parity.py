@@ -50,10 +50,12 @@ def test_merge_textures_bit_exact(dither, iso):
 @pytest.mark.parametrize("dither", [0, 1, 2, 3, 5])
 @pytest.mark.parametrize("iso", [False, True])
 @pytest.mark.parametrize("weights", [(2.0, 2.0, 2.0, 2.0), (1.0, 0.0, 3.5, 0.25)])
-def test_merge_scalar_sources_bit_exact(dither, iso, weights):
-    """Scalar sources with all-idem chains take the specialised merge."""
-    fields = scenes.precision_scene(27)
-    s = Scene(n=(27, 27, 27), volumes=[(f.numpy(), True) for f in fields], dither_mode=dither)
+@pytest.mark.parametrize("n", [27, 28])
+def test_merge_scalar_sources_bit_exact(dither, iso, weights, n):
+    """Scalar sources with all-idem chains take the specialised merge: one voxel per
+    thread (27: rows not a multiple of 4) or four per thread (28)."""
+    fields = scenes.precision_scene(n)
+    s = Scene(n=(n, n, n), volumes=[(f.numpy(), True) for f in fields], dither_mode=dither)
     s.transfer = [scenes.transfer_4point(0.7 * i) for i in range(4)]
     s.weights = list(weights)
     if iso:
