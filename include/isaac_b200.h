@@ -406,6 +406,43 @@ isaacb_status isaacb_composite(
     uint8_t* out,
     void* stream);
 
+/* ---- Frame output (IsaacCommunicator::serverSendFrame and setJpegQuality,
+ * lib/isaac/isaac_communicator.hpp:207-290).  An encoder turns a device RGBA8
+ * frame (row 0 = bottom, sent first as the reference does) into the payload
+ * message {"payload": "data:image/jpeg;base64,<text>"} (raw frames:
+ * "data:image/raw-rgba;base64,"), or into the JPEG bytes alone.  The JPEG is
+ * baseline, 2x2-subsampled chroma, standard Huffman tables, alpha dropped (the
+ * reference's libjpeg settings); base64 as boost's base64_from_binary: ceil(8n/6)
+ * characters, no '=' padding.  The returned pointers are pinned memory owned by
+ * the encoder, valid until its next encode call; the calls synchronize `stream`. */
+typedef struct isaacb_encoder isaacb_encoder;
+isaacb_status isaacb_encoder_create(isaacb_encoder** out);
+isaacb_status isaacb_encoder_destroy(isaacb_encoder* encoder);
+/* quality > 100 is clamped to 100 (setJpegQuality); the default is 90 */
+isaacb_status isaacb_encoder_set_quality(isaacb_encoder* encoder, uint32_t quality);
+isaacb_status isaacb_encoder_get_quality(const isaacb_encoder* encoder, uint32_t* quality);
+isaacb_status isaacb_encode_jpeg(
+    isaacb_encoder* encoder,
+    const uint8_t* rgba,
+    uint32_t width,
+    uint32_t height,
+    void* stream,
+    const uint8_t** jpeg,
+    size_t* length);
+/* jpeg = 0 sends the raw RGBA bytes (the reference built with ISAAC_JPEG off);
+ * *length excludes the terminating NUL */
+isaacb_status isaacb_encode_frame(
+    isaacb_encoder* encoder,
+    const uint8_t* rgba,
+    uint32_t width,
+    uint32_t height,
+    int32_t jpeg,
+    void* stream,
+    const char** message,
+    size_t* length);
+/* base64 of n device bytes into ceil(8n/6) device characters (no terminator), asynchronous */
+isaacb_status isaacb_base64(const uint8_t* in, size_t n, char* out, void* stream);
+
 /* Number of kernels the last isaacb_update / isaacb_render enqueued. */
 isaacb_status isaacb_get_launch_count(isaacb_ctx* ctx, uint32_t* update_launches, uint32_t* render_launches);
 

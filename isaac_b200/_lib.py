@@ -188,6 +188,13 @@ SIGNATURES = {
     "isaacb_set_advection": (_i32, [_P, _f, _f, _i32, _i32, _i32]),
     "isaacb_get_advection": (_i32, [_P, _P, _u32, _P]),
     "isaacb_get_noise": (_i32, [_P, _P, _fp]),
+    "isaacb_encoder_create": (_i32, [C.POINTER(_P)]),
+    "isaacb_encoder_destroy": (_i32, [_P]),
+    "isaacb_encoder_set_quality": (_i32, [_P, _u32]),
+    "isaacb_encoder_get_quality": (_i32, [_P, _u32p]),
+    "isaacb_encode_jpeg": (_i32, [_P, _P, _u32, _u32, _P, C.POINTER(_P), C.POINTER(C.c_size_t)]),
+    "isaacb_encode_frame": (_i32, [_P, _P, _u32, _u32, _i32, _P, C.POINTER(_P), C.POINTER(C.c_size_t)]),
+    "isaacb_base64": (_i32, [_P, C.c_size_t, _P, _P]),
 }
 
 

@@ -45,6 +45,7 @@ SOURCES = [
     "recon_gemm.cu",
     "recon.cu",
     "composite.cu",
+    "encode.cu",
 ]
 
 
@@ -95,7 +96,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
         msg = "\n".join(" ".join(c) + "\n" + e for c, e in failures)
         raise RuntimeError("nvcc failed:\n" + msg)
     if force or jobs or _stale(LIB, objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart"]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart", "-lnvjpeg"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -88,6 +88,15 @@ class DefaultController:
     def projections(cls, framebuffer_size) -> list:
         return [cls.updateProjection(framebuffer_size)]
 
+    @staticmethod
+    def handleMessage(message: dict) -> bool:
+        """Controller-specific keys of a server message; True when the projections changed."""
+        return False
+
+    @staticmethod
+    def sendFeedback(root: dict, force: bool = False) -> None:
+        """Controller state for the period message."""
+
 
 class OrthoController:
     """isaac_controllers.hpp:45-63: orthographic, right = 2 w/h, top = 2."""
@@ -103,6 +112,9 @@ class OrthoController:
     def projections(cls, framebuffer_size) -> list:
         return [cls.updateProjection(framebuffer_size)]
 
+    handleMessage = DefaultController.handleMessage
+    sendFeedback = DefaultController.sendFeedback
+
 
 class StereoController:
     """isaac_controllers.hpp:65-117: two off-axis frusta (45 degrees, convergence at
@@ -112,6 +124,21 @@ class StereoController:
 
     def __init__(self, eye_distance: float = 0.06):
         self.eyeDistance = float(eye_distance)
+        self.sendStereo = True
+
+    def handleMessage(self, message: dict) -> bool:
+        """"eye distance" sets the eye separation; True while the new projections
+        have not been reported (updateProjection, isaac_controllers.hpp:75-101)."""
+        if "eye distance" in message:
+            self.sendStereo = True
+            self.eyeDistance = float(message.pop("eye distance"))
+        return self.sendStereo
+
+    def sendFeedback(self, root: dict, force: bool = False) -> None:
+        """"eye distance" in the period message after a change or on request."""
+        if self.sendStereo or force:
+            root["eye distance"] = float(np.float32(self.eyeDistance))  # an isaac_float in the reference
+            self.sendStereo = False
 
     def updateProjection(self, framebuffer_size) -> np.ndarray:
         return self.projections(framebuffer_size)[0]

@@ -7,8 +7,10 @@ per-source transfer functions, weights, iso thresholds, clipping planes, the
 camera (projection, look-at, rotation, distance), ambient occlusion, render and
 dither modes -- and drives the sm_100a kernels through the C ABI
 (``include/isaac_b200.h``).  Steering messages use the reference's JSON keys
-(``lib/isaac.hpp:1345-1803``).  The IceT compositing, MPI and the streaming
-server are not part of this path.
+(``lib/isaac.hpp:1345-1803``).  Given a server URL, the object talks the
+reference's streaming protocol through ``isaac_b200.protocol`` (register, period
+messages with the frame as GPU-encoded JPEG, steering from the server).  The IceT
+compositing and MPI are not part of this path.
 """
 
 from __future__ import annotations
@@ -112,9 +114,13 @@ class IsaacVisualization:
         transfer_size: int = 1024,
         controller=DefaultController,
         compositor=None,
+        server_url: str | None = None,
+        server_port: int = 2458,
+        jpeg: bool = True,
     ):
         self.lib = _lib.load()
         self.name = name
+        self.globalSize = tuple(int(v) for v in global_size)
         self.framebufferSize = tuple(int(v) for v in framebuffer_size)
         self.volumeSources = list(volume_sources)
         self.particleSources = list(particle_sources)
@@ -173,9 +179,39 @@ class IsaacVisualization:
         for j, p in enumerate(self.particleSources):
             self._set_particles(n_vol + j, p)
         self._push_camera()
+        # the streaming server (the reference's communicator of the master rank)
+        self.communicator = None
+        self.session = None
+        self.metadata = None
+        self._frame_dev = None
+        if server_url is not None:
+            from .protocol import IsaacCommunicator, Session
+
+            self.communicator = IsaacCommunicator(server_url, server_port, jpeg)
+            self.session = Session(self, self.communicator)
+
+    def init(self, communicator_setting: int = 0) -> int:
+        """Connect to the server and register (lib/isaac.hpp:1276-1295): 0, or -1 when
+        the connection fails (ReturnAtError = 0; RetryEverySend = 1 keeps retrying on
+        each send).  Without a server URL there is nothing to do."""
+        if self.session is None:
+            return 0
+        return self.session.init(communicator_setting)
+
+    def getJsonMetaRoot(self) -> dict:
+        """The metadata object sent with the next period message."""
+        return self.session.metaRoot if self.session is not None else {}
+
+    def setJpegQuality(self, quality: int):
+        if self.communicator is not None:
+            self.communicator.setJpegQuality(quality)
 
     # ------------------------------------------------------------------ lifecycle
     def close(self):
+        if getattr(self, "session", None) is not None:
+            self.session.exit()
+            self.communicator.close()
+            self.session = None
         if getattr(self, "ctx", None):
             self.lib.isaacb_destroy(self.ctx)
             self.ctx = None
@@ -417,6 +453,18 @@ class IsaacVisualization:
         asynchronous.  ``timing`` records ``mergeTime`` / ``kernelTime`` (ms)
         with CUDA events, like the reference's per-phase counters.
         """
+        if self.session is not None:
+            # the server's messages first, then the frame, then the period message
+            # carrying it (lib/isaac.hpp:1345-1800, 2546-2856)
+            message, asked = self.session.receive()
+            redraw = self.session.apply(message) or asked or redraw
+            self.metadata = message.get("metadata")
+            frame = self._draw(pointer, redraw, host, out, timing, device_frame=True)
+            self.session.send_period(self._frame_dev)
+            return frame
+        return self._draw(pointer, redraw, host, out, timing)
+
+    def _draw(self, pointer, redraw, host, out, timing, device_frame=False):
         for i, s in enumerate(self.volumeSources):
             s.update(self.sourceWeight[i] != 0 or self.sourceIsoThreshold[i] != 0, pointer)
         for j, p in enumerate(self.particleSources):
@@ -427,7 +475,7 @@ class IsaacVisualization:
         st = self._stream()
         if len(self.projections) > 1 or not isinstance(self.compositor, DefaultCompositor):
             return self._multi_pass(host, st)
-        if host and not timing:
+        if host and not timing and not device_frame:
             if out is None:
                 out = np.empty((h, w, 4), dtype=np.uint8)
             check(self.lib.isaacb_frame(self.ctx, st, C.c_void_p(out.ctypes.data)), self.ctx)
@@ -447,6 +495,7 @@ class IsaacVisualization:
             e2.synchronize()
             self.mergeTime = e0.elapsed_time(e1)
             self.kernelTime = e1.elapsed_time(e2)
+        self._frame_dev = dev
         result = dev.cpu().numpy() if host else dev
         self._frame = result
         return result
@@ -467,6 +516,7 @@ class IsaacVisualization:
             images.append(img)
         self._push_camera()
         frame = self.compositor.compose(images)
+        self._frame_dev = frame
         result = frame.cpu().numpy() if host else frame
         self._frame = result
         return result

@@ -89,3 +89,17 @@ def test_batch_rejects_bad_arguments_without_gpu():
     assert lib.isaacb_batch_render(None, None, 0) == _lib.INVALID_ARG
     assert lib.isaacb_batch_launch_graph(None, None) == _lib.NOT_READY
     assert lib.isaacb_batch_set_config(None, None) == _lib.INVALID_ARG
+
+
+def test_encoder_rejects_bad_arguments_without_gpu():
+    lib = _lib.load()
+    ptr, n = C.c_void_p(), C.c_size_t()
+    assert lib.isaacb_encoder_create(None) == _lib.INVALID_ARG
+    assert lib.isaacb_encoder_destroy(None) == _lib.OK
+    assert lib.isaacb_encoder_set_quality(None, 90) == _lib.INVALID_ARG
+    assert lib.isaacb_encoder_get_quality(None, None) == _lib.INVALID_ARG
+    assert lib.isaacb_encode_jpeg(None, None, 16, 16, None, C.byref(ptr), C.byref(n)) == _lib.INVALID_ARG
+    assert lib.isaacb_encode_frame(None, None, 16, 16, 1, None, C.byref(ptr), C.byref(n)) == _lib.INVALID_ARG
+    assert b"isaacb_encode_frame" in lib.isaacb_last_error(None)
+    assert lib.isaacb_base64(None, 5, None, None) == _lib.INVALID_ARG
+    assert lib.isaacb_base64(None, 0, None, None) == _lib.OK
