@@ -62,6 +62,7 @@ def parse_args():
     ap.add_argument("--dtype", default="f32", choices=["f32", "bf16", "f16"], help="per-source renderer bricks")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-stream", action="store_true", help="skip the streamed-frame measurement")
     ap.add_argument("--cpu-rows", type=int, default=0, help="image rows of the CPU sample (0 = auto)")
     return ap.parse_args()
 
@@ -662,6 +663,13 @@ def run_batch(args, world, rank, local, barrier, max_over_ranks):
                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms}
         del host_src, host_frames
 
+    stream_line = None
+    if world == 1 and not args.no_stream:
+        try:
+            stream_line = measure_stream(args, viz)
+        except Exception as ex:  # reported, never required
+            stream_line = {"value": None, "unit": "frames/s", "error": str(ex)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -852,6 +860,13 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks):
                "d2h_bytes_per_step": H * W * 4, "ms_per_step": e2e_ms,
                "note": "inputs per step are the two camera matrices; the sources stay one resident timestep"}
 
+    stream_line = None
+    if world == 1 and not args.no_stream:
+        try:
+            stream_line = measure_stream(args, viz)
+        except Exception as ex:  # reported, never required
+            stream_line = {"value": None, "unit": "frames/s", "error": str(ex)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -906,6 +921,116 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks):
 
         dist.destroy_process_group()
     return 0
+
+
+class _SinkServer:
+    """Loopback stand-in for the ISAAC server: reads and discards what the client sends
+    and acknowledges each message ({"done": uid + 1}) so the done window never blocks."""
+
+    def __init__(self):
+        import socket
+
+        self.listener = socket.socket(socket.AF_INET, socket.SOCK_STREAM)
+        self.listener.bind(("127.0.0.1", 0))
+        self.listener.listen(1)
+        self.port = self.listener.getsockname()[1]
+        self.bytes = 0
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
+
+    def _run(self):
+        import re
+
+        uid = re.compile(rb'\{"uid": (-?\d+)')
+        try:
+            conn, _ = self.listener.accept()
+        except OSError:
+            return
+        tail = b""
+        while True:
+            try:
+                data = conn.recv(1 << 22)
+            except OSError:
+                break
+            if not data:
+                break
+            self.bytes += len(data)
+            buf = tail + data
+            ids = uid.findall(buf)
+            if ids:
+                conn.sendall(json.dumps({"done": int(ids[-1]) + 1}).encode())
+            tail = buf[-32:]
+        conn.close()
+
+    def close(self):
+        self.listener.close()
+
+
+def measure_stream(args, viz) -> dict:
+    """Frames streamed to a loopback server: doVisualization with the protocol on
+    (steering drained, update, draw, GPU JPEG + base64 payload, period message sent), the encode alone on the GPU, and libjpeg (PIL, the
+    reference's encoder at its settings: quality 90, 4:2:0) plus base64 on one host
+    core for the same frame."""
+    import base64
+    import io
+
+    import numpy as np
+    import torch
+
+    sink = _SinkServer()
+    viz.setServer("127.0.0.1", sink.port, jpeg=True)
+    if viz.init() != 0:
+        return {"value": None, "unit": "frames/s", "error": "loopback connect failed"}
+    # host=False: the frame stays on the device (the reference's doVisualization returns
+    # metadata; its frame only goes to the server)
+    for _ in range(2):
+        viz.doVisualization(host=False)
+    n = max(3, min(args.steps, 10))
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    sent0 = sink.bytes
+    e0.record(st)
+    for _ in range(n):
+        viz.doVisualization(host=False)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / n
+    frame = viz._frame_dev
+    enc = viz.communicator.encoder
+    e0.record(st)
+    for _ in range(n):
+        msg = enc.message(frame, True)
+    e1.record(st)
+    torch.cuda.synchronize()
+    enc_ms = e0.elapsed_time(e1) / n
+    jpeg_bytes = len(enc.jpeg(frame))
+    from PIL import Image
+
+    rgb = np.ascontiguousarray(frame.cpu().numpy()[..., :3])
+    k, t = 0, time.perf_counter()
+    while k < 3 or time.perf_counter() - t < 1.0:
+        buf = io.BytesIO()
+        Image.fromarray(rgb).save(buf, format="JPEG", quality=90, subsampling=2)
+        base64.b64encode(buf.getvalue())
+        k += 1
+    cpu_ms = (time.perf_counter() - t) * 1000.0 / k
+    viz.session.exit()
+    viz.communicator.close()
+    viz.session = None
+    sink.close()
+    return {
+        "value": 1000.0 / ms,
+        "unit": "frames/s",
+        "ms_per_step": ms,
+        "step": "doVisualization with the server protocol: update, draw, JPEG payload sent over loopback TCP",
+        "encode_ms": enc_ms,
+        "jpeg_bytes": jpeg_bytes,
+        "message_bytes": len(msg),
+        "bytes_sent_per_frame": (sink.bytes - sent0) / n,
+        "cpu_encode_ms": cpu_ms,
+        "cpu_encode": "libjpeg via PIL, quality 90, 4:2:0, plus base64, 1 host core, same frame",
+    }
 
 
 def main():
@@ -1047,6 +1172,13 @@ def main():
         e2e = {"value": world * 1000.0 / e2e_ms, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": e2e_ms}
 
+    stream_line = None
+    if world == 1 and not args.no_stream:
+        try:
+            stream_line = measure_stream(args, viz)
+        except Exception as ex:  # reported, never required
+            stream_line = {"value": None, "unit": "frames/s", "error": str(ex)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -1085,6 +1217,7 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "stream": stream_line,
             "clocks": clocks,
             "gpu_launches": launches,
         }

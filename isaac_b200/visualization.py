@@ -185,10 +185,15 @@ class IsaacVisualization:
         self.metadata = None
         self._frame_dev = None
         if server_url is not None:
-            from .protocol import IsaacCommunicator, Session
+            self.setServer(server_url, server_port, jpeg)
 
-            self.communicator = IsaacCommunicator(server_url, server_port, jpeg)
-            self.session = Session(self, self.communicator)
+    def setServer(self, url: str, port: int = 2458, jpeg: bool = True):
+        """Attach the streaming server (the constructor's server URL and port); ``init``
+        then connects and registers."""
+        from .protocol import IsaacCommunicator, Session
+
+        self.communicator = IsaacCommunicator(url, port, jpeg)
+        self.session = Session(self, self.communicator)
 
     def init(self, communicator_setting: int = 0) -> int:
         """Connect to the server and register (lib/isaac.hpp:1276-1295): 0, or -1 when
