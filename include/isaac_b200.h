@@ -443,6 +443,23 @@ isaacb_status isaacb_encode_frame(
 /* base64 of n device bytes into ceil(8n/6) device characters (no terminator), asynchronous */
 isaacb_status isaacb_base64(const uint8_t* in, size_t n, char* out, void* stream);
 
+/* Sort-last compositing of several ranks' frames (IceT's ordered BLEND composite,
+ * lib/isaac.hpp:820-826 and 2015-2055).  `images` are `count` (1-64) device RGBA8
+ * buffers of `pixels` pixels each (whole frames, or the same stripe of every
+ * frame); `order` lists the image indices front to back, as the reference's
+ * icetCompositeOrder array does.  Each channel is folded front to back with the
+ * premultiplied "under" operator in 8-bit integers,
+ * acc += src * (255 - acc.alpha) / 255; `background` (4 bytes RGBA, host) goes under
+ * the result when not null.  Asynchronous on `stream`. */
+isaacb_status isaacb_blend_ordered(
+    const uint8_t* const* images,
+    uint32_t count,
+    const int32_t* order,
+    uint32_t pixels,
+    const uint8_t* background,
+    uint8_t* out,
+    void* stream);
+
 /* Number of kernels the last isaacb_update / isaacb_render enqueued. */
 isaacb_status isaacb_get_launch_count(isaacb_ctx* ctx, uint32_t* update_launches, uint32_t* render_launches);
 

@@ -195,6 +195,7 @@ SIGNATURES = {
     "isaacb_encode_jpeg": (_i32, [_P, _P, _u32, _u32, _P, C.POINTER(_P), C.POINTER(C.c_size_t)]),
     "isaacb_encode_frame": (_i32, [_P, _P, _u32, _u32, _i32, _P, C.POINTER(_P), C.POINTER(C.c_size_t)]),
     "isaacb_base64": (_i32, [_P, C.c_size_t, _P, _P]),
+    "isaacb_blend_ordered": (_i32, [C.POINTER(_P), _u32, _i32p, _u32, _P, _P, _P]),
 }
 
 

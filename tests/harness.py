@@ -15,7 +15,9 @@ from oracle import oracle as O
 
 @dataclass
 class Scene:
-    n: tuple = (32, 32, 32)  # local size (x, y, z); global = local
+    n: tuple = (32, 32, 32)  # local size (x, y, z)
+    global_n: tuple | None = None  # global size; None: the local size
+    position: tuple = (0, 0, 0)  # of the local box inside the global volume
     fb: tuple = (64, 48)
     volumes: list = field(default_factory=list)  # list of (array (Z,Y,X[,C]) float32, persistent)
     particles: list = field(default_factory=list)  # list of (offsets, pos, attr, radii or None, const radius)
@@ -68,7 +70,8 @@ def build_oracle(s: Scene, f64: bool = False) -> O.Oracle:
     ]
     pers = [int(p) for _, p in s.volumes] + [1] * len(s.particles)
     o = O.Oracle(
-        s.fb, s.n, s.n, s.particle_cells, (0, 0, 0), s.scale, fdims, pers, nvol, transfer_size=s.transfer_size, f64=f64
+        s.fb, s.global_n or s.n, s.n, s.particle_cells, s.position, s.scale, fdims, pers, nvol,
+        transfer_size=s.transfer_size, f64=f64
     )
     for i, (v, _) in enumerate(s.volumes):
         dt = s.storage[i] if i < len(s.storage) else 0
@@ -103,7 +106,8 @@ def build_gpu(s: Scene):
             )
         )
     viz = IsaacVisualization(
-        "test", s.fb, s.n, s.n, s.particle_cells, (0, 0, 0), vols, parts, scale=s.scale, transfer_size=s.transfer_size
+        "test", s.fb, s.global_n or s.n, s.n, s.particle_cells, s.position, vols, parts, scale=s.scale,
+        transfer_size=s.transfer_size
     )
     viz._keep = (vols, parts)
     _apply_settings(s, viz, oracle=False)

@@ -103,3 +103,13 @@ def test_encoder_rejects_bad_arguments_without_gpu():
     assert b"isaacb_encode_frame" in lib.isaacb_last_error(None)
     assert lib.isaacb_base64(None, 5, None, None) == _lib.INVALID_ARG
     assert lib.isaacb_base64(None, 0, None, None) == _lib.OK
+
+
+def test_blend_rejects_bad_arguments_without_gpu():
+    lib = _lib.load()
+    ptrs = (C.c_void_p * 2)(16, 32)
+    bad = (C.c_int32 * 2)(0, 0)  # not a permutation
+    assert lib.isaacb_blend_ordered(ptrs, 2, bad, 4, None, C.c_void_p(64), None) == _lib.INVALID_ARG
+    assert b"permutation" in lib.isaacb_last_error(None)
+    assert lib.isaacb_blend_ordered(ptrs, 0, bad, 4, None, C.c_void_p(64), None) == _lib.INVALID_ARG
+    assert lib.isaacb_blend_ordered(ptrs, 65, bad, 4, None, C.c_void_p(64), None) == _lib.INVALID_ARG
