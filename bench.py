@@ -565,6 +565,7 @@ def run_batch(args, world, rank, local, barrier, max_over_ranks):
                      "render_ms": tms}
         cfg = batch.config
         batch.capture(update=True)
+        graph_launches = batch.launchCount()  # kernels in the captured batch frame
         for _ in range(args.warmup):
             batch.launchGraph()
     stream.synchronize()
@@ -714,7 +715,7 @@ def run_batch(args, world, rank, local, barrier, max_over_ranks):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clocks,
-            "gpu_launches": args.steps * (len(vis) + 1),
+            "gpu_launches": args.steps * graph_launches,
         }
         print(json.dumps(line), flush=True)
     batch.close()

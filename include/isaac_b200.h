@@ -283,6 +283,9 @@ isaacb_status isaacb_batch_autotune(isaacb_batch* batch, void* stream, isaacb_ba
 /* Ray-march loop trips of the last batch render (counting costs one atomic per warp). */
 isaacb_status isaacb_batch_set_counting(isaacb_batch* batch, int32_t enabled);
 isaacb_status isaacb_batch_get_samples(isaacb_batch* batch, void* stream, uint64_t* samples);
+/* Kernels the last isaacb_batch_render or isaacb_batch_capture enqueued (a graph
+ * launch replays the captured ones). */
+isaacb_status isaacb_batch_get_launch_count(isaacb_batch* batch, uint32_t* launches);
 
 /* ---- Tensor-core convolution (no counterpart in the reference): the
  * building block of the learned frame reconstructor, exposed for testing.

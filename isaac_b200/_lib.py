@@ -171,6 +171,7 @@ SIGNATURES = {
     "isaacb_batch_autotune": (_i32, [_P, _P, C.POINTER(BatchConfig), _fp]),
     "isaacb_batch_set_counting": (_i32, [_P, _i32]),
     "isaacb_batch_get_samples": (_i32, [_P, _P, _u64p]),
+    "isaacb_batch_get_launch_count": (_i32, [_P, _u32p]),
     "isaacb_conv_forward": (_i32, [C.POINTER(ConvArgs), _P]),
     "isaacb_conv_wgrad": (_i32, [C.POINTER(ConvArgs), _P]),
     "isaacb_recon_param_count": (_u32, []),

@@ -93,6 +93,12 @@ class IsaacBatch:
     def setCounting(self, on: bool):
         check(self.lib.isaacb_batch_set_counting(self.handle, int(on)))
 
+    def launchCount(self) -> int:
+        """Kernels the last render or capture enqueued (a graph launch replays the captured ones)."""
+        n = C.c_uint32()
+        check(self.lib.isaacb_batch_get_launch_count(self.handle, C.byref(n)))
+        return int(n.value)
+
     def samples(self) -> int:
         n = C.c_uint64()
         check(self.lib.isaacb_batch_get_samples(self.handle, self._stream(), C.byref(n)))

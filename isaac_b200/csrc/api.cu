@@ -275,6 +275,7 @@ struct isaacb_ctx
     bool isoWritten = false;
     // device buffers
     float4* lutDev = nullptr;
+    float4* lutPre = nullptr; // merge scratch: weighted premultiplied table entries
     float* lutPinned = nullptr;
     cudaEvent_t lutEvent = nullptr;
     uint32_t* volLin = nullptr; // merge scratch: the combined volume, linear RGBA8
@@ -535,6 +536,7 @@ namespace
         p.ditherMode = c->ditherMode;
         p.writeIso = any_iso_active(c) ? 1 : 0;
         p.lut = c->lutDev;
+        p.lutPre = c->lutPre;
         p.totalWeight = 0.0f;
         for(int s = 0; s < c->nVol; ++s)
         {
@@ -677,6 +679,7 @@ extern "C"
                 e = cudaMalloc(p, bytes);
         };
         alloc((void**) &c->lutDev, c->lutHost.size() * sizeof(float));
+        alloc((void**) &c->lutPre, c->lutHost.size() * sizeof(float));
         if(e == cudaSuccess)
             e = cudaMallocHost((void**) &c->lutPinned, c->lutHost.size() * sizeof(float));
         if(e == cudaSuccess)
@@ -725,6 +728,7 @@ extern "C"
         if(!c)
             return ISAACB_OK;
         cudaFree(c->lutDev);
+        cudaFree(c->lutPre);
         if(c->lutPinned)
             cudaFreeHost(c->lutPinned);
         if(c->lutEvent)
@@ -1062,9 +1066,8 @@ extern "C"
                 for(int k = 0; k < ISAACB_TIMING_SLOTS; ++k)
                     c->evUsed[k] = false;
                 PhaseTimer t(c, 0, st);
-                launch_merge(p, st);
+                c->updateLaunches += uint32_t(launch_merge(p, st));
             }
-            c->updateLaunches++;
             // the count comes back asynchronously; a later render reads it once the event completed
             if(cudaEventQuery(c->emptyEvent) != cudaErrorNotReady)
             {
@@ -1457,6 +1460,7 @@ struct isaacb_batch
     cudaGraphExec_t graphExec = nullptr;
     bool graphUpdate = false;
     std::vector<MergeParams> graphMerges; // merge parameters a captured graph holds
+    uint32_t launches = 0; // kernels the last enqueue (direct or captured) issued
 };
 
 namespace
@@ -1574,6 +1578,7 @@ namespace
     // the stream work of one batch frame; `capture` leaves out the read-back of the empty-brick counts
     isaacb_status batch_enqueue(isaacb_batch* b, cudaStream_t st, bool update, bool capture)
     {
+        b->launches = 0;
         if(update)
         {
             for(isaacb_ctx* c : b->ctxs)
@@ -1587,7 +1592,7 @@ namespace
                     b->graphMerges.push_back(p);
                 if(cudaMemsetAsync(c->emptyDev, 0, sizeof(unsigned int), st) != cudaSuccess)
                     return batch_fail(ISAACB_CUDA_ERROR, "isaacb_batch: empty brick counter");
-                launch_merge(p, st);
+                b->launches += uint32_t(launch_merge(p, st));
                 if(!capture && cudaEventQuery(c->emptyEvent) != cudaErrorNotReady)
                 {
                     if(cudaMemcpyAsync(c->emptyPinned, c->emptyDev, sizeof(unsigned int), cudaMemcpyDeviceToHost, st)
@@ -1611,6 +1616,7 @@ namespace
         if(b->counting && cudaMemsetAsync(b->samples, 0, sizeof(unsigned long long), st) != cudaSuccess)
             return batch_fail(ISAACB_CUDA_ERROR, "isaacb_batch: sample counter reset");
         launch_batch(bp, batch_blocks(b), st);
+        b->launches++;
         const cudaError_t e = cudaGetLastError();
         if(e != cudaSuccess)
             return batch_fail(ISAACB_CUDA_ERROR, std::string("isaacb_batch launch: ") + cudaGetErrorString(e));
@@ -1873,6 +1879,14 @@ extern "C"
             return ISAACB_INVALID_ARG;
         b->counting = on != 0;
         batch_drop_graph(b);
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_batch_get_launch_count(isaacb_batch* b, uint32_t* launches)
+    {
+        if(!b || !launches)
+            return ISAACB_INVALID_ARG;
+        *launches = b->launches;
         return ISAACB_OK;
     }
 

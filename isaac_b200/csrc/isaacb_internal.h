@@ -24,6 +24,7 @@ namespace isaacb
         Chain chain[kMaxSources];
         int32_t chainIdem[kMaxSources]; // 1: every functor is idem, the value is the x component
         const float4* lut; // nTotal * ts, source s at s*ts
+        float4* lutPre; // scratch of nTotal * ts: weighted premultiplied entries of the scalar merge
         float weight[kMaxSources];
         float iso[kMaxSources];
         float totalWeight;
@@ -61,7 +62,8 @@ namespace isaacb
         return std::max(1, std::min(n, 4));
     }
 
-    void launch_merge(const MergeParams& p, cudaStream_t s);
+    // returns the number of kernels it launched
+    int launch_merge(const MergeParams& p, cudaStream_t s);
 
     // field-source advection (kernels_merge.cu)
     struct NoiseParams

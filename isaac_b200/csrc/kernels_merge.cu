@@ -137,7 +137,22 @@ namespace isaacb
         const float4* lut[kMaxSources];
         float weight[kMaxSources];
         float iso[kMaxSources];
+        const float4* pre[kMaxSources]; // weighted premultiplied tables (k_merge_premultiply)
     };
+
+    // the volume term of every table entry of the active sources, computed once per merge
+    // instead of once per voxel: a = c.w * weight, (c.x * a, c.y * a, c.z * a, a) -- the
+    // same float products merge_accumulate forms, so the sums that use them are unchanged
+    __global__ void __launch_bounds__(256) k_merge_premultiply(const __grid_constant__ MergeActive act, float4* __restrict__ out, int ts)
+    {
+        const int k = blockIdx.y;
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if(i >= ts)
+            return;
+        const float4 c = __ldg(act.lut[k] + i);
+        const float a = c.w * act.weight[k];
+        out[size_t(k) * ts + i] = make_float4(c.x * a, c.y * a, c.z * a, a);
+    }
 
     // the voxel's volume texel (weighted sum / total weight, dithered) and iso texel
     __device__ __forceinline__ uint32_t merge_volume_texel(const MergeParams& p, const uint8_t* mask, int x, int y, int z, float4 vc)
@@ -207,21 +222,36 @@ namespace isaacb
         merge_store<ISO>(p, sMask, i, x, y, z, vc, ic);
     }
 
-    // As k_merge_voxels_n, four x-adjacent voxels per thread: one 16-byte load per source
-    // and one 16-byte store per texture (rows a multiple of 4 voxels, 16-byte aligned
-    // sources, fewer than 2^32 groups of four)
-    template<bool ISO, int NS>
-    __global__ void __launch_bounds__(256) k_merge_voxels_x4(const __grid_constant__ MergeParams p, const __grid_constant__ MergeActive act)
+    // the largest float below 1: a threshold of exactly 1 behaves as this one below
+    constexpr float kDitherMax = 0x1.fffffep-1f;
+
+    // the non-negative dither with threshold d (already capped at kDitherMax):
+    // floor(s) + (fract(s) > d) == ceil(s - d) for 0 <= d < 1 and s >= 0, and the
+    // round-up subtraction keeps the ceiling exact; ceil by an exact magic-number add
+    __device__ __forceinline__ uint32_t dither_rgba_ceil(float4 c, float d)
     {
-        __shared__ uint8_t sMask[64];
-        if(threadIdx.x < 64)
-            sMask[threadIdx.x] = p.ditherMode == 2 ? c_dither2[threadIdx.x] : c_dither1[threadIdx.x];
-        __syncthreads();
+        const float v[4] = {c.x, c.y, c.z, c.w};
+        uint32_t out = 0;
+#pragma unroll
+        for(int i = 0; i < 4; ++i)
+        {
+            const float s = fminf(v[i] * 255.0f, 257.0f);
+            const float t = __fadd_ru(__fsub_ru(s, d), 12582912.0f);
+            out |= uint32_t(min(__float_as_int(t) - 0x4B400000, 255)) << (8 * i);
+        }
+        return out;
+    }
+
+    // Four x-adjacent voxels (the quad q of rows of rowQuads) of the scalar merge: one
+    // 16-byte load per source and one 16-byte store per texture.  The transfer index is
+    // round(clamp(v * ts, 0, ts - 1)) (the same as clamping the rounded value), with the
+    // rounding as a round-down add of 0.5 and an exact magic-number floor; `entry(k, bits)`
+    // returns source k's table entry for the floor's float bits (0x4B400000 + index).
+    // Without iso output the tables are the premultiplied ones (k_merge_premultiply).
+    template<bool ISO, int NS, class Entry>
+    __device__ __forceinline__ void merge_quad(const MergeParams& p, const MergeActive& act, const uint8_t* sMask, uint32_t q, uint32_t rowQuads, Entry entry)
+    {
         const Geom& g = p.g;
-        const uint32_t rowQuads = uint32_t(g.ls[0]) >> 2;
-        const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-        if(q >= rowQuads * uint32_t(g.ls[1]) * uint32_t(g.ls[2]))
-            return;
         const uint32_t row = q / rowQuads;
         const int x = int(q - row * rowQuads) * 4;
         const int y = int(row % uint32_t(g.ls[1])), z = int(row / uint32_t(g.ls[1]));
@@ -229,6 +259,11 @@ namespace isaacb
 #pragma unroll
         for(int k = 0; k < NS; ++k)
             val[k] = __ldg(reinterpret_cast<const float4*>(act.src[k]) + q);
+        const float tsf = float(p.ts), tsMax = float(p.ts - 1);
+        // the four thresholds of modes 1 and 2: x is a multiple of 4, so they are the mask
+        // bytes (y&3)*4 + (z&3)*16 + 0..3, one aligned word
+        const bool fast = p.nonNegative && p.ditherMode != 0;
+        const uint32_t maskWord = *reinterpret_cast<const uint32_t*>(sMask + (y & 3) * 4 + (z & 3) * 16);
         uint32_t vo[4], io[4];
 #pragma unroll
         for(int j = 0; j < 4; ++j)
@@ -238,14 +273,80 @@ namespace isaacb
             for(int k = 0; k < NS; ++k)
             {
                 const float v = j == 0 ? val[k].x : j == 1 ? val[k].y : j == 2 ? val[k].z : val[k].w;
-                merge_accumulate(__ldg(act.lut[k] + lut_index_fast(v, p.ts)), act.weight[k], act.iso[k], ISO, vc, ic);
+                const float xi = fminf(fmaxf(v * tsf, 0.0f), tsMax);
+                const float t = __fadd_rd(__fadd_rd(xi, 0.5f), 12582912.0f);
+                const float4 c = entry(k, __float_as_uint(t));
+                if(ISO)
+                    merge_accumulate(c, act.weight[k], act.iso[k], true, vc, ic);
+                else if(act.weight[k] > 0.0f)
+                {
+                    vc.x += c.x;
+                    vc.y += c.y;
+                    vc.z += c.z;
+                    vc.w += c.w;
+                }
             }
-            vo[j] = merge_volume_texel(p, sMask, x + j, y, z, vc);
+            if(fast)
+            {
+                if(p.invTotalWeight != 0.0f)
+                    vc = make_float4(vc.x * p.invTotalWeight, vc.y * p.invTotalWeight, vc.z * p.invTotalWeight, vc.w * p.invTotalWeight);
+                else
+                    vc = make_float4(vc.x / p.totalWeight, vc.y / p.totalWeight, vc.z / p.totalWeight, vc.w / p.totalWeight);
+                const float d = (p.ditherMode == 1 || p.ditherMode == 2)
+                    ? float((maskWord >> (8 * j)) & 0xFFu) / 64.0f
+                    : dither_threshold(p.ditherMode, sMask, x + j, y, z);
+                vo[j] = dither_rgba_ceil(vc, fminf(d, kDitherMax));
+            }
+            else
+                vo[j] = merge_volume_texel(p, sMask, x + j, y, z, vc);
             io[j] = ISO ? merge_iso_texel(ic) : 0u;
         }
         reinterpret_cast<uint4*>(p.volLin)[q] = make_uint4(vo[0], vo[1], vo[2], vo[3]);
         if(ISO)
             reinterpret_cast<uint4*>(p.isoLin)[q] = make_uint4(io[0], io[1], io[2], io[3]);
+    }
+
+    // As k_merge_voxels_n, four x-adjacent voxels per thread (rows a multiple of 4 voxels,
+    // 16-byte aligned sources, fewer than 2^32 groups of four); table entries from global
+    // memory through a pointer biased so that the floor's bits address them
+    template<bool ISO, int NS>
+    __global__ void __launch_bounds__(256) k_merge_voxels_x4(const __grid_constant__ MergeParams p, const __grid_constant__ MergeActive act)
+    {
+        __shared__ __align__(4) uint8_t sMask[64];
+        if(threadIdx.x < 64)
+            sMask[threadIdx.x] = p.ditherMode == 2 ? c_dither2[threadIdx.x] : c_dither1[threadIdx.x];
+        __syncthreads();
+        const uint32_t rowQuads = uint32_t(p.g.ls[0]) >> 2;
+        const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+        if(q >= rowQuads * uint32_t(p.g.ls[1]) * uint32_t(p.g.ls[2]))
+            return;
+        merge_quad<ISO, NS>(p, act, sMask, q, rowQuads, [&](int k, uint32_t bits) {
+            const float4* table = ISO ? act.lut[k] : act.pre[k];
+            const char* biased = reinterpret_cast<const char*>(table) - size_t(0x4B400000u) * sizeof(float4);
+            return __ldg(reinterpret_cast<const float4*>(biased + size_t(bits) * sizeof(float4)));
+        });
+    }
+
+    // The same without iso output, with the NS premultiplied tables (NS * ts entries) in
+    // shared memory: persistent CTAs load them once and walk the quads, so each of the
+    // four gathers per voxel reads shared memory instead of scattering over L1 sectors.
+    template<int NS>
+    __global__ void __launch_bounds__(512) k_merge_voxels_x4_smem(const __grid_constant__ MergeParams p, const __grid_constant__ MergeActive act)
+    {
+        extern __shared__ float4 sLut[];
+        __shared__ __align__(4) uint8_t sMask[64];
+        if(threadIdx.x < 64)
+            sMask[threadIdx.x] = p.ditherMode == 2 ? c_dither2[threadIdx.x] : c_dither1[threadIdx.x];
+        const int ts = p.ts;
+        for(int i = threadIdx.x; i < NS * ts; i += blockDim.x)
+            sLut[i] = __ldg(p.lutPre + i);
+        __syncthreads();
+        const uint32_t rowQuads = uint32_t(p.g.ls[0]) >> 2;
+        const uint32_t quads = rowQuads * uint32_t(p.g.ls[1]) * uint32_t(p.g.ls[2]);
+        for(uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < quads; q += gridDim.x * blockDim.x)
+            merge_quad<false, NS>(p, act, sMask, q, rowQuads, [&](int k, uint32_t bits) {
+                return sLut[k * ts + int(bits - 0x4B400000u)];
+            });
     }
 
     template<bool ISO>
@@ -289,77 +390,136 @@ namespace isaacb
     }
 
     // ---------------------------------------------------------------- merge, pass 2: bricks
-    // One CTA per row of kPackRow bricks along x: the row's (8 kPackRow + 1) x 9 x 9
-    // texels (the bricks' voxels plus the apron on the low side, clamped at the volume
-    // border) from the linear textures into shared memory as rows of 33 texels, then
-    // the bricks' 576-slot quad blocks, contiguous in memory, as coalesced 16-byte
-    // stores.  Warp j scans brick j's 9^3 texels for the flags that drive empty-space
-    // skipping.  Every texel is a copy of a voxel pass 1 computed once.
+    // One CTA per row of kPackRow = 4 bricks along x.  The row's 33 x 9 x 9 texels (the
+    // bricks' voxels plus the apron on the low side, clamped at the volume border) come
+    // from the linear textures into shared memory, one texel row per warp with the lanes
+    // along x.  A lane's texels all have the same x, so they belong to the same one or two
+    // bricks: the lane keeps one "any non-zero" bit and one maximum alpha byte, and a warp
+    // reduction per brick gives the flags that drive empty-space skipping.  Then the 4
+    // bricks' 576-slot quad blocks, contiguous in memory, go out as 16-byte stores: thread
+    // (lx, ly) walks the slot layers lz of all 4 bricks, and slot index = layer * 64 + lxy.
+    // Every texel is a copy of a voxel pass 1 computed once.
     constexpr int kPackRow = 4;
-    constexpr int kPackW = 8 * kPackRow + 1;
-    constexpr int kPackTexels = kPackW * kApron * kApron;
+    constexpr int kPackW = 8 * kPackRow + 1; // texels per staged row
+    constexpr int kPackPitch = 40; // row pitch in words: 40 = 8 mod 32 keeps the quad reads conflict-free
+    constexpr int kPackRows = kApron * kApron; // (ly, lz) rows
+    constexpr int kPackWords = kPackRows * kPackPitch;
 
     template<bool ISO>
     __global__ void __launch_bounds__(256) k_merge_pack(const __grid_constant__ MergeParams p)
     {
-        __shared__ uint32_t volS[kPackTexels];
-        __shared__ uint32_t isoS[ISO ? kPackTexels : 1];
+        __shared__ uint32_t volS[kPackWords];
+        __shared__ uint32_t isoS[ISO ? kPackWords : 1];
+        __shared__ int anyS[kPackRow], isoMaxS[kPackRow];
         const Geom& g = p.g;
         const int bx0 = blockIdx.x * kPackRow, by = blockIdx.y, bz = blockIdx.z;
         const int nRow = min(kPackRow, g.nb[0] - bx0);
-        for(int t = threadIdx.x; t < kPackTexels; t += blockDim.x)
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if(threadIdx.x < kPackRow)
         {
-            const int lx = t % kPackW;
-            const int r = t / kPackW;
-            const int ly = r % kApron, lz = r / kApron;
-            const int x = iclamp(bx0 * 8 - 1 + lx, 0, g.ls[0] - 1);
+            anyS[threadIdx.x] = 0;
+            isoMaxS[threadIdx.x] = 0;
+        }
+        // staged texel lx belongs to the bricks j with 8j <= lx <= 8j + 8
+        const int x0 = iclamp(bx0 * 8 - 1 + lane, 0, g.ls[0] - 1);
+        const int x32 = iclamp(bx0 * 8 + 31, 0, g.ls[0] - 1); // lx = 32, brick 3, read by lane 0
+        const int jlo = lane >= 1 ? (lane - 1) >> 3 : 0, jhi = min(lane >> 3, kPackRow - 1);
+        int laneAny = 0, laneIso = 0, any32 = 0, iso32 = 0;
+        for(int r = warp; r < kPackRows; r += 8)
+        {
+            const int lz = r / kApron, ly = r - lz * kApron;
             const int y = iclamp(by * 8 - 1 + ly, 0, g.ls[1] - 1);
             const int z = iclamp(bz * 8 - 1 + lz, 0, g.ls[2] - 1);
-            const size_t i = (size_t(z) * g.ls[1] + y) * g.ls[0] + x;
-            volS[t] = __ldg(p.volLin + i);
+            const size_t row = (size_t(z) * g.ls[1] + y) * g.ls[0];
+            const uint32_t v = __ldg(p.volLin + row + x0);
+            volS[r * kPackPitch + lane] = v;
+            laneAny |= v != 0u;
             if(ISO)
-                isoS[t] = __ldg(p.isoLin + i);
+            {
+                const uint32_t w = __ldg(p.isoLin + row + x0);
+                isoS[r * kPackPitch + lane] = w;
+                laneIso = max(laneIso, int(w >> 24));
+            }
+            if(lane == 0)
+            {
+                const uint32_t v2 = __ldg(p.volLin + row + x32);
+                volS[r * kPackPitch + 32] = v2;
+                any32 |= v2 != 0u;
+                if(ISO)
+                {
+                    const uint32_t w2 = __ldg(p.isoLin + row + x32);
+                    isoS[r * kPackPitch + 32] = w2;
+                    iso32 = max(iso32, int(w2 >> 24));
+                }
+            }
+        }
+        __syncthreads(); // the flag slots are initialised
+#pragma unroll
+        for(int j = 0; j < kPackRow; ++j)
+        {
+            const bool mine = jlo <= j && j <= jhi;
+            const bool extra = j == kPackRow - 1 && lane == 0; // the lx = 32 texel
+            const int a = __any_sync(0xFFFFFFFFu, (mine && laneAny) || (extra && any32));
+            int m = 0;
+            if(ISO)
+                m = int(__reduce_max_sync(0xFFFFFFFFu, unsigned(max(mine ? laneIso : 0, extra ? iso32 : 0))));
+            if(lane == 0)
+            {
+                if(a)
+                    atomicOr(&anyS[j], 1);
+                if(ISO && m)
+                    atomicMax(&isoMaxS[j], m);
+            }
         }
         __syncthreads();
         const size_t brick0 = (size_t(bz) * g.nb[1] + by) * g.nb[0] + bx0;
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        if(warp < nRow)
+        if(threadIdx.x < nRow)
         {
-            int anyVol = 0, isoMax = 0;
-            for(int t = lane; t < kApron * kApron * kApron; t += 32)
-            {
-                const int lx = t % kApron, r = t / kApron;
-                const int o = r * kPackW + warp * 8 + lx; // r = lz * 9 + ly
-                anyVol |= volS[o] != 0u;
-                if(ISO)
-                    isoMax = max(isoMax, int(isoS[o] >> 24));
-            }
-            anyVol = __any_sync(0xFFFFFFFFu, anyVol);
+            const int j = threadIdx.x;
+            p.volFlag[brick0 + j] = anyS[j] ? 1 : 0;
+            if(!anyS[j])
+                atomicAdd(p.emptyBricks, 1u);
             if(ISO)
-                isoMax = int(__reduce_max_sync(0xFFFFFFFFu, unsigned(isoMax)));
-            if(lane == 0)
-            {
-                p.volFlag[brick0 + warp] = anyVol ? 1 : 0;
-                if(!anyVol)
-                    atomicAdd(p.emptyBricks, 1u);
-                if(ISO)
-                    p.isoFlag[brick0 + warp] = uint8_t(isoMax);
-            }
+                p.isoFlag[brick0 + j] = uint8_t(isoMaxS[j]);
         }
-        for(int s = threadIdx.x; s < nRow * kSlotsPerBrick; s += blockDim.x)
+        const int lxy = threadIdx.x & 63;
+        const int base = (lxy >> 3) * kPackPitch + (lxy & 7);
+        for(int layer = threadIdx.x >> 6; layer < nRow * kApron; layer += 4)
         {
-            const int j = s / kSlotsPerBrick, sl = s - j * kSlotsPerBrick;
-            const int lx = sl & 7, ly = (sl >> 3) & 7, lz = sl >> 6;
-            const int t = (lz * kApron + ly) * kPackW + j * 8 + lx;
-            p.volQ[brick0 * kSlotsPerBrick + s] = make_uint4(volS[t], volS[t + 1], volS[t + kPackW], volS[t + kPackW + 1]);
+            const int j = layer / kApron, lz = layer - j * kApron;
+            const int t = lz * (kApron * kPackPitch) + base + 8 * j;
+            const size_t slot = brick0 * kSlotsPerBrick + size_t(layer) * 64 + lxy;
+            p.volQ[slot] = make_uint4(volS[t], volS[t + 1], volS[t + kPackPitch], volS[t + kPackPitch + 1]);
             if(ISO)
-                p.isoAQ[brick0 * kSlotsPerBrick + s] = (isoS[t] >> 24) | ((isoS[t + 1] >> 24) << 8)
-                    | ((isoS[t + kPackW] >> 24) << 16) | ((isoS[t + kPackW + 1] >> 24) << 24);
+                p.isoAQ[slot] = (isoS[t] >> 24) | ((isoS[t + 1] >> 24) << 8) | ((isoS[t + kPackPitch] >> 24) << 16)
+                    | ((isoS[t + kPackPitch + 1] >> 24) << 24);
         }
     }
 
+    // largest set of premultiplied tables the persistent merge keeps in shared memory
+    // (4 sources x 1024 entries = 64 KiB leaves room for two 512-thread CTAs per SM)
+    constexpr size_t kMergeSmemTables = 96 * 1024;
+
+    template<int NS>
+    void launch_x4_smem(const MergeParams& p, const MergeActive& act, size_t quads, size_t tableBytes, cudaStream_t s)
+    {
+        // the opt-in to more than 48 KiB of dynamic shared memory, once per device
+        static uint64_t configured = 0;
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        if(dev < 64 && !((configured >> dev) & 1u)
+           && cudaFuncSetAttribute(k_merge_voxels_x4_smem<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMergeSmemTables))
+               == cudaSuccess)
+            configured |= uint64_t(1) << dev;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const size_t resident = size_t(sms) * ctas_per_sm(k_merge_voxels_x4_smem<NS>, 512, tableBytes);
+        const size_t grid = std::max<size_t>(1, std::min(resident, (quads + 511) / 512));
+        k_merge_voxels_x4_smem<NS><<<unsigned(grid), 512, tableBytes, s>>>(p, act);
+    }
+
+    // returns the number of kernels launched
     template<bool ISO>
-    void launch_merge_iso(const MergeParams& p, cudaStream_t s)
+    int launch_merge_iso(const MergeParams& p, cudaStream_t s)
     {
         const dim3 vgrid((p.g.ls[0] + 255) / 256, p.g.ls[1], p.g.ls[2]);
         MergeActive act{};
@@ -378,16 +538,38 @@ namespace isaacb
         bool x4 = (p.g.ls[0] & 3) == 0 && size_t(p.g.ls[0] / 4) * p.g.ls[1] * p.g.ls[2] < (size_t(1) << 32);
         for(int k = 0; k < act.n; ++k)
             x4 = x4 && (reinterpret_cast<uintptr_t>(act.src[k]) & 15u) == 0;
+        int launches = 2;
         if(scalar && x4 && act.n >= 1 && act.n <= 4)
         {
             const size_t quads = size_t(p.g.ls[0] / 4) * p.g.ls[1] * p.g.ls[2];
             const unsigned blocks = unsigned((quads + 255) / 256);
-            switch(act.n)
+            if(!ISO)
             {
-            case 1: k_merge_voxels_x4<ISO, 1><<<blocks, 256, 0, s>>>(p, act); break;
-            case 2: k_merge_voxels_x4<ISO, 2><<<blocks, 256, 0, s>>>(p, act); break;
-            case 3: k_merge_voxels_x4<ISO, 3><<<blocks, 256, 0, s>>>(p, act); break;
-            default: k_merge_voxels_x4<ISO, 4><<<blocks, 256, 0, s>>>(p, act); break;
+                for(int k = 0; k < act.n; ++k)
+                    act.pre[k] = p.lutPre + size_t(k) * p.ts;
+                k_merge_premultiply<<<dim3((p.ts + 255) / 256, act.n), 256, 0, s>>>(act, p.lutPre, p.ts);
+                launches++;
+            }
+            const size_t tableBytes = size_t(act.n) * p.ts * sizeof(float4);
+            if(!ISO && tableBytes <= kMergeSmemTables)
+            {
+                switch(act.n)
+                {
+                case 1: launch_x4_smem<1>(p, act, quads, tableBytes, s); break;
+                case 2: launch_x4_smem<2>(p, act, quads, tableBytes, s); break;
+                case 3: launch_x4_smem<3>(p, act, quads, tableBytes, s); break;
+                default: launch_x4_smem<4>(p, act, quads, tableBytes, s); break;
+                }
+            }
+            else
+            {
+                switch(act.n)
+                {
+                case 1: k_merge_voxels_x4<ISO, 1><<<blocks, 256, 0, s>>>(p, act); break;
+                case 2: k_merge_voxels_x4<ISO, 2><<<blocks, 256, 0, s>>>(p, act); break;
+                case 3: k_merge_voxels_x4<ISO, 3><<<blocks, 256, 0, s>>>(p, act); break;
+                default: k_merge_voxels_x4<ISO, 4><<<blocks, 256, 0, s>>>(p, act); break;
+                }
             }
         }
         else if(scalar && act.n >= 1 && act.n <= 4)
@@ -403,14 +585,12 @@ namespace isaacb
         else
             k_merge_voxels<ISO><<<vgrid, 256, 0, s>>>(p);
         k_merge_pack<ISO><<<dim3((p.g.nb[0] + kPackRow - 1) / kPackRow, p.g.nb[1], p.g.nb[2]), 256, 0, s>>>(p);
+        return launches;
     }
 
-    void launch_merge(const MergeParams& p, cudaStream_t s)
+    int launch_merge(const MergeParams& p, cudaStream_t s)
     {
-        if(p.writeIso)
-            launch_merge_iso<true>(p, s);
-        else
-            launch_merge_iso<false>(p, s);
+        return p.writeIso ? launch_merge_iso<true>(p, s) : launch_merge_iso<false>(p, s);
     }
 
     // ---------------------------------------------------------------- field-source advection

@@ -89,6 +89,7 @@ def test_batch_rejects_bad_arguments_without_gpu():
     assert lib.isaacb_batch_render(None, None, 0) == _lib.INVALID_ARG
     assert lib.isaacb_batch_launch_graph(None, None) == _lib.NOT_READY
     assert lib.isaacb_batch_set_config(None, None) == _lib.INVALID_ARG
+    assert lib.isaacb_batch_get_launch_count(None, None) == _lib.INVALID_ARG
 
 
 def test_encoder_rejects_bad_arguments_without_gpu():

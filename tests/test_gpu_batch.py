@@ -66,6 +66,8 @@ def test_batch_matches_single_views(setup):
     _, _, batch, refs = setup
     batch.render(update=True)
     _check(batch, refs)
+    # three merges of two kernels (pass 1, pass 2) and the one batch render
+    assert batch.launchCount() == 3 * 2 + 1
 
 
 @pytest.mark.parametrize("tile", [(32, 8), (16, 16), (8, 32), (64, 4)])

@@ -68,6 +68,8 @@ def test_merge_scalar_sources_bit_exact(dither, iso, weights, n):
     gv, gi = viz.combinedTextures()
     assert np.array_equal(gv, rv)
     assert np.array_equal(gi, ri)
+    # the four-voxel path without iso output premultiplies the tables first
+    assert viz.launchCounts()[0] == (3 if n == 28 and not iso else 2)
 
 
 def test_merge_weights_and_zero_total():
