@@ -404,6 +404,16 @@ namespace isaacb
     constexpr int kPackPitch = 40; // row pitch in words: 40 = 8 mod 32 keeps the quad reads conflict-free
     constexpr int kPackRows = kApron * kApron; // (ly, lz) rows
     constexpr int kPackWords = kPackRows * kPackPitch;
+    constexpr int kRowsPerWarp = (kPackRows + 7) / 8; // 8 warps share the 81 rows
+
+    // linear index of the first voxel of staged row r = lz * 9 + ly of brick row (by, bz)
+    __device__ __forceinline__ size_t pack_row(const Geom& g, int by, int bz, int r)
+    {
+        const int lz = r / kApron, ly = r - lz * kApron;
+        const int y = iclamp(by * 8 - 1 + ly, 0, g.ls[1] - 1);
+        const int z = iclamp(bz * 8 - 1 + lz, 0, g.ls[2] - 1);
+        return (size_t(z) * g.ls[1] + y) * g.ls[0];
+    }
 
     template<bool ISO>
     __global__ void __launch_bounds__(256) k_merge_pack(const __grid_constant__ MergeParams p)
@@ -425,31 +435,50 @@ namespace isaacb
         const int x32 = iclamp(bx0 * 8 + 31, 0, g.ls[0] - 1); // lx = 32, brick 3, read by lane 0
         const int jlo = lane >= 1 ? (lane - 1) >> 3 : 0, jhi = min(lane >> 3, kPackRow - 1);
         int laneAny = 0, laneIso = 0, any32 = 0, iso32 = 0;
-        for(int r = warp; r < kPackRows; r += 8)
+        // all of the warp's row loads are issued before any is used, so that enough
+        // bytes are in flight to cover the memory latency
+        // (lane 0 also reads the row's 33rd texel, lx = 32)
+        uint32_t v[kRowsPerWarp], w[kRowsPerWarp], v2[kRowsPerWarp], w2[kRowsPerWarp];
+#pragma unroll
+        for(int i = 0; i < kRowsPerWarp; ++i)
         {
-            const int lz = r / kApron, ly = r - lz * kApron;
-            const int y = iclamp(by * 8 - 1 + ly, 0, g.ls[1] - 1);
-            const int z = iclamp(bz * 8 - 1 + lz, 0, g.ls[2] - 1);
-            const size_t row = (size_t(z) * g.ls[1] + y) * g.ls[0];
-            const uint32_t v = __ldg(p.volLin + row + x0);
-            volS[r * kPackPitch + lane] = v;
-            laneAny |= v != 0u;
-            if(ISO)
+            const int r = warp + 8 * i;
+            if(r < kPackRows)
             {
-                const uint32_t w = __ldg(p.isoLin + row + x0);
-                isoS[r * kPackPitch + lane] = w;
-                laneIso = max(laneIso, int(w >> 24));
+                const size_t row = pack_row(g, by, bz, r);
+                v[i] = __ldg(p.volLin + row + x0);
+                if(ISO)
+                    w[i] = __ldg(p.isoLin + row + x0);
+                if(lane == 0)
+                {
+                    v2[i] = __ldg(p.volLin + row + x32);
+                    if(ISO)
+                        w2[i] = __ldg(p.isoLin + row + x32);
+                }
             }
-            if(lane == 0)
+        }
+#pragma unroll
+        for(int i = 0; i < kRowsPerWarp; ++i)
+        {
+            const int r = warp + 8 * i;
+            if(r < kPackRows)
             {
-                const uint32_t v2 = __ldg(p.volLin + row + x32);
-                volS[r * kPackPitch + 32] = v2;
-                any32 |= v2 != 0u;
+                volS[r * kPackPitch + lane] = v[i];
+                laneAny |= v[i] != 0u;
                 if(ISO)
                 {
-                    const uint32_t w2 = __ldg(p.isoLin + row + x32);
-                    isoS[r * kPackPitch + 32] = w2;
-                    iso32 = max(iso32, int(w2 >> 24));
+                    isoS[r * kPackPitch + lane] = w[i];
+                    laneIso = max(laneIso, int(w[i] >> 24));
+                }
+                if(lane == 0)
+                {
+                    volS[r * kPackPitch + 32] = v2[i];
+                    any32 |= v2[i] != 0u;
+                    if(ISO)
+                    {
+                        isoS[r * kPackPitch + 32] = w2[i];
+                        iso32 = max(iso32, int(w2[i] >> 24));
+                    }
                 }
             }
         }
@@ -805,8 +834,149 @@ namespace isaacb
         }
     }
 
+    // the stored value of voxel idx of a one-component brick set: the functor chain's
+    // result (non-persistent sources) or the first component
+    __device__ __forceinline__ float source_value(const SourceBrickParams& p, size_t idx)
+    {
+        const float* sp = p.src + idx * p.fdim;
+        if(!p.applyChain)
+            return __ldg(sp);
+        float v[4];
+        v[0] = __ldg(sp);
+        v[1] = p.fdim > 1 ? __ldg(sp + 1) : 0.0f;
+        v[2] = p.fdim > 2 ? __ldg(sp + 2) : 0.0f;
+        v[3] = p.fdim > 3 ? __ldg(sp + 3) : 0.0f;
+        return apply_chain(v, p.fdim, p.chain);
+    }
+
+    // two values as one 32-bit word of BF16 (DT 1) or FP16 (DT 2), the first in the low
+    // half, each rounded to nearest even as __float2bfloat16_rn / __float2half_rn do
+    template<int DT>
+    __device__ __forceinline__ void pack_pair(float a, float b, uint32_t& out)
+    {
+        if(DT == 1)
+        {
+            const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+            out = *reinterpret_cast<const uint32_t*>(&h);
+        }
+        else
+        {
+            const __half2 h = __floats2half2_rn(a, b);
+            out = *reinterpret_cast<const uint32_t*>(&h);
+        }
+    }
+
+    // one quad slot of 4 elements as one store: 16 bytes (FP32) or 8 bytes (BF16 / FP16,
+    // rounded to nearest even as __float2bfloat16_rn / __float2half_rn do)
+    template<int DT>
+    __device__ __forceinline__ void store_quad(void* out, size_t slot, float a, float b, float c, float d)
+    {
+        if(DT == 0)
+            reinterpret_cast<float4*>(out)[slot] = make_float4(a, b, c, d);
+        else if(DT == 1)
+        {
+            const __nv_bfloat162 lo = __floats2bfloat162_rn(a, b), hi = __floats2bfloat162_rn(c, d);
+            reinterpret_cast<uint2*>(out)[slot]
+                = make_uint2(*reinterpret_cast<const uint32_t*>(&lo), *reinterpret_cast<const uint32_t*>(&hi));
+        }
+        else
+        {
+            const __half2 lo = __floats2half2_rn(a, b), hi = __floats2half2_rn(c, d);
+            reinterpret_cast<uint2*>(out)[slot]
+                = make_uint2(*reinterpret_cast<const uint32_t*>(&lo), *reinterpret_cast<const uint32_t*>(&hi));
+        }
+    }
+
+    // One-component bricks as k_merge_pack builds the combined ones: one CTA per row of 4
+    // bricks along x, texel rows staged one per warp with the lanes along x, then every
+    // slot of the 4 bricks as one vector store, contiguous in memory.
+    template<int DT>
+    __global__ void __launch_bounds__(256) k_source_bricks_row(const __grid_constant__ SourceBrickParams p)
+    {
+        __shared__ float valS[kPackWords];
+        const Geom& g = p.g;
+        const int bx0 = blockIdx.x * kPackRow, by = blockIdx.y, bz = blockIdx.z;
+        const int nRow = min(kPackRow, g.nb[0] - bx0);
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int x0 = iclamp(bx0 * 8 - 1 + lane, 0, g.ls[0] - 1);
+        const int x32 = iclamp(bx0 * 8 + 31, 0, g.ls[0] - 1);
+        // all of the warp's row loads are issued before any is used (lane 0 also reads
+        // the row's 33rd texel, lx = 32)
+        float v[kRowsPerWarp], v2[kRowsPerWarp];
+#pragma unroll
+        for(int i = 0; i < kRowsPerWarp; ++i)
+        {
+            const int r = warp + 8 * i;
+            if(r < kPackRows)
+            {
+                const size_t row = pack_row(g, by, bz, r);
+                v[i] = source_value(p, row + x0);
+                if(lane == 0)
+                    v2[i] = source_value(p, row + x32);
+            }
+        }
+#pragma unroll
+        for(int i = 0; i < kRowsPerWarp; ++i)
+        {
+            const int r = warp + 8 * i;
+            if(r < kPackRows)
+            {
+                valS[r * kPackPitch + lane] = v[i];
+                if(lane == 0)
+                    valS[r * kPackPitch + 32] = v2[i];
+            }
+        }
+        __syncthreads();
+        const size_t brick0 = (size_t(bz) * g.nb[1] + by) * g.nb[0] + bx0;
+        if(DT == 0)
+        {
+            // one 16-byte slot per thread
+            const int lxy = threadIdx.x & 63;
+            const int base = (lxy >> 3) * kPackPitch + (lxy & 7);
+            for(int layer = threadIdx.x >> 6; layer < nRow * kApron; layer += 4)
+            {
+                const int j = layer / kApron, lz = layer - j * kApron;
+                const int t = lz * (kApron * kPackPitch) + base + 8 * j;
+                store_quad<0>(p.out, brick0 * kSlotsPerBrick + size_t(layer) * 64 + lxy, valS[t], valS[t + 1],
+                              valS[t + kPackPitch], valS[t + kPackPitch + 1]);
+            }
+        }
+        else
+        {
+            // 8-byte slots: two x-adjacent slots per thread, one 16-byte store
+            const int pair = threadIdx.x & 31; // lx = 2 * (pair & 3), ly = pair >> 2
+            const int lxy = (pair >> 2) * 8 + 2 * (pair & 3);
+            const int base = (pair >> 2) * kPackPitch + 2 * (pair & 3);
+            for(int layer = threadIdx.x >> 5; layer < nRow * kApron; layer += 8)
+            {
+                const int j = layer / kApron, lz = layer - j * kApron;
+                const int t = lz * (kApron * kPackPitch) + base + 8 * j;
+                const float a0 = valS[t], a1 = valS[t + 1], a2 = valS[t + 2];
+                const float b0 = valS[t + kPackPitch], b1 = valS[t + kPackPitch + 1], b2 = valS[t + kPackPitch + 2];
+                uint32_t w[4];
+                pack_pair<DT>(a0, a1, w[0]);
+                pack_pair<DT>(b0, b1, w[1]);
+                pack_pair<DT>(a1, a2, w[2]);
+                pack_pair<DT>(b1, b2, w[3]);
+                const size_t slot = brick0 * kSlotsPerBrick + size_t(layer) * 64 + lxy; // even
+                reinterpret_cast<uint4*>(p.out)[slot >> 1] = make_uint4(w[0], w[1], w[2], w[3]);
+            }
+        }
+    }
+
     void launch_source_bricks(const SourceBrickParams& p, cudaStream_t s)
     {
+        if(p.ncomp == 1)
+        {
+            const dim3 grid((p.g.nb[0] + kPackRow - 1) / kPackRow, p.g.nb[1], p.g.nb[2]);
+            if(p.dtype == 1)
+                k_source_bricks_row<1><<<grid, 256, 0, s>>>(p);
+            else if(p.dtype == 2)
+                k_source_bricks_row<2><<<grid, 256, 0, s>>>(p);
+            else
+                k_source_bricks_row<0><<<grid, 256, 0, s>>>(p);
+            return;
+        }
         dim3 grid(p.g.nb[0], p.g.nb[1], p.g.nb[2]);
         if(p.dtype == 1)
             k_source_bricks<1><<<grid, 256, 0, s>>>(p);
