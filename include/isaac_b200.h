@@ -393,6 +393,29 @@ isaacb_status isaacb_set_advection(
 isaacb_status isaacb_get_advection(isaacb_ctx* ctx, void* stream, uint32_t source, uint8_t* host);
 isaacb_status isaacb_get_noise(isaacb_ctx* ctx, void* stream, float* host);
 
+/* ---- Advection borders between ranks (the reference's guard exchange,
+ * lib/isaac.hpp:1856-1913, and its advection textures' guard band,
+ * lib/isaac.hpp:206-214).  Each field source's advection texture carries a guard
+ * band of ceil((ISAAC_MAX_ADVECTION_STEP_SIZE + 1) / scale) voxels per axis
+ * (isaacb_advection_guard); the advection step samples it, so a neighbour's
+ * border values reach across the boundary.  A multi-rank caller runs, per frame:
+ * isaacb_advect; per field source and per neighbour direction, isaacb_pack_guard
+ * into a device buffer, the exchange with that neighbour, isaacb_unpack_guard
+ * from the received buffer; then isaacb_update, which merges without advecting
+ * again.  Directions are the reference's neighbour indices 1-26 (base-3 digits
+ * x, y, z; digit 2 = -1; lib/isaac/isaac_types.hpp:133-161); a slab is
+ * (|d| ? guard : local) voxels per axis, x fastest.  Pack and unpack follow the
+ * reference's SyncToOwnGuard / SyncFromNeighbourGuard index arithmetic
+ * (lib/isaac/isaac_common_kernel.hpp:454-498), including its placement of the
+ * positive-side slabs one voxel lower.  Asynchronous on `stream`. */
+isaacb_status isaacb_advect(isaacb_ctx* ctx, void* stream);
+isaacb_status isaacb_advection_guard(const isaacb_ctx* ctx, uint32_t guard[3]);
+isaacb_status isaacb_pack_guard(isaacb_ctx* ctx, uint32_t src, uint32_t direction, uint8_t* slab, void* stream);
+isaacb_status isaacb_unpack_guard(isaacb_ctx* ctx, uint32_t src, uint32_t direction, const uint8_t* slab, void* stream);
+/* the "advection border" key switched off: both advection textures of every field
+ * source are cleared (lib/isaac.hpp:1668-1683) */
+isaacb_status isaacb_clear_advection(isaacb_ctx* ctx, void* stream);
+
 /* ---- Stereo compositing (lib/isaac/isaac_compositors.hpp:37-116, done on the GPU).
  * mode 0: out = left (width x height); mode 1: left and right side by side
  * (2*width x height); mode 2: per pixel (left & left_filter) | (right & right_filter)

@@ -189,6 +189,11 @@ SIGNATURES = {
     "isaacb_set_advection": (_i32, [_P, _f, _f, _i32, _i32, _i32]),
     "isaacb_get_advection": (_i32, [_P, _P, _u32, _P]),
     "isaacb_get_noise": (_i32, [_P, _P, _fp]),
+    "isaacb_advect": (_i32, [_P, _P]),
+    "isaacb_advection_guard": (_i32, [_P, _u32p]),
+    "isaacb_pack_guard": (_i32, [_P, _u32, _u32, _P, _P]),
+    "isaacb_unpack_guard": (_i32, [_P, _u32, _u32, _P, _P]),
+    "isaacb_clear_advection": (_i32, [_P, _P]),
     "isaacb_encoder_create": (_i32, [C.POINTER(_P)]),
     "isaacb_encoder_destroy": (_i32, [_P]),
     "isaacb_encoder_set_quality": (_i32, [_P, _u32]),

@@ -303,8 +303,10 @@ struct isaacb_ctx
     long long lastEmpty = -1;
     // field-source advection (defaults of lib/isaac.hpp:606-643); the textures start at zero
     bool field[kMaxSources]{};
-    uint8_t* adv[kMaxSources]{};
+    uint8_t* adv[kMaxSources]{}; // guarded: (local + 2 * advG) per axis
     uint8_t* advBack[kMaxSources]{};
+    int advG[3] = {0, 0, 0}; // guard band: ceil((ISAAC_MAX_ADVECTION_STEP_SIZE + 1) / scale) per axis
+    bool advectedThisFrame = false; // isaacb_advect ran; the next update merges without advecting
     float* noise = nullptr;
     float* noiseTmp = nullptr;
     bool noiseDirty = true;
@@ -461,6 +463,15 @@ namespace
         return size_t(c->desc.local_size[0]) * c->desc.local_size[1] * c->desc.local_size[2];
     }
 
+    // bytes of one guarded advection texture
+    size_t adv_count(const isaacb_ctx* c)
+    {
+        size_t n = 1;
+        for(int a = 0; a < 3; ++a)
+            n *= size_t(c->desc.local_size[a]) + 2 * size_t(c->advG[a]);
+        return n;
+    }
+
     // Per update with field sources (lib/isaac.hpp:1819-1850): the noise texture when its
     // seed count changed, the swap of every field source's front and back advection
     // texture, the step counter, and the advection of each enabled field source.
@@ -496,10 +507,11 @@ namespace
                 continue;
             if(!c->adv[s])
             {
-                ISAACB_CUDA(c, cudaMalloc(&c->adv[s], n), "advection texture");
-                ISAACB_CUDA(c, cudaMalloc(&c->advBack[s], n), "advection texture");
-                ISAACB_CUDA(c, cudaMemsetAsync(c->adv[s], 0, n, st), "advection texture");
-                ISAACB_CUDA(c, cudaMemsetAsync(c->advBack[s], 0, n, st), "advection texture");
+                const size_t na = adv_count(c);
+                ISAACB_CUDA(c, cudaMalloc(&c->adv[s], na), "advection texture");
+                ISAACB_CUDA(c, cudaMalloc(&c->advBack[s], na), "advection texture");
+                ISAACB_CUDA(c, cudaMemsetAsync(c->adv[s], 0, na, st), "advection texture");
+                ISAACB_CUDA(c, cudaMemsetAsync(c->advBack[s], 0, na, st), "advection texture");
             }
             std::swap(c->adv[s], c->advBack[s]);
         }
@@ -516,6 +528,8 @@ namespace
             ap.LX = np.LX;
             ap.LY = np.LY;
             ap.LZ = np.LZ;
+            for(int a = 0; a < 3; ++a)
+                ap.G[a] = c->advG[a];
             for(int i = 0; i < 3; ++i)
                 ap.scale[i] = np.scale[i];
             ap.stepSize = c->advStepFactor * 3.0f; // ISAAC_MAX_ADVECTION_STEP_SIZE (isaac_defines.hpp:21)
@@ -524,6 +538,37 @@ namespace
             launch_advect(ap, st);
         }
         ISAACB_CUDA(c, cudaGetLastError(), "advection");
+        return ISAACB_OK;
+    }
+
+    // one guard slab of field source s between its current advection texture and a
+    // device buffer: pack (SyncToOwnGuard) or unpack (SyncFromNeighbourGuard)
+    isaacb_status guard_slab(isaacb_ctx* c, uint32_t s, uint32_t direction, uint8_t* slab, bool pack, cudaStream_t stream)
+    {
+        if(!c || !slab || s >= uint32_t(c->nVol) || direction < 1 || direction > 26)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_pack_guard / isaacb_unpack_guard: bad arguments (direction 1-26)");
+        if(!c->field[s] || !c->adv[s])
+            return fail(c, ISAACB_NOT_READY, "guard slab: source " + std::to_string(s) + " has no advection texture yet");
+        GuardParams g{};
+        g.tex = c->adv[s];
+        g.slab = slab;
+        uint32_t idx = direction;
+        for(int a = 0; a < 3; ++a)
+        {
+            const int m = int(idx % 3);
+            idx /= 3;
+            g.d[a] = m == 2 ? -1 : m;
+            g.L[a] = int(c->desc.local_size[a]);
+            g.G[a] = c->advG[a];
+            g.e[a] = g.d[a] != 0 ? g.G[a] : g.L[a];
+            if(g.d[a] != 0 && g.L[a] < g.G[a] + 1)
+                return fail(c, ISAACB_INVALID_ARG, "guard slab: local size smaller than the guard band + 1");
+        }
+        if(pack)
+            launch_pack_guard(g, stream);
+        else
+            launch_unpack_guard(g, stream);
+        ISAACB_CUDA(c, cudaGetLastError(), "guard slab");
         return ISAACB_OK;
     }
 
@@ -580,6 +625,8 @@ namespace
         p.emptyBricks = c->emptyDev;
         for(int s = 0; s < c->nVol; ++s)
             p.adv[s] = c->field[s] ? c->adv[s] : nullptr;
+        for(int a = 0; a < 3; ++a)
+            p.advG[a] = c->advG[a];
     }
 } // namespace
 
@@ -630,6 +677,8 @@ extern "C"
         }
         isaacb_ctx* c = new isaacb_ctx;
         c->desc = *d;
+        for(int a = 0; a < 3; ++a)
+            c->advG[a] = int(std::ceil(float(3 + 1) / d->scale[a])); // isaac.hpp:206-214
         c->nVol = int(d->n_volume_sources);
         c->nPart = int(d->n_particle_sources);
         c->nTotal = int(nTotal);
@@ -943,8 +992,66 @@ extern "C"
             std::memset(host, 0, n);
             return ISAACB_OK;
         }
-        ISAACB_CUDA(c, cudaMemcpyAsync(host, c->adv[s], n, cudaMemcpyDeviceToHost, st), "advection readback");
+        // the interior of the guarded texture
+        const size_t LX = c->desc.local_size[0], LY = c->desc.local_size[1], LZ = c->desc.local_size[2];
+        const size_t SX = LX + 2 * c->advG[0], SY = LY + 2 * c->advG[1];
+        cudaMemcpy3DParms m{};
+        m.srcPtr = make_cudaPitchedPtr(c->adv[s], SX, SX, SY);
+        m.srcPos = make_cudaPos(size_t(c->advG[0]), size_t(c->advG[1]), size_t(c->advG[2]));
+        m.dstPtr = make_cudaPitchedPtr(host, LX, LX, LY);
+        m.extent = make_cudaExtent(LX, LY, LZ);
+        m.kind = cudaMemcpyDeviceToHost;
+        ISAACB_CUDA(c, cudaMemcpy3DAsync(&m, st), "advection readback");
         ISAACB_CUDA(c, cudaStreamSynchronize(st), "advection readback");
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_advect(isaacb_ctx* c, void* stream)
+    {
+        if(!c)
+            return ISAACB_INVALID_ARG;
+        for(int s = 0; s < c->nVol; ++s)
+            if(c->field[s] && !c->src[s] && (c->weight[s] != 0.0f || c->iso[s] != 0.0f))
+                return fail(c, ISAACB_NOT_READY, "isaacb_advect: field source " + std::to_string(s) + " has no memory");
+        const isaacb_status r = advect_fields(c, (cudaStream_t) stream);
+        if(r != ISAACB_OK)
+            return r;
+        ISAACB_CUDA(c, cudaGetLastError(), "isaacb_advect");
+        c->advectedThisFrame = true;
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_advection_guard(const isaacb_ctx* c, uint32_t guard[3])
+    {
+        if(!c || !guard)
+            return ISAACB_INVALID_ARG;
+        for(int a = 0; a < 3; ++a)
+            guard[a] = uint32_t(c->advG[a]);
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_pack_guard(isaacb_ctx* c, uint32_t s, uint32_t direction, uint8_t* slab, void* stream)
+    {
+        return guard_slab(c, s, direction, slab, true, (cudaStream_t) stream);
+    }
+
+    isaacb_status isaacb_unpack_guard(isaacb_ctx* c, uint32_t s, uint32_t direction, const uint8_t* slab, void* stream)
+    {
+        return guard_slab(c, s, direction, const_cast<uint8_t*>(slab), false, (cudaStream_t) stream);
+    }
+
+    isaacb_status isaacb_clear_advection(isaacb_ctx* c, void* stream)
+    {
+        if(!c)
+            return ISAACB_INVALID_ARG;
+        const size_t na = adv_count(c);
+        for(int s = 0; s < c->nVol; ++s)
+        {
+            if(c->adv[s])
+                ISAACB_CUDA(c, cudaMemsetAsync(c->adv[s], 0, na, (cudaStream_t) stream), "clear advection");
+            if(c->advBack[s])
+                ISAACB_CUDA(c, cudaMemsetAsync(c->advBack[s], 0, na, (cudaStream_t) stream), "clear advection");
+        }
         return ISAACB_OK;
     }
     isaacb_status isaacb_get_noise(isaacb_ctx* c, void* stream, float* host)
@@ -1056,9 +1163,13 @@ extern "C"
         c->updateLaunches = 0;
         if(c->renderer == ISAACB_RENDERER_COMBINED)
         {
-            r = advect_fields(c, st);
-            if(r != ISAACB_OK)
-                return r;
+            if(!c->advectedThisFrame)
+            {
+                r = advect_fields(c, st);
+                if(r != ISAACB_OK)
+                    return r;
+            }
+            c->advectedThisFrame = false;
             MergeParams p{};
             prepare_merge(c, p);
             ISAACB_CUDA(c, cudaMemsetAsync(c->emptyDev, 0, sizeof(unsigned int), st), "empty brick counter");

@@ -30,7 +30,8 @@ namespace isaacb
         float totalWeight;
         float invTotalWeight; // 2^-k when totalWeight == 2^k exactly, else 0
         int32_t nonNegative; // every colour sum is finite and >= 0 (tables and weights >= 0, total > 0)
-        const uint8_t* adv[kMaxSources]; // field sources: advection texture (localSize, x fastest), else null
+        const uint8_t* adv[kMaxSources]; // field sources: advection texture (guarded, x fastest), else null
+        int32_t advG[3]; // the advection textures' guard band per axis
         uint32_t* volLin; // combined volume RGBA8, linear (merge scratch between the two passes)
         uint4* volQ; // combined volume, quad bricks
         uint32_t* isoAQ; // combined iso alpha, quad bricks
@@ -81,12 +82,25 @@ namespace isaacb
         uint8_t* out;
         const float* noise;
         int LX, LY, LZ;
+        int G[3]; // guard band of the advection textures, (L + 2G) per axis, x fastest
         float scale[3];
         float stepSize; // step factor * ISAAC_MAX_ADVECTION_STEP_SIZE
         float historyWeight;
         int seedNoise; // 1: this step adds the noise (timeStep % period < seeding time)
     };
     void launch_advect(const AdvectParams& p, cudaStream_t s);
+
+    // one guard slab of an advection texture (the reference's SyncToOwnGuard /
+    // SyncFromNeighbourGuard): direction d, slab extent e (G across d, L along it)
+    struct GuardParams
+    {
+        uint8_t* tex; // guarded advection texture
+        uint8_t* slab; // e[0] * e[1] * e[2] bytes, x fastest
+        int L[3], G[3];
+        int d[3], e[3];
+    };
+    void launch_pack_guard(const GuardParams& p, cudaStream_t s);
+    void launch_unpack_guard(const GuardParams& p, cudaStream_t s);
 
     // per-source renderer bricks: persistent sources keep their raw components,
     // non-persistent sources their functor-chain value (UpdatePersistendTextureKernel)

@@ -382,7 +382,9 @@ namespace isaacb
             {
                 // field source: alpha blended with the advection texture
                 // (MergeAdvectionToCombinedTextureIterator, isaac_common_kernel.hpp:664-665)
-                c.w *= float(__ldg(p.adv[s] + i)) / 255.0f;
+                const size_t ai = (size_t(z + p.advG[2]) * (g.ls[1] + 2 * p.advG[1]) + (y + p.advG[1])) * (g.ls[0] + 2 * p.advG[0])
+                    + (x + p.advG[0]);
+                c.w *= float(__ldg(p.adv[s] + ai)) / 255.0f;
             }
             merge_accumulate(c, vw, it, ISO, vc, ic);
         }
@@ -730,11 +732,16 @@ namespace isaacb
     __global__ void k_advect(const __grid_constant__ AdvectParams p)
     {
         const size_t n = size_t(p.LX) * p.LY * p.LZ;
+        const int SX = p.LX + 2 * p.G[0], SY = p.LY + 2 * p.G[1];
+        auto at = [&](int x, int y, int z) {
+            return (size_t(z + p.G[2]) * SY + (y + p.G[1])) * SX + (x + p.G[0]);
+        };
         auto fetch = [&](int x, int y, int z) {
-            // VALUE border 0 (the guard cells are zero too)
-            if(x < 0 || y < 0 || z < 0 || x >= p.LX || y >= p.LY || z >= p.LZ)
+            // VALUE border 0 outside the guard band (Sampler::safeMemoryAccess,
+            // isaac_texture.hpp:201-206); the band holds zeros or a neighbour's slabs
+            if(x < -p.G[0] || y < -p.G[1] || z < -p.G[2] || x >= p.LX + p.G[0] || y >= p.LY + p.G[1] || z >= p.LZ + p.G[2])
                 return 0.0f;
-            return float(__ldg(p.back + (size_t(z) * p.LY + y) * p.LX + x));
+            return float(__ldg(p.back + at(x, y, z)));
         };
         for(size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
         {
@@ -763,7 +770,7 @@ namespace isaacb
             float fl;
             int fi;
             floor_split(sv, fl, fi);
-            p.out[i] = uint8_t(min(max(ti + ((sv - fl) > d ? 1 : 0), 0), 255));
+            p.out[at(x, y, z)] = uint8_t(min(max(ti + ((sv - fl) > d ? 1 : 0), 0), 255));
         }
     }
 
@@ -771,6 +778,44 @@ namespace isaacb
     {
         const size_t n = size_t(p.LX) * p.LY * p.LZ;
         k_advect<<<int(std::min<size_t>((n + 255) / 256, 148 * 16)), 256, 0, s>>>(p);
+    }
+
+    // guard slab voxel c <-> texture voxel, per axis (the reference's index arithmetic,
+    // including where it places the positive-side slabs):
+    //   pack (SyncToOwnGuard, isaac_common_kernel.hpp:454-474):
+    //     source = max(d, 0) * (L - e - 1) + c
+    //   unpack (SyncFromNeighbourGuard, :477-498):
+    //     target = max(d, 0) * (L - 1) + min(d, 0) * e + c
+    template<bool PACK>
+    __global__ void k_guard(const __grid_constant__ GuardParams p)
+    {
+        const size_t n = size_t(p.e[0]) * p.e[1] * p.e[2];
+        const int SX = p.L[0] + 2 * p.G[0], SY = p.L[1] + 2 * p.G[1];
+        for(size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        {
+            const int c[3] = {int(i % p.e[0]), int((i / p.e[0]) % p.e[1]), int(i / (size_t(p.e[0]) * p.e[1]))};
+            int t[3];
+#pragma unroll
+            for(int a = 0; a < 3; ++a)
+                t[a] = PACK ? (p.d[a] > 0 ? p.L[a] - p.e[a] - 1 : 0) + c[a]
+                            : (p.d[a] > 0 ? p.L[a] - 1 : 0) + (p.d[a] < 0 ? -p.e[a] : 0) + c[a];
+            const size_t ti = (size_t(t[2] + p.G[2]) * SY + (t[1] + p.G[1])) * SX + (t[0] + p.G[0]);
+            if(PACK)
+                p.slab[i] = p.tex[ti];
+            else
+                p.tex[ti] = p.slab[i];
+        }
+    }
+
+    void launch_pack_guard(const GuardParams& p, cudaStream_t s)
+    {
+        const size_t n = size_t(p.e[0]) * p.e[1] * p.e[2];
+        k_guard<true><<<int(std::min<size_t>((n + 255) / 256, 148 * 8)), 256, 0, s>>>(p);
+    }
+    void launch_unpack_guard(const GuardParams& p, cudaStream_t s)
+    {
+        const size_t n = size_t(p.e[0]) * p.e[1] * p.e[2];
+        k_guard<false><<<int(std::min<size_t>((n + 255) / 256, 148 * 8)), 256, 0, s>>>(p);
     }
 
     // ---------------------------------------------------------------- per-source bricks

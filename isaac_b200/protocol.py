@@ -623,7 +623,7 @@ class Session:
             ("advection seeding period", int(adv["period"])),
             ("advection seeding duration", int(adv["duration"])),
             ("advection on pause", bool(getattr(viz, "advectionOnPause", False))),
-            ("advection border", False),
+            ("advection border", bool(getattr(viz, "advectionBorder", True))),
         ):
             if flag in f:
                 root[flag] = val

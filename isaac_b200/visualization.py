@@ -121,6 +121,7 @@ class IsaacVisualization:
         self.lib = _lib.load()
         self.name = name
         self.globalSize = tuple(int(v) for v in global_size)
+        self.localSize = tuple(int(v) for v in local_size)
         self.framebufferSize = tuple(int(v) for v in framebuffer_size)
         self.volumeSources = list(volume_sources)
         self.particleSources = list(particle_sources)
@@ -184,6 +185,12 @@ class IsaacVisualization:
         self.session = None
         self.metadata = None
         self._frame_dev = None
+        # advection borders between ranks (updateNeighbours; "advection border" defaults on)
+        self.fieldSources: set[int] = set()
+        self.neighbourNodeIds = [-1] * 27
+        self.advectionBorder = True
+        self.borderGroup = None
+        self._borders = None
         if server_url is not None:
             self.setServer(server_url, server_port, jpeg)
 
@@ -317,6 +324,10 @@ class IsaacVisualization:
         """Make volume source ``src`` (a float3 vector field, after every plain volume
         source) an advected field source (the reference's FieldSourceList)."""
         check(self.lib.isaacb_set_field_source(self.ctx, int(src), int(enabled)), self.ctx)
+        if enabled:
+            self.fieldSources.add(int(src))
+        else:
+            self.fieldSources.discard(int(src))
 
     def setAdvection(self, step_factor=1.0, history_weight=0.95, seeding_period=1, seeding_duration=1, seed_points=1000):
         """The "advection step", "advection weight", "advection seeding period",
@@ -325,6 +336,50 @@ class IsaacVisualization:
                               duration=seeding_duration, seeds=seed_points)
         check(self.lib.isaacb_set_advection(self.ctx, float(step_factor), float(history_weight), int(seeding_period),
                                              int(seeding_duration), int(seed_points)), self.ctx)
+
+    # ------------------------------------------------------------------ advection borders between ranks
+    def updateNeighbours(self, neighbours):
+        """The ranks of the 26 neighbouring sub-volumes (index = the reference's direction
+        index, -1 for none; lib/isaac.hpp:1049-1053).  With a process group (``group``,
+        or the default one) the advection borders are exchanged with them every frame."""
+        self.neighbourNodeIds = [int(v) for v in neighbours]
+
+    def setAdvectionBorder(self, enabled: bool):
+        """The "advection border" key: off clears the advection textures and stops the exchange."""
+        self.advectionBorder = bool(enabled)
+        if not enabled:
+            check(self.lib.isaacb_clear_advection(self.ctx, self._stream()), self.ctx)
+
+    def advectionGuard(self) -> tuple:
+        g = (C.c_uint32 * 3)()
+        check(self.lib.isaacb_advection_guard(self.ctx, g), self.ctx)
+        return tuple(int(v) for v in g)
+
+    def advect(self):
+        """The advection step alone; the next update merges without advecting again."""
+        check(self.lib.isaacb_advect(self.ctx, self._stream()), self.ctx)
+
+    def packGuard(self, src: int, direction: int, out):
+        check(self.lib.isaacb_pack_guard(self.ctx, int(src), int(direction), C.c_void_p(out.data_ptr()), self._stream()),
+              self.ctx)
+
+    def unpackGuard(self, src: int, direction: int, data):
+        check(self.lib.isaacb_unpack_guard(self.ctx, int(src), int(direction), C.c_void_p(data.data_ptr()),
+                                           self._stream()), self.ctx)
+
+    def _exchange_borders(self):
+        """Advect and swap guard slabs with the neighbour ranks (lib/isaac.hpp:1856-1913)."""
+        if not any(n >= 0 for n in self.neighbourNodeIds[1:]) or not self.advectionBorder or not self.fieldSources:
+            return
+        if self._borders is None:
+            from .borders import AdvectionBorders
+
+            self._borders = AdvectionBorders.for_visualization(self, self.neighbourNodeIds, self.borderGroup)
+        self._borders.neighbours = list(self.neighbourNodeIds)
+        self.advect()
+        for s in sorted(self.fieldSources):
+            if self.sourceWeight[s] != 0 or self.sourceIsoThreshold[s] != 0:
+                self._borders.exchange(s)
 
     def advectionTexture(self, src: int) -> np.ndarray:
         lx, ly, lz = (int(v) for v in self.desc.local_size)
@@ -433,6 +488,8 @@ class IsaacVisualization:
             if "seed points" in message:
                 a["seeds"] = max(int(a["seeds"]), 0)
             self.setAdvection(a["step"], a["weight"], a["period"], a["duration"], a["seeds"])
+        if "advection border" in message:
+            self.setAdvectionBorder(bool(message["advection border"]))
         if "clipping edit" in message:
             c = message["clipping edit"]
             self.editClipping(int(c["nr"]), *c["position"], *c["normal"])
@@ -478,6 +535,7 @@ class IsaacVisualization:
             return self._frame
         w, h = self.framebufferSize
         st = self._stream()
+        self._exchange_borders()
         if len(self.projections) > 1 or not isinstance(self.compositor, DefaultCompositor):
             return self._multi_pass(host, st)
         if host and not timing and not device_frame:
@@ -527,7 +585,9 @@ class IsaacVisualization:
         return result
 
     def update(self):
-        """Buffer update only (merge / per-source bricks), asynchronous."""
+        """Buffer update only (merge / per-source bricks), asynchronous; with neighbour
+        ranks the advection borders are exchanged first."""
+        self._exchange_borders()
         check(self.lib.isaacb_update(self.ctx, self._stream()), self.ctx)
 
     def render(self, out=None):

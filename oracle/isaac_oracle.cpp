@@ -761,7 +761,11 @@ namespace orc
         // isaac.hpp:606-643.  The reference leaves the advection textures and their guard
         // cells uninitialised; here they start at zero.
         bool field[MAX_SOURCES] = {};
-        std::vector<uint8_t> adv[MAX_SOURCES], advBack[MAX_SOURCES]; // localSize, x fastest
+        // advection textures with the guard band of SyncedTexture3DAllocator
+        // (isaac.hpp:206-214): ceil((ISAAC_MAX_ADVECTION_STEP_SIZE + 1) / scale) per axis,
+        // x fastest over (localSize + 2 * advGuard)
+        std::vector<uint8_t> adv[MAX_SOURCES], advBack[MAX_SOURCES];
+        bool advectedThisFrame = false; // advectFrame() ran; the next update() skips it
         std::vector<T> noise; // localSize
         float advStepFactor = 1.0f, advHistoryWeight = 0.95f;
         int advSeedPeriod = 1, advSeedTime = 1, seedPoints = 1000;
@@ -860,11 +864,95 @@ namespace orc
                 noiseDirty = true;
             seedPoints = seeds;
         }
+        int64_t advGuard(int a) const
+        {
+            return int64_t(std::ceil(float(3 + 1) / scale[a]));
+        }
+        int64_t advSize(int a) const
+        {
+            return localSize[a] + 2 * advGuard(a);
+        }
+        size_t advCount() const
+        {
+            return size_t(advSize(0) * advSize(1) * advSize(2));
+        }
+        // index of (x, y, z), each in [-guard, local + guard), in a guarded advection texture
+        size_t advIndex(int64_t x, int64_t y, int64_t z) const
+        {
+            return size_t((x + advGuard(0)) + advSize(0) * ((y + advGuard(1)) + advSize(1) * (z + advGuard(2))));
+        }
         void getAdvection(int s, uint8_t* out) const
         {
-            const size_t n = size_t(localSize[0] * localSize[1] * localSize[2]);
-            for(size_t i = 0; i < n; ++i)
-                out[i] = adv[s].size() == n ? adv[s][i] : 0;
+            const int64_t LX = localSize[0], LY = localSize[1], LZ = localSize[2];
+            const bool have = adv[s].size() == advCount();
+            for(int64_t z = 0; z < LZ; ++z)
+                for(int64_t y = 0; y < LY; ++y)
+                    for(int64_t x = 0; x < LX; ++x)
+                        out[size_t(x + LX * (y + LY * z))] = have ? adv[s][advIndex(x, y, z)] : 0;
+        }
+
+        // direction of neighbour index i (indexToDirection, isaac_types.hpp:133-143)
+        static void guardDirection(int i, int d[3])
+        {
+            for(int a = 0; a < 3; ++a)
+            {
+                const int m = i % 3;
+                d[a] = m == 2 ? -1 : m;
+                i /= 3;
+            }
+        }
+        // extent of the guard slab of direction d: guard across it, the local size along it
+        void guardSlab(const int d[3], int64_t e[3]) const
+        {
+            for(int a = 0; a < 3; ++a)
+                e[a] = d[a] != 0 ? advGuard(a) : localSize[a];
+        }
+        // SyncToOwnGuard (isaac_common_kernel.hpp:454-474) on the current advection texture:
+        // slab voxel c comes from max(d, 0) * (local - slab - 1) + c per axis
+        void packGuard(int s, int i, uint8_t* out) const
+        {
+            int d[3];
+            int64_t e[3];
+            guardDirection(i, d);
+            guardSlab(d, e);
+            for(int64_t z = 0; z < e[2]; ++z)
+                for(int64_t y = 0; y < e[1]; ++y)
+                    for(int64_t x = 0; x < e[0]; ++x)
+                    {
+                        const int64_t c[3] = {x, y, z};
+                        int64_t src[3];
+                        for(int a = 0; a < 3; ++a)
+                            src[a] = (d[a] > 0 ? localSize[a] - e[a] - 1 : 0) + c[a];
+                        out[size_t(x + e[0] * (y + e[1] * z))] = adv[s][advIndex(src[0], src[1], src[2])];
+                    }
+        }
+        // SyncFromNeighbourGuard (isaac_common_kernel.hpp:477-498): slab voxel c goes to
+        // max(d, 0) * (local - 1) + min(d, 0) * slab + c per axis
+        void unpackGuard(int s, int i, const uint8_t* in)
+        {
+            int d[3];
+            int64_t e[3];
+            guardDirection(i, d);
+            guardSlab(d, e);
+            for(int64_t z = 0; z < e[2]; ++z)
+                for(int64_t y = 0; y < e[1]; ++y)
+                    for(int64_t x = 0; x < e[0]; ++x)
+                    {
+                        const int64_t c[3] = {x, y, z};
+                        int64_t dst[3];
+                        for(int a = 0; a < 3; ++a)
+                            dst[a] = (d[a] > 0 ? localSize[a] - 1 : 0) + (d[a] < 0 ? -e[a] : 0) + c[a];
+                        adv[s][advIndex(dst[0], dst[1], dst[2])] = in[size_t(x + e[0] * (y + e[1] * z))];
+                    }
+        }
+        // "advection border" switched off clears both advection textures (isaac.hpp:1668-1683)
+        void clearAdvection()
+        {
+            for(int s = 0; s < nVol; ++s)
+            {
+                std::fill(adv[s].begin(), adv[s].end(), uint8_t(0));
+                std::fill(advBack[s].begin(), advBack[s].end(), uint8_t(0));
+            }
         }
         void getNoise(float* out)
         {
@@ -1054,11 +1142,13 @@ namespace orc
             const int64_t LX = localSize[0], LY = localSize[1], LZ = localSize[2];
             const T stepSize = T(advStepFactor * float(3)); // ISAAC_MAX_ADVECTION_STEP_SIZE
             const std::vector<uint8_t>& back = advBack[s];
+            const int64_t gx = advGuard(0), gy = advGuard(1), gz = advGuard(2);
             auto fetch = [&](int64_t x, int64_t y, int64_t z) {
-                // VALUE border (0); the guard cells are zero as well
-                if(x < 0 || y < 0 || z < 0 || x >= LX || y >= LY || z >= LZ)
+                // VALUE border (0) outside the guard band (Sampler::safeMemoryAccess,
+                // isaac_texture.hpp:201-206); the band holds zeros or a neighbour's slabs
+                if(x < -gx || y < -gy || z < -gz || x >= LX + gx || y >= LY + gy || z >= LZ + gz)
                     return T(0);
-                return T(back[size_t(x + y * LX + z * LX * LY)]);
+                return T(back[advIndex(x, y, z)]);
             };
 #pragma omp parallel for schedule(static)
             for(int64_t z = 0; z < LZ; ++z)
@@ -1079,7 +1169,7 @@ namespace orc
                         V4<T> c{nv + history * T(advHistoryWeight) * (T(1) - nv), T(0), T(0), T(0)};
                         uint8_t out[4];
                         dither(5, x, y, z, c, out);
-                        adv[s][size_t(x + y * LX + z * LX * LY)] = out[0];
+                        adv[s][advIndex(x, y, z)] = out[0];
                     }
         }
 
@@ -1099,10 +1189,10 @@ namespace orc
             {
                 if(!field[s])
                     continue;
-                if(adv[s].size() != n)
+                if(adv[s].size() != advCount())
                 {
-                    adv[s].assign(n, 0);
-                    advBack[s].assign(n, 0);
+                    adv[s].assign(advCount(), 0);
+                    advBack[s].assign(advCount(), 0);
                 }
                 std::swap(adv[s], advBack[s]);
             }
@@ -1114,9 +1204,18 @@ namespace orc
 
         // ----- buffer update: UpdatePersistendTextureKernel (lib/isaac/isaac_common_kernel.hpp:432-451)
         // and MergeToCombinedTextureKernel (lib/isaac/isaac_common_kernel.hpp:690-759).
-        void update()
+        // the advection step alone, so that guard slabs can be exchanged before the merge
+        void advectFrame()
         {
             updateAdvection();
+            advectedThisFrame = true;
+        }
+
+        void update()
+        {
+            if(!advectedThisFrame)
+                updateAdvection();
+            advectedThisFrame = false;
             for(int s = 0; s < nVol; ++s)
             {
                 bool enabled = weight[s] != 0.0f || iso[s] != 0.0f;
@@ -1161,7 +1260,7 @@ namespace orc
                             // field sources: alpha blended with the advection texture
                             // (MergeAdvectionToCombinedTextureIterator, isaac_common_kernel.hpp:664-665)
                             if(field[s])
-                                color.w *= (T(adv[s][size_t(x + y * LX + z * LX * LY)]) / T(255));
+                                color.w *= (T(adv[s][advIndex(x, y, z)]) / T(255));
                             if(vw > T(0))
                             {
                                 V4<T> c = color;
@@ -2296,6 +2395,22 @@ extern "C"
     void or_get_advection(void* p, int s, uint8_t* out)
     {
         OR_DISPATCH((OrHandle*) p, c->getAdvection(s, out));
+    }
+    void or_advect(void* p)
+    {
+        OR_DISPATCH((OrHandle*) p, c->advectFrame());
+    }
+    void or_pack_guard(void* p, int s, int direction, uint8_t* out)
+    {
+        OR_DISPATCH((OrHandle*) p, c->packGuard(s, direction, out));
+    }
+    void or_unpack_guard(void* p, int s, int direction, const uint8_t* in)
+    {
+        OR_DISPATCH((OrHandle*) p, c->unpackGuard(s, direction, in));
+    }
+    void or_clear_advection(void* p)
+    {
+        OR_DISPATCH((OrHandle*) p, c->clearAdvection());
     }
     void or_get_noise(void* p, float* out)
     {

@@ -50,6 +50,10 @@ SIG = {
     "or_set_field": (None, [_P, C.c_int, C.c_int]),
     "or_set_advection": (None, [_P, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int]),
     "or_get_advection": (None, [_P, C.c_int, _u8p]),
+    "or_advect": (None, [_P]),
+    "or_pack_guard": (None, [_P, C.c_int, C.c_int, _u8p]),
+    "or_unpack_guard": (None, [_P, C.c_int, C.c_int, _u8p]),
+    "or_clear_advection": (None, [_P]),
     "or_get_noise": (None, [_P, _fp]),
     "or_update": (None, [_P]),
     "or_render": (None, [_P, _u8p, C.c_int, C.c_int]),
@@ -100,6 +104,21 @@ def _iarr(v):
     return (C.c_int * len(v))(*[int(x) for x in v])
 
 
+def direction_of(index: int) -> tuple:
+    """indexToDirection (lib/isaac/isaac_types.hpp:133-143): base-3 digits x, y, z, 2 -> -1."""
+    d = []
+    for _ in range(3):
+        m = index % 3
+        d.append(-1 if m == 2 else m)
+        index //= 3
+    return tuple(d)
+
+
+def mirrored(index: int) -> int:
+    """toMirroredIndex (lib/isaac/isaac_types.hpp:158-161)."""
+    return sum((2 if -v == -1 else -v) * 3**a for a, v in enumerate(direction_of(index)))
+
+
 class Oracle:
     """One oracle context; mirrors the product's setters (test infrastructure)."""
 
@@ -120,6 +139,7 @@ class Oracle:
         self.lib = load()
         self.W, self.H = (int(v) for v in framebuffer)
         self.local_size = tuple(int(v) for v in local_size)
+        self.scale = tuple(float(v) for v in scale)
         n = len(feature_dims)
         self.n = n
         self.n_volume = n_volume
@@ -240,6 +260,33 @@ class Oracle:
         out = np.zeros((lz, ly, lx), dtype=np.uint8)
         self.lib.or_get_advection(self.ctx, int(src), _ptr(out, _u8p))
         return out
+
+    # ----- advection guard slabs between ranks (SyncToOwnGuard / SyncFromNeighbourGuard)
+    def advect(self):
+        """The advection step alone; the next update() merges without advecting again."""
+        self.lib.or_advect(self.ctx)
+
+    def guard_slab(self, direction: int) -> tuple:
+        """(x, y, z) extent of the guard slab of neighbour index ``direction``."""
+        e = []
+        for a in range(3):
+            d = direction_of(direction)[a]
+            g = int(np.ceil(np.float32(4.0) / np.float32(self.scale[a])))
+            e.append(g if d != 0 else self.local_size[a])
+        return tuple(e)
+
+    def pack_guard(self, src: int, direction: int) -> np.ndarray:
+        out = np.zeros(int(np.prod(self.guard_slab(direction))), dtype=np.uint8)
+        self.lib.or_pack_guard(self.ctx, int(src), int(direction), _ptr(out, _u8p))
+        return out
+
+    def unpack_guard(self, src: int, direction: int, data: np.ndarray):
+        data = np.ascontiguousarray(data, dtype=np.uint8).reshape(-1)
+        assert data.size == int(np.prod(self.guard_slab(direction)))
+        self.lib.or_unpack_guard(self.ctx, int(src), int(direction), _ptr(data, _u8p))
+
+    def clear_advection(self):
+        self.lib.or_clear_advection(self.ctx)
 
     def noise(self) -> np.ndarray:
         lx, ly, lz = self.local_size

@@ -33,10 +33,29 @@ def _frames(s: Scene):
 # --------------------------------------------------------------------- merge
 @pytest.mark.parametrize("dither", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("iso", [False, True])
-def test_merge_textures_bit_exact(dither, iso):
-    s = gaussian_pair(n=29, dither_mode=dither)
+@pytest.mark.parametrize("n", [29, 28])
+def test_merge_textures_bit_exact(dither, iso, n):
+    """A scalar and a vector source (chain "length"), rows of odd and even length."""
+    s = gaussian_pair(n=n, dither_mode=dither)
     if iso:
         s.iso = [0.6, 0.3]
+    o = build_oracle(s)
+    o.update()
+    rv, ri = o.combined()
+    viz = build_gpu(s)
+    viz.update()
+    gv, gi = viz.combinedTextures()
+    assert np.array_equal(gv, rv)
+    assert np.array_equal(gi, ri)
+
+
+@pytest.mark.parametrize("chain", ["mul(2)|add(1)", "mul(-3)|add(0.5)", "sum", "pow(2)"])
+@pytest.mark.parametrize("n", [27, 28])
+def test_merge_functor_chains_bit_exact(chain, n):
+    """Functor chains on both sources (the general merge; a negative chain takes the
+    general dither), rows of odd and even length."""
+    s = gaussian_pair(n=n, iso=[0.5, 0.0])
+    s.functions = [chain, chain]
     o = build_oracle(s)
     o.update()
     rv, ri = o.combined()
