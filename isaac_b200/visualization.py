@@ -175,8 +175,10 @@ class IsaacVisualization:
         self.mergeTime = 0.0
         self.copyTime = 0.0
         self._frame = None
+        self._srcPtrs = [0] * len(self.volumeSources)
         for i, s in enumerate(self.volumeSources):
             check(self.lib.isaacb_set_source(ctx, i, C.c_void_p(s.data.data_ptr())), ctx)
+            self._srcPtrs[i] = s.data.data_ptr()
         for j, p in enumerate(self.particleSources):
             self._set_particles(n_vol + j, p)
         self._push_camera()
@@ -502,6 +504,15 @@ class IsaacVisualization:
             self.setDitherMode(int(message["dither mode"]["mode"]))
 
     # ------------------------------------------------------------------ per frame
+    def _sync_source_pointers(self):
+        """A source whose ``update`` hook replaced its ``data`` (another buffer of the
+        same shape, e.g. double-buffered inputs) is read from the new memory."""
+        for i, s in enumerate(self.volumeSources):
+            ptr = s.data.data_ptr()
+            if ptr != self._srcPtrs[i]:
+                check(self.lib.isaacb_set_source(self.ctx, i, C.c_void_p(ptr)), self.ctx)
+                self._srcPtrs[i] = ptr
+
     def _stream(self):
         return C.c_void_p(_torch().cuda.current_stream().cuda_stream)
 
@@ -531,6 +542,7 @@ class IsaacVisualization:
             s.update(self.sourceWeight[i] != 0 or self.sourceIsoThreshold[i] != 0, pointer)
         for j, p in enumerate(self.particleSources):
             p.update(self.sourceWeight[len(self.volumeSources) + j] != 0, pointer)
+        self._sync_source_pointers()
         if not redraw:
             return self._frame
         w, h = self.framebufferSize
@@ -587,6 +599,7 @@ class IsaacVisualization:
     def update(self):
         """Buffer update only (merge / per-source bricks), asynchronous; with neighbour
         ranks the advection borders are exchanged first."""
+        self._sync_source_pointers()
         self._exchange_borders()
         check(self.lib.isaacb_update(self.ctx, self._stream()), self.ctx)
 

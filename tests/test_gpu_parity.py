@@ -291,3 +291,18 @@ def test_repeat_frames_identical():
     a = viz.doVisualization()
     b = viz.doVisualization()
     assert np.array_equal(a, b)
+
+
+def test_source_buffer_swap_between_frames():
+    """A source whose data is replaced between frames (double-buffered inputs) is read
+    from the new memory: the frame equals a fresh context's over the new data."""
+    s1 = gaussian_pair(n=24, seed=1)
+    s2 = gaussian_pair(n=24, seed=2)
+    viz = build_gpu(s1)
+    first = viz.doVisualization()
+    for src, (v, _) in zip(viz.volumeSources, s2.volumes):
+        src.data = torch.from_numpy(np.ascontiguousarray(v)).cuda()
+    swapped = viz.doVisualization()
+    fresh = build_gpu(s2).doVisualization()
+    assert np.array_equal(swapped, fresh)
+    assert not np.array_equal(first, fresh)
