@@ -755,13 +755,18 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks):
     jr = recon.JudgedRenderer(pr.full, pr.low, net, judge_every=16, threshold=40.0)
     full = torch.empty((H, W, 4), dtype=torch.uint8, device="cuda")
 
-    # samples per full-size and half-size frame (untimed)
+    # samples per full-size and half-size frame, averaged over the orbit of the timed
+    # frames (untimed)
     pr.full.setCounting(True)
     pr.low.setCounting(True)
-    pr.full.render(full)
-    pr.low.render(jr.half)
-    full_samples = pr.full.counters()[0]
-    half_samples = pr.low.counters()[0]
+    full_samples = half_samples = 0
+    for P, MV in cams:
+        jr.setCamera(P, MV)
+        pr.full.render(full)
+        pr.low.render(jr.half)
+        full_samples += pr.full.counters()[0] / len(cams)
+        half_samples += pr.low.counters()[0] / len(cams)
+    full_samples, half_samples = int(full_samples), int(half_samples)
     pr.full.setCounting(False)
     pr.low.setCounting(False)
 
@@ -809,8 +814,10 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks):
     judged = [p for _, p in jr.judged[-(n_frames // 16):]]
 
     # phases of one learned frame (events on the launch stream)
+    # (over the same orbit of cameras as the timed frames: the samples per frame follow
+    # the view angle)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-    nt = 8
+    nt = n_frames
     half_ms = net_ms = 0.0
     for k in range(nt):
         pr.low.setCamera(*cams[k])

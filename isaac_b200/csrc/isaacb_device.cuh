@@ -393,6 +393,33 @@ namespace isaacb
         return brick * kSlotsPerBrick + size_t((az & 7) * 64 + (ay & 7) * 8 + (ax & 7));
     }
 
+    // Per-source bricks order their slots along a Morton curve: slot (lx, ly, lz) of a
+    // brick is the bit interleave of lx, ly, lz (bits x0 y0 z0 x1 y1 z1 x2 y2 z2) for the
+    // 8 layers of its own voxels, and 512 + ly * 8 + lx in the apron layer lz = 8.  The
+    // rays of a warp sample a small patch of voxels that faces the camera; in x-fastest
+    // order a patch facing the x axis spans 64- and 512-byte strides, in Morton order
+    // every 2x2x2 block is contiguous whatever the view direction.
+    __device__ __forceinline__ uint32_t spread3(int v)
+    {
+        // 3-bit v -> bits 0, 3, 6: byte v of the table 0x49 48 41 40 09 08 01 00
+        return __byte_perm(0x09080100u, 0x49484140u, uint32_t(v));
+    }
+    __device__ __forceinline__ uint32_t morton_slot(int lx, int ly, int lz)
+    {
+        return lz < 8 ? (spread3(lx) | (spread3(ly) << 1) | (spread3(lz) << 2)) : uint32_t(512 + ly * 8 + lx);
+    }
+    // the slot of the trilinear footprint based at (x0, y0, z0) in [-1, L-1] in the
+    // per-source bricks, and in `above` the slot of the layer z0 + 1
+    __device__ __forceinline__ size_t source_slot(const Geom& g, int x0, int y0, int z0, size_t& above)
+    {
+        const int ax = x0 + 1, ay = y0 + 1, az = z0 + 1;
+        const size_t base = ((size_t(az >> 3) * g.nb[1] + size_t(ay >> 3)) * g.nb[0] + size_t(ax >> 3)) * kSlotsPerBrick;
+        const int lx = ax & 7, ly = ay & 7, lz = az & 7;
+        const uint32_t xy = spread3(lx) | (spread3(ly) << 1);
+        above = base + (lz < 7 ? (xy | (spread3(lz + 1) << 2)) : uint32_t(512 + ly * 8 + lx));
+        return base + (xy | (spread3(lz) << 2));
+    }
+
     __device__ __forceinline__ float byte_f(uint32_t w, int c)
     {
         return float((w >> (8 * c)) & 0xffu);

@@ -54,8 +54,9 @@ namespace isaacb
             ix = iclamp(ix, -1, g.ls[0] - 1);
             iy = iclamp(iy, -1, g.ls[1] - 1);
             iz = iclamp(iz, -1, g.ls[2] - 1);
-            const size_t s0 = brick_slot(g, ix, iy, iz) * per;
-            const size_t s1 = s0 + size_t(64) * per;
+            size_t above;
+            const size_t s0 = source_slot(g, ix, iy, iz, above) * per;
+            const size_t s1 = above * per;
 #pragma unroll
             for(int c = 0; c < 4; ++c)
             {
@@ -81,7 +82,8 @@ namespace isaacb
             const int ix = iclamp(f2i(pos.x), 0, g.ls[0] - 1);
             const int iy = iclamp(f2i(pos.y), 0, g.ls[1] - 1);
             const int iz = iclamp(f2i(pos.z), 0, g.ls[2] - 1);
-            const size_t s0 = brick_slot(g, ix, iy, iz) * per;
+            size_t above;
+            const size_t s0 = source_slot(g, ix, iy, iz, above) * per;
 #pragma unroll
             for(int c = 0; c < 4; ++c)
                 if(c < S.ncomp)
@@ -353,7 +355,7 @@ namespace isaacb
                     {
                         ++n;
                         const float3 pos = march_pos(m, i);
-                        size_t q0;
+                        size_t q0, q1;
                         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
                         if(LINEAR)
                         {
@@ -365,14 +367,14 @@ namespace isaacb
                             const int ix = iclamp(f2i(cx), -1, g.ls[0] - 1);
                             const int iy = iclamp(f2i(cy), -1, g.ls[1] - 1);
                             const int iz = iclamp(f2i(cz), -1, g.ls[2] - 1);
-                            q0 = brick_slot(g, ix, iy, iz);
+                            q0 = source_slot(g, ix, iy, iz, q1);
                         }
                         else
                         {
                             const int ix = iclamp(f2i(pos.x), 0, g.ls[0] - 1);
                             const int iy = iclamp(f2i(pos.y), 0, g.ls[1] - 1);
                             const int iz = iclamp(f2i(pos.z), 0, g.ls[2] - 1);
-                            q0 = brick_slot(g, ix, iy, iz);
+                            q0 = source_slot(g, ix, iy, iz, q1);
                         }
                         for(int s = 0; s < p.nVol; ++s)
                         {
@@ -385,7 +387,7 @@ namespace isaacb
                             float v[4] = {0, 0, 0, 0};
                             if(LINEAR)
                             {
-                                load_quad<DT>(S.bricks, q0 + 64, b);
+                                load_quad<DT>(S.bricks, q1, b);
                                 v[0] = tri_q(fx, fy, fz, a[0], a[1], a[2], a[3], b[0], b[1], b[2], b[3]);
                             }
                             else
@@ -439,8 +441,9 @@ namespace isaacb
     // FP32 trilinear arithmetic (two lanes, the scalar roundings), and with IDEM the
     // functor chain is skipped.  Same operations in the same order per source, so the
     // frame is bit-identical to the general kernels'.
+    // (4 CTAs per SM: 61 registers without spills, twice the warps of the unbounded 88)
     template<int DT, bool LINEAR, int NS, bool IDEM>
-    __global__ void __launch_bounds__(256) k_shade_volume_per_source_n(
+    __global__ void __launch_bounds__(256, 4) k_shade_volume_per_source_n(
         const __grid_constant__ FrameParams p,
         const __grid_constant__ ActiveSources act)
     {
@@ -476,8 +479,9 @@ namespace isaacb
                     {
                         ++n;
                         const float3 pos = march_pos(m, i);
-                        uint32_t q0;
+                        uint32_t q0, q1 = 0;
                         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+                        size_t above;
                         if(LINEAR)
                         {
                             const float cx = pos.x - 0.5f, cy = pos.y - 0.5f, cz = pos.z - 0.5f;
@@ -487,14 +491,15 @@ namespace isaacb
                             const int ix = iclamp(f2i(cx), -1, g.ls[0] - 1);
                             const int iy = iclamp(f2i(cy), -1, g.ls[1] - 1);
                             const int iz = iclamp(f2i(cz), -1, g.ls[2] - 1);
-                            q0 = uint32_t(brick_slot(g, ix, iy, iz));
+                            q0 = uint32_t(source_slot(g, ix, iy, iz, above));
+                            q1 = uint32_t(above);
                         }
                         else
                         {
                             const int ix = iclamp(f2i(pos.x), 0, g.ls[0] - 1);
                             const int iy = iclamp(f2i(pos.y), 0, g.ls[1] - 1);
                             const int iz = iclamp(f2i(pos.z), 0, g.ls[2] - 1);
-                            q0 = uint32_t(brick_slot(g, ix, iy, iz));
+                            q0 = uint32_t(source_slot(g, ix, iy, iz, above));
                         }
                         float a[NS][4], b[NS][4], val[NS];
 #pragma unroll
@@ -502,7 +507,7 @@ namespace isaacb
                         {
                             load_quad<DT>(br[k], q0, a[k]);
                             if(LINEAR)
-                                load_quad<DT>(br[k], q0 + 64u, b[k]);
+                                load_quad<DT>(br[k], q1, b[k]);
                         }
                         if(LINEAR)
                         {

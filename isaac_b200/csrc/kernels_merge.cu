@@ -868,7 +868,7 @@ namespace isaacb
         {
             const int lx = s & 7, ly = (s >> 3) & 7, lz = s >> 6;
             const int t = (lz * kApron + ly) * kApron + lx;
-            const size_t base = (brick * kSlotsPerBrick + s) * per;
+            const size_t base = (brick * kSlotsPerBrick + morton_slot(lx, ly, lz)) * per;
             for(int c = 0; c < p.ncomp; ++c)
             {
                 store_elem<DT>(p.out, base + 4 * c + 0, valS[c][t]);
@@ -982,8 +982,8 @@ namespace isaacb
             {
                 const int j = layer / kApron, lz = layer - j * kApron;
                 const int t = lz * (kApron * kPackPitch) + base + 8 * j;
-                store_quad<0>(p.out, brick0 * kSlotsPerBrick + size_t(layer) * 64 + lxy, valS[t], valS[t + 1],
-                              valS[t + kPackPitch], valS[t + kPackPitch + 1]);
+                store_quad<0>(p.out, (brick0 + j) * kSlotsPerBrick + morton_slot(lxy & 7, lxy >> 3, lz), valS[t],
+                              valS[t + 1], valS[t + kPackPitch], valS[t + kPackPitch + 1]);
             }
         }
         else
@@ -1003,7 +1003,8 @@ namespace isaacb
                 pack_pair<DT>(b0, b1, w[1]);
                 pack_pair<DT>(a1, a2, w[2]);
                 pack_pair<DT>(b1, b2, w[3]);
-                const size_t slot = brick0 * kSlotsPerBrick + size_t(layer) * 64 + lxy; // even
+                // x-adjacent slots (lx even, lx + 1) are adjacent in Morton order too
+                const size_t slot = (brick0 + j) * kSlotsPerBrick + morton_slot(lxy & 7, lxy >> 3, lz); // even
                 reinterpret_cast<uint4*>(p.out)[slot >> 1] = make_uint4(w[0], w[1], w[2], w[3]);
             }
         }
