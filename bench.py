@@ -1078,6 +1078,9 @@ def measure_blend(args, ranks: int = 8) -> dict:
     n = 10
     total = 0.0
     for _ in range(n):
+        # the device sleeps while the host queues the flush, the events and the blend, so
+        # that no host time falls between the two events
+        torch.cuda._sleep(2_000_000)
         flush.sum()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)

@@ -51,17 +51,23 @@ namespace isaacb
             uint32_t bg;
         };
 
+        // Two channels per 32-bit word, one in each 16-bit lane: b * f <= 255 * 255 fits a
+        // lane, and for 0 <= x <= 65025, floor(x / 255) == (x + 1 + (x >> 8)) >> 8 with
+        // the sum <= 65280, so no lane carries into the next.  Byte permutes pick the
+        // lanes' bytes; the final permute keeps the low byte of each channel sum, which is
+        // the mod-256 result.
+        __device__ __forceinline__ uint32_t div255_lanes(uint32_t x)
+        {
+            const uint32_t t = x + 0x00010001u + __byte_perm(x, 0u, 0x4341);
+            return __byte_perm(t, 0u, 0x4341);
+        }
+
         __device__ __forceinline__ uint32_t under(uint32_t acc, uint32_t src)
         {
             const uint32_t f = 255u - (acc >> 24);
-            uint32_t out = 0;
-#pragma unroll
-            for(int c = 0; c < 4; ++c)
-            {
-                const uint32_t a = (acc >> (8 * c)) & 0xFFu, b = (src >> (8 * c)) & 0xFFu;
-                out |= ((a + b * f / 255u) & 0xFFu) << (8 * c);
-            }
-            return out;
+            const uint32_t lo = __byte_perm(acc, 0u, 0x4240) + div255_lanes(__byte_perm(src, 0u, 0x4240) * f);
+            const uint32_t hi = __byte_perm(acc, 0u, 0x4341) + div255_lanes(__byte_perm(src, 0u, 0x4341) * f);
+            return __byte_perm(lo, hi, 0x6240);
         }
 
         // four pixels per thread: one 16-byte load per image, all issued before the fold
@@ -69,8 +75,9 @@ namespace isaacb
         {
             for(size_t q = blockIdx.x * size_t(blockDim.x) + threadIdx.x; q < quads; q += size_t(gridDim.x) * blockDim.x)
             {
-                uint4 acc = make_uint4(0, 0, 0, 0);
-                for(int k0 = 0; k0 < a.count; k0 += 8)
+                // the first image under an empty accumulator is itself (f = 255)
+                uint4 acc = __ldg(reinterpret_cast<const uint4*>(a.img[0]) + q);
+                for(int k0 = 1; k0 < a.count; k0 += 8)
                 {
                     uint4 v[8];
                     const int m = min(8, a.count - k0);
