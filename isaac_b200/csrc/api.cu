@@ -276,6 +276,7 @@ struct isaacb_ctx
     // device buffers
     float4* lutDev = nullptr;
     float4* lutPre = nullptr; // merge scratch: weighted premultiplied table entries
+    float4* psPre = nullptr; // per-source march scratch: the same for the active sources
     float* lutPinned = nullptr;
     cudaEvent_t lutEvent = nullptr;
     uint32_t* volLin = nullptr; // merge scratch: the combined volume, linear RGBA8
@@ -729,6 +730,7 @@ extern "C"
         };
         alloc((void**) &c->lutDev, c->lutHost.size() * sizeof(float));
         alloc((void**) &c->lutPre, c->lutHost.size() * sizeof(float));
+        alloc((void**) &c->psPre, c->lutHost.size() * sizeof(float));
         if(e == cudaSuccess)
             e = cudaMallocHost((void**) &c->lutPinned, c->lutHost.size() * sizeof(float));
         if(e == cudaSuccess)
@@ -778,6 +780,7 @@ extern "C"
             return ISAACB_OK;
         cudaFree(c->lutDev);
         cudaFree(c->lutPre);
+        cudaFree(c->psPre);
         if(c->lutPinned)
             cudaFreeHost(c->lutPinned);
         if(c->lutEvent)
@@ -1314,6 +1317,8 @@ extern "C"
             if(c->renderer == ISAACB_RENDERER_PER_SOURCE && (S.weight != 0.0f || S.iso != 0.0f) && !S.bricks)
                 return fail(c, ISAACB_NOT_READY, "isaacb_render: per-source bricks missing; call isaacb_update");
         }
+        p.psPre = c->psPre;
+        p.negZero = -0.0f;
         p.color = c->color;
         p.depth = c->depth;
         p.normal = c->normal;
@@ -1356,11 +1361,13 @@ extern "C"
         {
             PhaseTimer t(c, 4, st);
             if(c->renderer == ISAACB_RENDERER_COMBINED)
+            {
                 launch_shade_volume(p, p.totalWeightAll > 0.0f, st);
+                c->renderLaunches++;
+            }
             else
-                launch_shade_volume_per_source(p, st);
+                c->renderLaunches += uint32_t(launch_shade_volume_per_source(p, st));
         }
-        c->renderLaunches++;
         ISAACB_CUDA(c, cudaGetLastError(), "isaacb_render launch");
         if(rgba_dev)
         {

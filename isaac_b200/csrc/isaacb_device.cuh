@@ -627,17 +627,21 @@ namespace isaacb
         asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
         return r;
     }
-    __device__ __forceinline__ f2p f2p_mul(f2p a, f2p b)
-    {
-        f2p r;
-        asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-        return r;
-    }
     __device__ __forceinline__ f2p f2p_add(f2p a, f2p b)
     {
         f2p r;
         asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
         return r;
+    }
+    // a * b rounded once, for a product that feeds an add.  The assembler contracts
+    // mul.rn.f32x2 followed by add.rn.f32x2 into one fma.rn.f32x2 (the explicit rounding
+    // does not stop it for the packed forms, as it does for mul.rn.f32), which rounds
+    // once instead of twice.  An fma whose addend is -0 is the rounded product for every
+    // a and b (x + -0 = x, +0 included), and with the -0 taken from a kernel parameter the
+    // assembler cannot turn it back into a multiply.
+    __device__ __forceinline__ f2p f2p_mul_exact(f2p a, f2p b, f2p negZero)
+    {
+        return f2p_fma(a, b, negZero);
     }
     // bytes (c, c+1) of w as an exact float pair: 2^23 + b bit patterns minus 2^23
     __device__ __forceinline__ f2p ubyte_pair(uint32_t w, int c, f2p bias)

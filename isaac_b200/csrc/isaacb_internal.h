@@ -192,6 +192,8 @@ namespace isaacb
         ParticleSrc part[kMaxSources];
         // per-source renderer
         PerSourceSrc ps[kMaxSources];
+        float4* psPre; // scratch: the weighted premultiplied tables of the active sources
+        float negZero; // -0.0f, the addend of packed products that must round on their own (f2p_mul_exact)
         // G-buffer
         uchar4* color;
         float* depth;
@@ -250,5 +252,6 @@ namespace isaacb
     void launch_iso_per_source(const FrameParams& p, cudaStream_t s);
     void launch_ssao(const FrameParams& p, cudaStream_t s);
     void launch_shade_volume(const FrameParams& p, bool volume, cudaStream_t s);
-    void launch_shade_volume_per_source(const FrameParams& p, cudaStream_t s);
+    // returns the number of kernels it launched
+    int launch_shade_volume_per_source(const FrameParams& p, cudaStream_t s);
 } // namespace isaacb

@@ -428,20 +428,55 @@ namespace isaacb
         int idx[kMaxSources];
         const void* bricks[kMaxSources];
         float weight[kMaxSources];
+        // active source k's premultiplied table, biased so that the float bits of
+        // 1.5 * 2^23 + index address entry index (see transfer_entry)
+        const char* pre[kMaxSources];
     };
 
-    // a*(1-o) + b*o on two lanes (two sources), each lane rounded exactly like lin()
-    __device__ __forceinline__ f2p lin2(f2p omo, f2p o, f2p a, f2p b)
+    // The volume term of every table entry of the active sources, once per frame instead
+    // of once per sample: a = c.w * weight, (c.x * a, c.y * a, c.z * a, a).  These are the
+    // products the per-sample loop of PerSourceVolumeRenderKernel forms
+    // (lib/isaac/isaac_volume_kernel.hpp:365-377: color.w *= weight; value += color * color.w),
+    // so the sums that use them round the same way.
+    __global__ void __launch_bounds__(256) k_ps_premultiply(const float4* __restrict__ lut, ActiveSources act, float4* __restrict__ out, int ts)
     {
-        return f2p_add(f2p_mul(a, omo), f2p_mul(b, o));
+        const int k = blockIdx.y;
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if(i >= ts)
+            return;
+        const float4 c = __ldg(lut + size_t(act.idx[k]) * ts + i);
+        const float a = c.w * act.weight[k];
+        out[size_t(k) * ts + i] = make_float4(c.x * a, c.y * a, c.z * a, a);
+    }
+
+    // the premultiplied entry of lut_index_fast(v, ts) as two FP32 pairs (r, g) and (b, a):
+    // round(clamp(v * ts, 0, ts - 1)) is floor(x + 0.5) with the add rounded down (it never
+    // crosses the next integer), and the floor comes as float bits from a magic-number add
+    // also rounded down; both give lut_index_fast's index for every v, NaN included
+    __device__ __forceinline__ void transfer_entry(const char* biased, float v, float tsf, float tsMax, f2p& rg, f2p& ba)
+    {
+        const float xi = fminf(fmaxf(v * tsf, 0.0f), tsMax);
+        const float t = __fadd_rd(__fadd_rd(xi, 0.5f), 12582912.0f);
+        const ulonglong2 e = __ldg(reinterpret_cast<const ulonglong2*>(biased + size_t(uint32_t(__float_as_int(t))) * sizeof(float4)));
+        rg.v = e.x;
+        ba.v = e.y;
+    }
+
+    // a*(1-o) + b*o on two lanes (two sources), each lane rounded exactly like lin():
+    // both products round before the add (f2p_mul_exact)
+    __device__ __forceinline__ f2p lin2(f2p omo, f2p o, f2p a, f2p b, f2p nz)
+    {
+        return f2p_add(f2p_mul_exact(a, omo, nz), f2p_mul_exact(b, o, nz));
     }
 
     // k_shade_volume_per_source_scalar for 1..4 weighted sources known at compile time:
     // the sources' quads are all loaded before any is used, pairs of sources share packed
     // FP32 trilinear arithmetic (two lanes, the scalar roundings), and with IDEM the
-    // functor chain is skipped.  Same operations in the same order per source, so the
-    // frame is bit-identical to the general kernels'.
-    // (4 CTAs per SM: 61 registers without spills, twice the warps of the unbounded 88)
+    // functor chain is skipped.  The weighted premultiplied table entries come from
+    // k_ps_premultiply, found with a 6-instruction index, and value and colour run as
+    // FP32 pairs.  Same operations in the same order per source, so the frame is
+    // bit-identical to the general kernels'.
+    // (4 CTAs per SM: 58 registers without spills, twice the warps of the unbounded 88)
     template<int DT, bool LINEAR, int NS, bool IDEM>
     __global__ void __launch_bounds__(256, 4) k_shade_volume_per_source_n(
         const __grid_constant__ FrameParams p,
@@ -464,17 +499,17 @@ namespace isaacb
                     legacy_bounds(p.g, m);
                     const Geom& g = p.g;
                     const void* br[NS];
-                    float wt[NS];
-                    const float4* lut[NS];
 #pragma unroll
                     for(int k = 0; k < NS; ++k)
-                    {
                         br[k] = act.bricks[k];
-                        wt[k] = act.weight[k];
-                        lut[k] = p.lut + size_t(act.idx[k]) * p.ts;
-                    }
-                    float4 value = make_float4(0, 0, 0, 0);
-                    float4 color = make_float4(0, 0, 0, 0);
+                    const float tsf = float(p.ts), tsMax = float(p.ts - 1);
+                    const f2p fac = f2p_make(m.factor, m.factor);
+                    const f2p nz = f2p_make(p.negZero, p.negZero);
+                    // value and colour as FP32 pairs (r, g), (b, a); every lane rounds like
+                    // the scalar op
+                    f2p vrg = f2p_make(0.0f, 0.0f), vba = f2p_make(0.0f, 0.0f);
+                    f2p crg = f2p_make(0.0f, 0.0f), cba = f2p_make(0.0f, 0.0f);
+                    float cw = 0.0f;
                     for(int i = m.startSteps; i <= m.endSteps; i++)
                     {
                         ++n;
@@ -518,13 +553,13 @@ namespace isaacb
                             for(int k = 0; k + 1 < NS; k += 2)
                             {
                                 // quad order (x0,y0),(x0+1,y0),(x0,y0+1),(x0+1,y0+1); tri_q's lerp tree
-                                const f2p z00 = lin2(omz, vz, f2p_make(a[k][0], a[k + 1][0]), f2p_make(b[k][0], b[k + 1][0]));
-                                const f2p z01 = lin2(omz, vz, f2p_make(a[k][2], a[k + 1][2]), f2p_make(b[k][2], b[k + 1][2]));
-                                const f2p z10 = lin2(omz, vz, f2p_make(a[k][1], a[k + 1][1]), f2p_make(b[k][1], b[k + 1][1]));
-                                const f2p z11 = lin2(omz, vz, f2p_make(a[k][3], a[k + 1][3]), f2p_make(b[k][3], b[k + 1][3]));
-                                const f2p A = lin2(omy, vy, z00, z01);
-                                const f2p B = lin2(omy, vy, z10, z11);
-                                f2p_split(lin2(omx, vx, A, B), val[k], val[k + 1]);
+                                const f2p z00 = lin2(omz, vz, f2p_make(a[k][0], a[k + 1][0]), f2p_make(b[k][0], b[k + 1][0]), nz);
+                                const f2p z01 = lin2(omz, vz, f2p_make(a[k][2], a[k + 1][2]), f2p_make(b[k][2], b[k + 1][2]), nz);
+                                const f2p z10 = lin2(omz, vz, f2p_make(a[k][1], a[k + 1][1]), f2p_make(b[k][1], b[k + 1][1]), nz);
+                                const f2p z11 = lin2(omz, vz, f2p_make(a[k][3], a[k + 1][3]), f2p_make(b[k][3], b[k + 1][3]), nz);
+                                const f2p A = lin2(omy, vy, z00, z01, nz);
+                                const f2p B = lin2(omy, vy, z10, z11, nz);
+                                f2p_split(lin2(omx, vx, A, B, nz), val[k], val[k + 1]);
                             }
                             if(NS & 1)
                             {
@@ -538,6 +573,8 @@ namespace isaacb
                             for(int k = 0; k < NS; ++k)
                                 val[k] = a[k][0];
                         }
+                        // value gains the weighted premultiplied entries (it carries over
+                        // from the previous sample, scaled by the factor, as in the reference)
 #pragma unroll
                         for(int k = 0; k < NS; ++k)
                         {
@@ -547,22 +584,25 @@ namespace isaacb
                                 float v[4] = {val[k], 0.0f, 0.0f, 0.0f};
                                 result = apply_chain(v, 1, p.ps[act.idx[k]].chain);
                             }
-                            float4 c = __ldg(lut[k] + lut_index_fast(result, p.ts));
-                            c.w *= wt[k];
-                            value.x += c.x * c.w;
-                            value.y += c.y * c.w;
-                            value.z += c.z * c.w;
-                            value.w += c.w;
+                            f2p erg, eba;
+                            transfer_entry(act.pre[k], result, tsf, tsMax, erg, eba);
+                            vrg = f2p_add(vrg, erg);
+                            vba = f2p_add(vba, eba);
                         }
-                        const float oma = 1.0f - color.w;
-                        value = make_float4(value.x * m.factor, value.y * m.factor, value.z * m.factor, value.w * m.factor);
-                        color.x += oma * value.x;
-                        color.y += oma * value.y;
-                        color.z += oma * value.z;
-                        color.w += oma * value.w;
-                        if(color.w > 0.99f)
+                        const float oma = 1.0f - cw;
+                        const f2p om = f2p_make(oma, oma);
+                        vrg = f2p_mul_exact(vrg, fac, nz);
+                        vba = f2p_mul_exact(vba, fac, nz);
+                        crg = f2p_add(crg, f2p_mul_exact(om, vrg, nz));
+                        cba = f2p_add(cba, f2p_mul_exact(om, vba, nz));
+                        float cb;
+                        f2p_split(cba, cb, cw);
+                        if(cw > 0.99f)
                             break;
                     }
+                    float4 color;
+                    f2p_split(crg, color.x, color.y);
+                    f2p_split(cba, color.z, color.w);
                     const float4 solid = from_byte4(p.color[o]);
                     const float r = 1.0f - color.w;
                     color = make_float4(color.x + r * solid.x, color.y + r * solid.y, color.z + r * solid.z, color.w + r * solid.w);
@@ -577,6 +617,7 @@ namespace isaacb
     template<int DT, bool LINEAR, bool IDEM>
     void launch_ps_n(const FrameParams& p, const ActiveSources& act, dim3 grid, cudaStream_t s)
     {
+        k_ps_premultiply<<<dim3((p.ts + 255) / 256, act.n), 256, 0, s>>>(p.lut, act, p.psPre, p.ts);
         switch(act.n)
         {
         case 1: k_shade_volume_per_source_n<DT, LINEAR, 1, IDEM><<<grid, 256, 0, s>>>(p, act); break;
@@ -594,7 +635,7 @@ namespace isaacb
             idem ? launch_ps_n<DT, false, true>(p, act, grid, s) : launch_ps_n<DT, false, false>(p, act, grid, s);
     }
 
-    void launch_shade_volume_per_source(const FrameParams& p, cudaStream_t s)
+    int launch_shade_volume_per_source(const FrameParams& p, cudaStream_t s)
     {
         dim3 grid((p.v.W + 31) / 32, (p.v.H + 7) / 8);
         // the scalar kernel serves frames whose weighted sources are all scalar, persistent and of one type
@@ -621,6 +662,8 @@ namespace isaacb
                 act.idx[act.n] = k;
                 act.bricks[act.n] = S.bricks;
                 act.weight[act.n] = S.weight;
+                act.pre[act.n] = reinterpret_cast<const char*>(p.psPre + size_t(act.n) * p.ts)
+                    - size_t(0x4B400000u) * sizeof(float4);
                 act.n++;
                 idem = idem && S.chain.op[0] == OP_IDEM && S.chain.op[1] == OP_IDEM && S.chain.op[2] == OP_IDEM;
             }
@@ -634,7 +677,7 @@ namespace isaacb
                     launch_ps_dt<1>(p, act, lin, idem, grid, s);
                 else
                     launch_ps_dt<2>(p, act, lin, idem, grid, s);
-                return;
+                return 2;
             }
             if(dt == 0)
                 lin ? k_shade_volume_per_source_scalar<0, true><<<grid, 256, 0, s>>>(p)
@@ -645,8 +688,9 @@ namespace isaacb
             else
                 lin ? k_shade_volume_per_source_scalar<2, true><<<grid, 256, 0, s>>>(p)
                     : k_shade_volume_per_source_scalar<2, false><<<grid, 256, 0, s>>>(p);
-            return;
+            return 1;
         }
         k_shade_volume_per_source<<<grid, 256, 0, s>>>(p);
+        return 1;
     }
 } // namespace isaacb

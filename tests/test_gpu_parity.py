@@ -278,6 +278,27 @@ def test_per_source_scalar_sources(dtype, interp):
     assert_image_parity(got, ref)
 
 
+@pytest.mark.parametrize("dtype", [0, 1, 2])
+@pytest.mark.parametrize("interp", [True, False])
+@pytest.mark.parametrize("seed", [1, 2])
+def test_per_source_packed_arithmetic_is_exact(dtype, interp, seed):
+    """The specialised per-source kernel pairs sources and colour channels in packed FP32
+    arithmetic and takes weighted premultiplied table entries; every lane must round like
+    the oracle's scalar float ops.  With non-unit weights (1.5 rounds) the frames equal
+    the oracle's exactly -- a packed multiply contracted into the following add shows up
+    here as single-pixel 1 LSB differences."""
+    fields = [f.numpy() for f in scenes.precision_scene(48)]
+    s = Scene(n=(48, 48, 48), fb=(128, 96), volumes=[(f, True) for f in fields], optimized=False)
+    s.transfer = [scenes.transfer_4point(0.7 * i) for i in range(4)]
+    s.storage = [dtype] * 4
+    s.interpolation = interp
+    s.weights = [2.0, 0.0, 1.5, 2.0]
+    s.camera_seed = seed
+    got, ref, _, _ = _frames(s)
+    st = image_diff(got, ref)
+    assert st["max"] == 0, st
+
+
 @pytest.mark.parametrize("interp", [True, False])
 def test_per_source_iso(interp):
     s = gaussian_pair(n=32, fb=(64, 48), optimized=False, interpolation=interp, iso=[0.3, 0.2])
