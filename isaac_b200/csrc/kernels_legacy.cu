@@ -510,8 +510,16 @@ namespace isaacb
                     f2p vrg = f2p_make(0.0f, 0.0f), vba = f2p_make(0.0f, 0.0f);
                     f2p crg = f2p_make(0.0f, 0.0f), cba = f2p_make(0.0f, 0.0f);
                     float cw = 0.0f;
-                    for(int i = m.startSteps; i <= m.endSteps; i++)
+                    // The warp walks absolute step indices together from its earliest first
+                    // step, each lane sampling only inside its own range: lanes then sample
+                    // the same depth shell at once, which keeps their taps close where the
+                    // entry face is oblique to the view.  Each ray's samples and their
+                    // order are unchanged.
+                    const int wStart = __reduce_min_sync(__activemask(), m.startSteps);
+                    for(int i = wStart; i <= m.endSteps; i++)
                     {
+                        if(i < m.startSteps)
+                            continue;
                         ++n;
                         const float3 pos = march_pos(m, i);
                         uint32_t q0, q1 = 0;
