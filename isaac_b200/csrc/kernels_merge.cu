@@ -394,28 +394,17 @@ namespace isaacb
     // ---------------------------------------------------------------- merge, pass 2: bricks
     // One CTA per row of kPackRow = 4 bricks along x.  The row's 33 x 9 x 9 texels (the
     // bricks' voxels plus the apron on the low side, clamped at the volume border) come
-    // from the linear textures into shared memory, one texel row per warp with the lanes
-    // along x.  A lane's texels all have the same x, so they belong to the same one or two
+    // from the linear textures into shared memory (staged row r = lz * 9 + ly at pitch
+    // kPackPitch), texel rows per warp with the lanes along x.  A lane's texels all have the same x, so they belong to the same one or two
     // bricks: the lane keeps one "any non-zero" bit and one maximum alpha byte, and a warp
     // reduction per brick gives the flags that drive empty-space skipping.  Then the 4
     // bricks' 576-slot quad blocks, contiguous in memory, go out as 16-byte stores: thread
     // (lx, ly) walks the slot layers lz of all 4 bricks, and slot index = layer * 64 + lxy.
     // Every texel is a copy of a voxel pass 1 computed once.
     constexpr int kPackRow = 4;
-    constexpr int kPackW = 8 * kPackRow + 1; // texels per staged row
     constexpr int kPackPitch = 40; // row pitch in words: 40 = 8 mod 32 keeps the quad reads conflict-free
     constexpr int kPackRows = kApron * kApron; // (ly, lz) rows
     constexpr int kPackWords = kPackRows * kPackPitch;
-    constexpr int kRowsPerWarp = (kPackRows + 7) / 8; // 8 warps share the 81 rows
-
-    // linear index of the first voxel of staged row r = lz * 9 + ly of brick row (by, bz)
-    __device__ __forceinline__ size_t pack_row(const Geom& g, int by, int bz, int r)
-    {
-        const int lz = r / kApron, ly = r - lz * kApron;
-        const int y = iclamp(by * 8 - 1 + ly, 0, g.ls[1] - 1);
-        const int z = iclamp(bz * 8 - 1 + lz, 0, g.ls[2] - 1);
-        return (size_t(z) * g.ls[1] + y) * g.ls[0];
-    }
 
     template<bool ISO>
     __global__ void __launch_bounds__(256) k_merge_pack(const __grid_constant__ MergeParams p)
@@ -438,32 +427,43 @@ namespace isaacb
         const int jlo = lane >= 1 ? (lane - 1) >> 3 : 0, jhi = min(lane >> 3, kPackRow - 1);
         int laneAny = 0, laneIso = 0, any32 = 0, iso32 = 0;
         // all of the warp's row loads are issued before any is used, so that enough
-        // bytes are in flight to cover the memory latency
-        // (lane 0 also reads the row's 33rd texel, lx = 32)
-        uint32_t v[kRowsPerWarp], w[kRowsPerWarp], v2[kRowsPerWarp], w2[kRowsPerWarp];
+        // bytes are in flight to cover the memory latency (lane 0 also reads the row's
+        // 33rd texel, lx = 32).  Warp w stages the rows ly = w of all 9 planes lz and the
+        // row ly = 8 of plane w (warp 0 also of plane 8): one y offset per warp and one
+        // multiply per plane, as the kernel is bound by instruction issue.
+        const size_t plane = size_t(g.ls[0]) * size_t(g.ls[1]);
+        const size_t yA = size_t(iclamp(by * 8 - 1 + warp, 0, g.ls[1] - 1)) * size_t(g.ls[0]);
+        const size_t yB = size_t(iclamp(by * 8 + 7, 0, g.ls[1] - 1)) * size_t(g.ls[0]);
+        constexpr int kRows = kApron + 2; // 9 planes of row ly = w, then row ly = 8 of planes w and 8
+        uint32_t v[kRows], w[kRows], v2[kRows], w2[kRows];
+        int rr[kRows];
 #pragma unroll
-        for(int i = 0; i < kRowsPerWarp; ++i)
+        for(int i = 0; i < kRows; ++i)
         {
-            const int r = warp + 8 * i;
-            if(r < kPackRows)
+            const int lz = i < kApron ? i : (i == kApron ? warp : 8);
+            const int ly = i < kApron ? warp : 8;
+            rr[i] = lz * kApron + ly;
+            if(i == kApron + 1 && warp != 0)
             {
-                const size_t row = pack_row(g, by, bz, r);
-                v[i] = __ldg(p.volLin + row + x0);
+                rr[i] = -1;
+                continue;
+            }
+            const size_t row = size_t(iclamp(bz * 8 - 1 + lz, 0, g.ls[2] - 1)) * plane + (i < kApron ? yA : yB);
+            v[i] = __ldg(p.volLin + row + x0);
+            if(ISO)
+                w[i] = __ldg(p.isoLin + row + x0);
+            if(lane == 0)
+            {
+                v2[i] = __ldg(p.volLin + row + x32);
                 if(ISO)
-                    w[i] = __ldg(p.isoLin + row + x0);
-                if(lane == 0)
-                {
-                    v2[i] = __ldg(p.volLin + row + x32);
-                    if(ISO)
-                        w2[i] = __ldg(p.isoLin + row + x32);
-                }
+                    w2[i] = __ldg(p.isoLin + row + x32);
             }
         }
 #pragma unroll
-        for(int i = 0; i < kRowsPerWarp; ++i)
+        for(int i = 0; i < kRows; ++i)
         {
-            const int r = warp + 8 * i;
-            if(r < kPackRows)
+            const int r = rr[i];
+            if(r >= 0)
             {
                 volS[r * kPackPitch + lane] = v[i];
                 laneAny |= v[i] != 0u;
@@ -932,10 +932,24 @@ namespace isaacb
         }
     }
 
+    // the stored value of voxel idx: with SIMPLE the source has one component and no
+    // functor chain, and the value is the voxel itself
+    template<bool SIMPLE>
+    __device__ __forceinline__ float source_value_t(const SourceBrickParams& p, size_t idx)
+    {
+        if constexpr(SIMPLE)
+            return __ldg(p.src + idx);
+        else
+            return source_value(p, idx);
+    }
+
     // One-component bricks as k_merge_pack builds the combined ones: one CTA per row of 4
-    // bricks along x, texel rows staged one per warp with the lanes along x, then every
-    // slot of the 4 bricks as one vector store, contiguous in memory.
-    template<int DT>
+    // bricks along x, texel rows staged with the lanes along x, then every slot of the 4
+    // bricks as one vector store, contiguous in memory.  The kernel is bound by
+    // instruction issue, so the staging is arranged for little index arithmetic: warp w
+    // stages the rows ly = w of all 9 planes lz (one y offset per warp, one multiply per
+    // plane) and the row ly = 8 of plane w (warp 0 also of plane 8).
+    template<int DT, bool SIMPLE>
     __global__ void __launch_bounds__(256) k_source_bricks_row(const __grid_constant__ SourceBrickParams p)
     {
         __shared__ float valS[kPackWords];
@@ -945,31 +959,54 @@ namespace isaacb
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         const int x0 = iclamp(bx0 * 8 - 1 + lane, 0, g.ls[0] - 1);
         const int x32 = iclamp(bx0 * 8 + 31, 0, g.ls[0] - 1);
+        const size_t plane = size_t(g.ls[0]) * size_t(g.ls[1]);
+        const size_t yA = size_t(iclamp(by * 8 - 1 + warp, 0, g.ls[1] - 1)) * size_t(g.ls[0]);
+        const size_t yB = size_t(iclamp(by * 8 + 7, 0, g.ls[1] - 1)) * size_t(g.ls[0]);
         // all of the warp's row loads are issued before any is used (lane 0 also reads
         // the row's 33rd texel, lx = 32)
-        float v[kRowsPerWarp], v2[kRowsPerWarp];
+        float v[kApron], v2[kApron], u[2], u2[2];
 #pragma unroll
-        for(int i = 0; i < kRowsPerWarp; ++i)
+        for(int lz = 0; lz < kApron; ++lz)
         {
-            const int r = warp + 8 * i;
-            if(r < kPackRows)
-            {
-                const size_t row = pack_row(g, by, bz, r);
-                v[i] = source_value(p, row + x0);
-                if(lane == 0)
-                    v2[i] = source_value(p, row + x32);
-            }
+            const size_t row = size_t(iclamp(bz * 8 - 1 + lz, 0, g.ls[2] - 1)) * plane + yA;
+            v[lz] = source_value_t<SIMPLE>(p, row + x0);
+            if(lane == 0)
+                v2[lz] = source_value_t<SIMPLE>(p, row + x32);
         }
-#pragma unroll
-        for(int i = 0; i < kRowsPerWarp; ++i)
         {
-            const int r = warp + 8 * i;
-            if(r < kPackRows)
-            {
-                valS[r * kPackPitch + lane] = v[i];
-                if(lane == 0)
-                    valS[r * kPackPitch + 32] = v2[i];
-            }
+            const size_t row = size_t(iclamp(bz * 8 - 1 + warp, 0, g.ls[2] - 1)) * plane + yB;
+            u[0] = source_value_t<SIMPLE>(p, row + x0);
+            if(lane == 0)
+                u2[0] = source_value_t<SIMPLE>(p, row + x32);
+        }
+        if(warp == 0)
+        {
+            const size_t row = size_t(iclamp(bz * 8 + 7, 0, g.ls[2] - 1)) * plane + yB;
+            u[1] = source_value_t<SIMPLE>(p, row + x0);
+            if(lane == 0)
+                u2[1] = source_value_t<SIMPLE>(p, row + x32);
+        }
+        // staged row r = lz * 9 + ly
+#pragma unroll
+        for(int lz = 0; lz < kApron; ++lz)
+        {
+            const int r = lz * kApron + warp;
+            valS[r * kPackPitch + lane] = v[lz];
+            if(lane == 0)
+                valS[r * kPackPitch + 32] = v2[lz];
+        }
+        {
+            const int r = warp * kApron + 8;
+            valS[r * kPackPitch + lane] = u[0];
+            if(lane == 0)
+                valS[r * kPackPitch + 32] = u2[0];
+        }
+        if(warp == 0)
+        {
+            const int r = 8 * kApron + 8;
+            valS[r * kPackPitch + lane] = u[1];
+            if(lane == 0)
+                valS[r * kPackPitch + 32] = u2[1];
         }
         __syncthreads();
         const size_t brick0 = (size_t(bz) * g.nb[1] + by) * g.nb[0] + bx0;
@@ -1015,12 +1052,13 @@ namespace isaacb
         if(p.ncomp == 1)
         {
             const dim3 grid((p.g.nb[0] + kPackRow - 1) / kPackRow, p.g.nb[1], p.g.nb[2]);
+            const bool simple = p.fdim == 1 && !p.applyChain;
             if(p.dtype == 1)
-                k_source_bricks_row<1><<<grid, 256, 0, s>>>(p);
+                simple ? k_source_bricks_row<1, true><<<grid, 256, 0, s>>>(p) : k_source_bricks_row<1, false><<<grid, 256, 0, s>>>(p);
             else if(p.dtype == 2)
-                k_source_bricks_row<2><<<grid, 256, 0, s>>>(p);
+                simple ? k_source_bricks_row<2, true><<<grid, 256, 0, s>>>(p) : k_source_bricks_row<2, false><<<grid, 256, 0, s>>>(p);
             else
-                k_source_bricks_row<0><<<grid, 256, 0, s>>>(p);
+                simple ? k_source_bricks_row<0, true><<<grid, 256, 0, s>>>(p) : k_source_bricks_row<0, false><<<grid, 256, 0, s>>>(p);
             return;
         }
         dim3 grid(p.g.nb[0], p.g.nb[1], p.g.nb[2]);
