@@ -67,6 +67,16 @@ def parse_args():
     return ap.parse_args()
 
 
+def recorded_traffic(key: str):
+    """DRAM bytes (read + write) of one launch of the line's dominant kernel, from a 1-pass
+    ncu capture of the same workload recorded in profiles/traffic.json; None if absent."""
+    prof = ROOT / "profiles" / "traffic.json"
+    try:
+        return json.loads(prof.read_text()).get(key)
+    except Exception:
+        return None
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -623,7 +633,7 @@ def run_batch(args, world, rank, local, barrier, max_over_ranks):
         "peak_kind": peak_kind,
         "unit": "GB/s",
         "frac": (achieved / peak) if achieved else None,
-        "traffic": None,
+        "traffic": recorded_traffic(f"batch_{args.size}_{args.timesteps}"),
         "algorithmic_bytes_per_sample": 32,
         "samples_per_launch": samples,
         "kernel_ms": render_ms,
@@ -843,7 +853,7 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks):
         "peak_kind": "measured",
         "unit": "GB/s",
         "frac": half_gbs / peaks["hbm_gbs"] if half_gbs else None,
-        "traffic": None,
+        "traffic": recorded_traffic(f"learned_half_{args.size}_{W // 2}x{H // 2}"),
         "algorithmic_bytes_per_sample": 64,
         "samples_per_launch": half_samples,
         "kernel_ms": half_ms,
@@ -1184,13 +1194,8 @@ def main():
     esz = {"f32": 4, "bf16": 2, "f16": 2}[args.dtype]
     bytes_per_sample = 32 if args.renderer == "combined" else esz * 8 * sum(fd for _, fd in sc.volumes)
     achieved = samples * bytes_per_sample / (vol_ms * 1e-3) / 1e9 if vol_ms > 0 else None
-    traffic = None
-    prof = ROOT / "profiles" / "traffic.json"
-    if prof.exists():
-        try:
-            traffic = json.loads(prof.read_text()).get(f"{args.renderer}_{args.size}_{args.width}x{args.height}")
-        except Exception:
-            traffic = None
+    kind = "combined" if args.renderer == "combined" else f"per_source_{args.dtype}"
+    traffic = recorded_traffic(f"{kind}_{args.size}_{args.width}x{args.height}")
     roofline = {
         "bound": "hbm",
         "kernel": "k_shade_volume (shading + volume ray-march)",
