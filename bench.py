@@ -45,11 +45,12 @@ def parse_args():
     ap.add_argument(
         "--scene",
         default="precision",
-        choices=["precision", "gaussian", "full", "batch", "learned"],
+        choices=["precision", "gaussian", "full", "batch", "learned", "sweep"],
         help="precision: N sources of size^3 (default); gaussian: 128^3 scalar + curl at 512x512; "
         "full: 3 x 256^3 + 1M particles, iso, 2 clipping planes, SSAO at 1080p; "
         "batch: the precision sources over 4 timesteps, 16 views of uneven resolution in one launch; "
-        "learned: BF16 bricks, half-size render at twice the step + U-Net vs the plain full-size render",
+        "learned: BF16 bricks, half-size render at twice the step + U-Net vs the plain full-size render; "
+        "sweep: ray-march speed of both renderers against the view angle (a diagnostic, one JSON line per yaw)",
     )
     ap.add_argument("--timesteps", type=int, default=4, help="batch scene: timesteps (contexts)")
     ap.add_argument("--shift", type=float, default=0.05, help="batch scene: advection per timestep, fraction of the box")
@@ -64,6 +65,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-stream", action="store_true", help="skip the streamed-frame measurement")
     ap.add_argument("--cpu-rows", type=int, default=0, help="image rows of the CPU sample (0 = auto)")
+    ap.add_argument("--yaws", default="0,10,20,30,45,60,75,90", help="sweep scene: camera yaws in degrees")
+    ap.add_argument("--pitch", type=float, default=0.35, help="sweep scene: camera pitch in radians")
     return ap.parse_args()
 
 
@@ -738,6 +741,73 @@ def run_batch(args, world, rank, local, barrier, max_over_ranks):
     return 0
 
 
+# ---------------------------------------------------------------------------- view-angle sweep (diagnostic)
+def _sweep_time(viz, buf, repeat=5):
+    import torch
+
+    viz.setCounting(True)
+    viz.render(buf)
+    samples = viz.counters()[0]
+    viz.setCounting(False)
+    for _ in range(2):
+        viz.render(buf)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(repeat):
+        viz.render(buf)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / repeat
+    return round(ms, 3), int(samples), round(samples / ms / 1e6, 1)
+
+
+def run_sweep(args):
+    """Ray-march speed against the viewing angle, a diagnostic for the brick layouts.
+
+    Renders the four spectral sources from an orbit of cameras (``--yaws``) with the
+    per-source renderer (BF16 bricks, full size at step 0.5 and half size at step 1.0,
+    as the learned path uses) and with the combined renderer (full size, step 0.5), and
+    prints one JSON line per view: milliseconds per frame (CUDA events, 5 frames after
+    2 untimed ones), samples per frame (the kernels' own count) and millions of samples
+    per millisecond.  The samples hardly change with the angle, so the rate shows how
+    each layout's access pattern depends on the view direction."""
+    import torch
+
+    from isaac_b200 import IsaacVisualization, VolumeSource, scenes
+    from isaac_b200.recon_train import PairRenderer
+
+    W, H = args.width, args.height
+    n = args.size
+    pr = PairRenderer(n, W, H)
+    pr.set_timestep(0)
+    tfs = [scenes.transfer_4point(0.7 * i) for i in range(4)]
+    pr.set_view(*scenes.orbit_camera(W, H, yaw=0.0, pitch=args.pitch, distance=2.4), tfs)
+    pr.full.update()
+    pr.low.update()
+    fields = scenes.precision_scene(n, device="cuda")
+    comb = IsaacVisualization("combined", (W, H), (n, n, n), (n, n, n), (1, 1, 1), (0, 0, 0),
+                              [VolumeSource(f"s{i}", f.contiguous(), 1) for i, f in enumerate(fields)])
+    comb.setInterpolation(True)
+    for i in range(4):
+        comb.setTransferPoints(i, tfs[i])
+    comb.update()
+    full = torch.empty((H, W, 4), dtype=torch.uint8, device="cuda")
+    half = torch.empty((H // 2, W // 2, 4), dtype=torch.uint8, device="cuda")
+    for deg in (float(v) for v in args.yaws.split(",")):
+        P, MV = scenes.orbit_camera(W, H, yaw=math.radians(deg), pitch=args.pitch, distance=2.4)
+        line = {"yaw_deg": deg, "pitch_rad": args.pitch, "fields": "[ms, samples, Msamples/ms]"}
+        pr.low.setCamera(P, MV)
+        line["per_source_half"] = _sweep_time(pr.low, half)
+        pr.full.setCamera(P, MV)
+        line["per_source_full"] = _sweep_time(pr.full, full)
+        comb.setCamera(P, MV)
+        line["combined_full"] = _sweep_time(comb, full)
+        print(json.dumps(line), flush=True)
+    comb.close()
+    return 0
+
+
 # ---------------------------------------------------------------------------- learned reconstruction scene
 def run_learned(args, world, rank, local, barrier, max_over_ranks):
     """Plain full-size frames against the judged learned path on the same
@@ -1137,6 +1207,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    if args.scene == "sweep":
+        return run_sweep(args)
     if args.scene == "batch":
         return run_batch(args, world, rank, local, barrier, max_over_ranks)
     if args.scene == "learned":

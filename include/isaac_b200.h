@@ -216,9 +216,11 @@ isaacb_status isaacb_get_timing(isaacb_ctx* ctx, void* stream, float ms[ISAACB_T
  * voxels, x fastest, feature_dim floats each), bytecode/params come from
  * isaacb_parse_chain, `result` is 2 device floats (min, max), bit-identical to
  * isaacb_minmax.  Scratch is one static device array of 2 MiB per GPU: sources
- * with more than 262144 (x,y) columns are rejected (INVALID_ARG); the first call
- * on a device resolves the array's address and should precede any stream
- * capture; calls that overlap on the GPU race on the shared array.
+ * with more than 262144 (x,y) columns or more than 2^20 z planes are rejected
+ * (INVALID_ARG).  Every call looks the array's address up in the current
+ * context (nothing is cached across device resets); the first call in a
+ * context should precede any stream capture.  Calls that overlap on the GPU
+ * race on the shared array.
  * Asynchronous on `stream`; errors via isaacb_last_error(NULL). */
 isaacb_status isaacb_minmax_noalloc(
     const float* src,

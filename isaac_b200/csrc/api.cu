@@ -37,103 +37,139 @@ namespace
 {
     const char* kFunctorNames[6] = {"idem", "add", "mul", "length", "pow", "sum"};
 
-    // Per-source body of IsaacVisualization::updateFunctions (lib/isaac.hpp:1084-1186).
+    // The functor-chain grammar of IsaacVisualization::updateFunctions
+    // (lib/isaac.hpp:1084-1186), per source:
+    //
+    //   chain   := functor { '|' functor }     at most kMaxFunctors functors
+    //   functor := name [ '(' args ')' ... ]   whitespace anywhere is ignored;
+    //                                          text after the first ')' is ignored
+    //   args    := number { ',' number }       at most 4; missing ones repeat the last
+    //
+    // Status (the reference's errorCode, the last one raised wins):
+    //    1  more than kMaxFunctors functors (parsing stops)
+    //   -1  '(' without any ')'              (parsing stops)
+    //   -2  unknown functor name             (parsing stops) or an argument that is
+    //       not a number                     (the functor is still taken)
+    //    2  more than four arguments         (the functor is still taken)
+    // Functors that were not taken become idem with zero parameters.
+
+    std::vector<std::string> split(const std::string& text, char sep)
+    {
+        std::vector<std::string> out(1);
+        for(const char c : text)
+        {
+            if(c == sep)
+                out.emplace_back();
+            else
+                out.back().push_back(c);
+        }
+        return out;
+    }
+
+    std::string without_spaces(const std::string& text)
+    {
+        std::string out;
+        for(const char c : text)
+            if(!std::isspace(static_cast<unsigned char>(c)))
+                out.push_back(c);
+        return out;
+    }
+
+    // One number as std::stof reads it (leading numeric prefix, range checked).
+    bool read_number(const std::string& item, float& out)
+    {
+        try
+        {
+            out = std::stof(item);
+            return true;
+        }
+        catch(const std::logic_error&) // invalid_argument and out_of_range
+        {
+            return false;
+        }
+    }
+
+    // The argument list between the parentheses into p[0..3]; returns 0, 2 or -2.
+    int read_arguments(const std::string& list, float* p)
+    {
+        const std::vector<std::string> items = split(list, ',');
+        int status = 0;
+        int taken = 0;
+        for(const std::string& item : items)
+        {
+            if(taken == 4)
+            {
+                status = 2;
+                break;
+            }
+            const bool ok = read_number(item, p[taken]);
+            ++taken;
+            if(!ok)
+            {
+                status = -2;
+                break;
+            }
+        }
+        for(int k = taken; k < 4; ++k)
+            p[k] = p[k - 1];
+        return status;
+    }
+
+    int functor_index(const std::string& name)
+    {
+        for(int f = 0; f < 6; ++f)
+            if(name == kFunctorNames[f])
+                return f;
+        return -1;
+    }
+
     int parse_chain(const std::string& text, int32_t* bytecode, float* params)
     {
-        int errorCode = 0;
-        std::string source = text;
-        size_t pos = 0;
-        bool again = true;
-        int elem = 0;
-        for(int i = 0; i < 4 * kMaxFunctors; ++i)
-            params[i] = 0.0f;
-        while(again && ((pos = source.find('|')) != std::string::npos || ((again = false) == false)))
+        std::fill(bytecode, bytecode + kMaxFunctors, 0);
+        std::fill(params, params + 4 * kMaxFunctors, 0.0f);
+        int status = 0;
+        int taken = 0;
+        for(const std::string& piece : split(text, '|'))
         {
-            if(elem >= kMaxFunctors)
+            if(taken == kMaxFunctors)
             {
-                errorCode = 1;
+                status = 1;
                 break;
             }
-            std::string token = source.substr(0, pos);
-            source.erase(0, pos + 1);
-            token.erase(
-                std::remove_if(token.begin(), token.end(), [](unsigned char c) { return std::isspace(c) != 0; }),
-                token.end());
-            const size_t open = token.find('(');
-            float* p = params + 4 * elem;
+            const std::string functor = without_spaces(piece);
+            float* p = params + 4 * taken;
+            std::string name = functor;
+            const size_t open = functor.find('(');
             if(open != std::string::npos)
             {
-                const size_t close = token.find(')');
+                const size_t close = functor.find(')');
                 if(close == std::string::npos)
                 {
-                    errorCode = -1;
+                    status = -1;
                     break;
                 }
-                if(close - open == 1)
+                // "()" leaves the parameters at zero.  A ')' before the '(' leaves
+                // the list running to the end of the functor.
+                if(close != open + 1)
                 {
-                    p[0] = p[1] = p[2] = p[3] = 0.0f;
+                    const std::string list
+                        = close > open ? functor.substr(open + 1, close - open - 1) : functor.substr(open + 1);
+                    const int s = read_arguments(list, p);
+                    if(s != 0)
+                        status = s;
                 }
-                else
-                {
-                    std::string args = token.substr(open + 1, close - open - 1);
-                    size_t cpos = 0;
-                    bool more = true;
-                    int n = 0;
-                    while(more && ((cpos = args.find(',')) != std::string::npos || ((more = false) == false)))
-                    {
-                        if(n >= 4)
-                        {
-                            errorCode = 2;
-                            break;
-                        }
-                        const std::string one = args.substr(0, cpos);
-                        args.erase(0, cpos + 1);
-                        try
-                        {
-                            p[n] = std::stof(one);
-                        }
-                        catch(const std::invalid_argument&)
-                        {
-                            errorCode = -2;
-                            n++;
-                            break;
-                        }
-                        catch(const std::out_of_range&)
-                        {
-                            errorCode = -2;
-                            n++;
-                            break;
-                        }
-                        n++;
-                    }
-                    for(; n < 4; n++)
-                        p[n] = p[n - 1];
-                }
-                token = token.substr(0, open);
+                name = functor.substr(0, open);
             }
-            else
+            const int op = functor_index(name);
+            if(op < 0)
             {
-                p[0] = p[1] = p[2] = p[3] = 0.0f;
-            }
-            int found = -1;
-            for(int f = 0; f < 6 && found < 0; ++f)
-                if(token == kFunctorNames[f])
-                    found = f;
-            if(found < 0)
-            {
-                errorCode = -2;
+                std::fill(p, p + 4, 0.0f);
+                status = -2;
                 break;
             }
-            bytecode[elem] = found;
-            elem++;
+            bytecode[taken++] = op;
         }
-        for(; elem < kMaxFunctors; elem++)
-        {
-            bytecode[elem] = 0;
-            float* p = params + 4 * elem;
-            p[0] = p[1] = p[2] = p[3] = 0.0f;
-        }
-        return errorCode;
+        return status;
     }
 
     // getHSVA (lib/isaac/isaac_helper.hpp:221-264)
@@ -394,10 +430,6 @@ namespace
         c->lutDirty = false;
         return ISAACB_OK;
     }
-
-
-    // 3-D tensor map over a source seen as (X*featureDim, Y, Z) floats with box
-    // (16*featureDim, 9, 9): the region a merge brick needs, x start on a 16-byte boundary
 
     size_t brick_count(const Geom& g)
     {

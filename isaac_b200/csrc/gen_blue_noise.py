@@ -3,7 +3,7 @@ reference vendors in lib/isaac/isaac_dither_kernel.hpp (dither modes 3 and >= 4;
 generated there with the MomentsInGraphics BlueNoise tool).  The masks decide the
 output bytes of those modes, so they are kept identical.
 
-    python isaac_b200/csrc/gen_blue_noise.py /root/reference/lib/isaac/isaac_dither_kernel.hpp
+    python isaac_b200/csrc/gen_blue_noise.py <reference tree>/lib/isaac/isaac_dither_kernel.hpp
 """
 
 import re

@@ -22,9 +22,12 @@
 //    columns (2 MiB); every GPU that loads this library keeps it until exit.
 //  * A source with more than kNoAllocMaxColumns (x,y) columns is rejected
 //    with ISAACB_INVALID_ARG.
-//  * The first call on a device looks up the array's device address on that
-//    device (cudaGetSymbolAddress with the device current) and caches it; make
-//    that first call before any stream capture on the device.
+//  * Every call looks up the array's device address in the current context
+//    (cudaGetSymbolAddress, a host-side lookup).  Nothing is cached, so an
+//    address never outlives the context it came from (cudaDeviceReset, or a
+//    different driver context made current on the same device).  The first
+//    call in a context may load this module's device code there; make it
+//    before any stream capture.
 //  * Each call overwrites every column entry it later reads, so nothing has to
 //    start at zero; the array keeps the last call's contents.
 //  * All calls share the one array: calls whose kernels overlap on the GPU
@@ -34,7 +37,6 @@
 #include "isaacb_internal.h"
 
 #include <cfloat>
-#include <mutex>
 #include <string>
 
 namespace isaacb
@@ -42,13 +44,11 @@ namespace isaacb
     void set_global_error(const std::string& msg);
 
     constexpr uint32_t kNoAllocMaxColumns = 262144; // 2 floats each: 2 MiB
+    constexpr uint32_t kNoAllocMaxDepth = 1u << 20; // z planes scanned per column
     __device__ __align__(256) float g_columnMinMax[2 * kNoAllocMaxColumns];
 
     namespace
     {
-        constexpr int kMaxDevices = 128;
-        float* g_scratch[kMaxDevices] = {};
-        std::mutex g_scratchMutex;
 
         // per (x,y) column: min/max over z in scan order
         __global__ void __launch_bounds__(256) k_column_minmax(
@@ -127,34 +127,19 @@ namespace isaacb
             }
         }
 
-        isaacb_status scratch_for_current_device(float** out)
+        // The array's address in the context current on this thread.  Looked up
+        // on every call: a cached address would outlive a device reset or point
+        // into another context of the same device.
+        isaacb_status scratch_for_current_context(float** out)
         {
-            int dev = -1;
-            cudaError_t e = cudaGetDevice(&dev);
-            if(e != cudaSuccess)
+            void* p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_columnMinMax);
+            if(e != cudaSuccess || !p)
             {
-                set_global_error(std::string("isaacb_minmax_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
+                set_global_error(std::string("isaacb_minmax_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
                 return ISAACB_CUDA_ERROR;
             }
-            if(dev < 0 || dev >= kMaxDevices)
-            {
-                set_global_error("isaacb_minmax_noalloc: device ordinal out of range");
-                return ISAACB_INVALID_ARG;
-            }
-            std::lock_guard<std::mutex> lock(g_scratchMutex);
-            if(!g_scratch[dev])
-            {
-                void* p = nullptr;
-                e = cudaGetSymbolAddress(&p, g_columnMinMax);
-                if(e != cudaSuccess || !p)
-                {
-                    set_global_error(
-                        std::string("isaacb_minmax_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-                    return ISAACB_CUDA_ERROR;
-                }
-                g_scratch[dev] = static_cast<float*>(p);
-            }
-            *out = g_scratch[dev];
+            *out = static_cast<float*>(p);
             return ISAACB_OK;
         }
     } // namespace
@@ -182,11 +167,18 @@ extern "C" isaacb_status isaacb_minmax_noalloc(
         return ISAACB_INVALID_ARG;
     }
     const uint64_t columns = uint64_t(size[0]) * size[1];
-    if(columns > kNoAllocMaxColumns || size[2] > (1u << 20))
+    if(columns > kNoAllocMaxColumns)
     {
         set_global_error(
             "isaacb_minmax_noalloc: " + std::to_string(columns) + " (x,y) columns exceed the static scratch of "
             + std::to_string(kNoAllocMaxColumns) + " columns");
+        return ISAACB_INVALID_ARG;
+    }
+    if(size[2] > kNoAllocMaxDepth)
+    {
+        set_global_error(
+            "isaacb_minmax_noalloc: depth " + std::to_string(size[2]) + " exceeds the limit of "
+            + std::to_string(kNoAllocMaxDepth) + " z planes");
         return ISAACB_INVALID_ARG;
     }
     Chain ch{};
@@ -202,7 +194,7 @@ extern "C" isaacb_status isaacb_minmax_noalloc(
     for(int k = 0; k < 4 * kMaxFunctors; ++k)
         ch.p[k] = params[k];
     float* scratch = nullptr;
-    const isaacb_status st = scratch_for_current_device(&scratch);
+    const isaacb_status st = scratch_for_current_context(&scratch);
     if(st != ISAACB_OK)
         return st;
     cudaStream_t s = (cudaStream_t) stream;

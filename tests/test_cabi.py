@@ -114,3 +114,17 @@ def test_blend_rejects_bad_arguments_without_gpu():
     assert b"permutation" in lib.isaacb_last_error(None)
     assert lib.isaacb_blend_ordered(ptrs, 0, bad, 4, None, C.c_void_p(64), None) == _lib.INVALID_ARG
     assert lib.isaacb_blend_ordered(ptrs, 65, bad, 4, None, C.c_void_p(64), None) == _lib.INVALID_ARG
+
+
+def test_parser_token_fuzz_matches_oracle():
+    """Strings built from whole tokens reach the argument lists and the functor limit
+    far more often than single characters do."""
+    rng = np.random.default_rng(12)
+    tokens = ["idem", "add", "mul", "length", "pow", "sum", "foo", "(", ")", ",", "|", " ", "2", "-1.5", "1e40",
+              "1e-45", "x", "nan", "0x10", ""]
+    for _ in range(5000):
+        text = "".join(rng.choice(tokens, size=int(rng.integers(0, 14))))
+        e1, b1, p1 = _product_parse(text)
+        e2, b2, p2 = O.parse_chain(text)
+        assert (e1, b1) == (e2, b2), text
+        assert np.array_equal(np.array(p1, dtype=np.float32), np.array(p2, dtype=np.float32), equal_nan=True), text

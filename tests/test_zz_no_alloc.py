@@ -75,6 +75,27 @@ def test_noalloc_matches_context_minmax_on_consecutive_calls():
     assert r3[0].tobytes() == mn_s[0].tobytes() and r3[1].tobytes() == mx_s[0].tobytes()
 
 
+def test_noalloc_signed_zero_in_column_order():
+    """The reference scans each (x,y) column over z, then the columns in order, keeping
+    the earlier value on ties.  With +0 at (column 5, z 0) and -0 at (column 0, z 1) the
+    column order meets -0 first, while a scan in memory order would meet +0 first."""
+    n = 16
+    rng = np.random.default_rng(11)
+    neg = -rng.uniform(0.1, 1.0, (n, n, n)).astype(np.float32)  # (z, y, x), all < 0
+    neg[0, 0, 5] = 0.0
+    neg[1, 0, 0] = -0.0
+    pos = -neg  # all > 0; -0 at (column 5, z 0), +0 at (column 0, z 1)
+    a = torch.from_numpy(neg).cuda()
+    b = torch.from_numpy(pos).cuda()
+    mn, mx = _with_context([a, b], ["idem", "idem"])
+    ra = _noalloc(a, (n, n, n), 1, "idem")
+    rb = _noalloc(b, (n, n, n), 1, "idem")
+    torch.cuda.synchronize()
+    assert ra[1].tobytes() == mx[0].tobytes() == np.float32(-0.0).tobytes()
+    assert rb[0].tobytes() == mn[1].tobytes() == np.float32(0.0).tobytes()
+    assert ra[0].tobytes() == mn[0].tobytes() and rb[1].tobytes() == mx[1].tobytes()
+
+
 def test_noalloc_rejects_sources_beyond_the_static_scratch():
     lib = _lib.load()
     bc, pr = _parse("idem")
@@ -84,3 +105,7 @@ def test_noalloc_rejects_sources_beyond_the_static_scratch():
     st = lib.isaacb_minmax_noalloc(C.c_void_p(dummy.data_ptr()), sz, 1, bc, pr, C.c_void_p(out.data_ptr()), None)
     assert st == _lib.INVALID_ARG
     assert b"static scratch" in lib.isaacb_last_error(None)
+    deep = (C.c_uint32 * 3)(1, 1, (1 << 20) + 1)
+    st = lib.isaacb_minmax_noalloc(C.c_void_p(dummy.data_ptr()), deep, 1, bc, pr, C.c_void_p(out.data_ptr()), None)
+    assert st == _lib.INVALID_ARG
+    assert b"z planes" in lib.isaacb_last_error(None)
