@@ -64,6 +64,13 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-stream", action="store_true", help="skip the streamed-frame measurement")
+    ap.add_argument("--no-learned", action="store_true", help="precision scene: skip the learned-path record")
+    ap.add_argument(
+        "--cpu-check",
+        action="store_true",
+        help="check of the rank plumbing without a GPU: gloo ranks, each step one frame of the CPU oracle on a "
+        "tiny scene; prints the same JSON line (its numbers are not a measurement of the product)",
+    )
     ap.add_argument("--cpu-rows", type=int, default=0, help="image rows of the CPU sample (0 = auto)")
     ap.add_argument("--yaws", default="0,10,20,30,45,60,75,90", help="sweep scene: camera yaws in degrees")
     ap.add_argument("--pitch", type=float, default=0.35, help="sweep scene: camera pitch in radians")
@@ -324,9 +331,25 @@ def cpu_sample(args, o, rows_hint=0):
     return frame_s, samples / max(band_s, 1e-9), rows, merge_s, band_s, samples, threads
 
 
+def cpu_frame(o):
+    """Time one whole frame of the oracle (merge + every row); returns (frame s,
+    samples/s, merge s, render s, samples, threads)."""
+    from oracle import oracle as O
+
+    t0 = time.perf_counter()
+    o.update()
+    t1 = time.perf_counter()
+    o.render()
+    t2 = time.perf_counter()
+    samples = o.samples()[0]
+    return t2 - t0, samples / max(t2 - t1, 1e-9), t1 - t0, t2 - t1, samples, O.num_threads()
+
+
 def run_reference(args):
-    """CPU stand-in for the reference's own CPU backend (see module docstring)."""
-    import numpy as np
+    """CPU stand-in for the reference's own CPU backend (see module docstring): every
+    step is one whole frame (merge + every row) on all host threads.  With
+    ``--cpu-rows R`` a step is instead the merge plus R centre rows, extrapolated to a
+    frame (a labelled fallback for slow hosts)."""
     import torch
 
     rank = int(os.environ.get("RANK", "0"))
@@ -337,17 +360,26 @@ def run_reference(args):
     o = oracle_for(args, sc)
     del sc
     frame_times, sps = [], []
-    rows = args.cpu_rows
+    band = args.cpu_rows > 0
     info = None
+    t_region = 0.0
     for i in range(args.warmup + args.steps):
-        info = cpu_sample(args, o, rows)
+        t0 = time.perf_counter()
+        info = cpu_sample(args, o, args.cpu_rows) if band else cpu_frame(o)
         if i >= args.warmup:
+            t_region += time.perf_counter() - t0
             frame_times.append(info[0])
             sps.append(info[1])
-    frame_s = sorted(frame_times)[len(frame_times) // 2]
+    cores = info[6] if band else info[5]
+    if band:
+        frame_s = sorted(frame_times)[len(frame_times) // 2]
+        sample = (f"full merge of {args.sources}x{args.size}^3 + {info[2]} of {args.height} rows per step, "
+                  "extrapolated to a frame (median)")
+    else:
+        frame_s = t_region / args.steps
+        sample = (f"whole frames: merge of {args.sources}x{args.size}^3 + all {args.height} rows of "
+                  f"{args.width}x{args.height} per step")
     fps = 1.0 / frame_s
-    cores = info[6]
-    sample = f"full merge of {args.sources}x{args.size}^3 + {info[2]} of {args.height} rows per step, extrapolated to a frame"
     line = {
         "metric": metric_name(args),
         "value": fps,
@@ -809,10 +841,15 @@ def run_sweep(args):
 
 
 # ---------------------------------------------------------------------------- learned reconstruction scene
-def run_learned(args, world, rank, local, barrier, max_over_ranks):
+def run_learned(args, world, rank, local, barrier, max_over_ranks, emit=True):
     """Plain full-size frames against the judged learned path on the same
     orbiting camera: every frame a half-size render at twice the step and the
-    U-Net; every 16th frame also the plain render as judge (fallback below 40 dB)."""
+    U-Net; every 16th frame also the plain render as judge (fallback below 40 dB).
+
+    With ``emit`` the line is printed (``--scene learned``); without, only the
+    learned and plain frame rates, quality and phases are measured (no end-to-end,
+    stream or CPU legs) and the line is returned for the headline's ``learned``
+    record."""
     import numpy as np
     import torch
 
@@ -942,7 +979,7 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks):
 
     # end to end through the public API: camera in, frame D2H to pinned host memory
     e2e = None
-    if not args.no_e2e:
+    if emit and not args.no_e2e:
         host = torch.empty((H, W, 4), dtype=torch.uint8).pin_memory()
 
         def e2e_step(k):
@@ -955,22 +992,8 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks):
                "d2h_bytes_per_step": H * W * 4, "ms_per_step": e2e_ms,
                "note": "inputs per step are the two camera matrices; the sources stay one resident timestep"}
 
-    blend_line = None
-    if world == 1 and not args.no_stream:
-        try:
-            blend_line = measure_blend(args)
-        except Exception as ex:  # reported, never required
-            blend_line = {"error": str(ex)}
-
-    stream_line = None
-    if world == 1 and not args.no_stream:
-        try:
-            stream_line = measure_stream(args, viz)
-        except Exception as ex:  # reported, never required
-            stream_line = {"value": None, "unit": "frames/s", "error": str(ex)}
-
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if emit and rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             sc = build_scene(args, "cuda")
             sc.P, sc.MV = cams[0]
@@ -1016,8 +1039,13 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks):
             "clocks": clocks,
             "gpu_launches": None,
         }
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
     net.close()
+    for v in (pr.full, pr.low):
+        v.close()
+    if not emit:
+        return line if rank == 0 else None
     if world > 1:
         import torch.distributed as dist
 
@@ -1177,11 +1205,63 @@ def measure_blend(args, ranks: int = 8) -> dict:
             "note": "ranks emulated on one GPU; the NCCL exchange around it needs several GPUs"}
 
 
+def spawn_ranks(args) -> int | None:
+    """``--gpus N`` started without torchrun: start N ranks on this node (one process
+    per GPU, torch.distributed.run on 127.0.0.1) and return their exit status.  None
+    when this process is already a rank or one rank is asked for."""
+    if args.gpus <= 1 or "WORLD_SIZE" in os.environ or args.impl == "reference":
+        return None
+    import socket
+
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(Path(__file__).resolve())] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def run_cpu_check(args, world, rank, barrier, max_over_ranks):
+    """Rank plumbing without a GPU: each step renders one frame of a 16^3 Gaussian scene
+    with the CPU oracle on every rank; the barrier, the max over ranks and the whole-job
+    value follow the GPU path."""
+    from isaac_b200 import scenes
+    from oracle import oracle as O
+
+    sc, curl = scenes.gaussian_scene(16, 1)
+    o = O.Oracle((32, 32), (16, 16, 16), (16, 16, 16), (1, 1, 1), (0, 0, 0), (1, 1, 1), [1, 3], [1, 1], 2)
+    o.set_source(0, sc.numpy())
+    o.set_source(1, curl.numpy())
+    o.set_functions(1, "length")
+    P, MV = scenes.camera(32, 32, seed=1)
+    o.set_camera(P, MV)
+    for _ in range(args.warmup):
+        o.frame()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.frame()
+    barrier()
+    ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
+    if rank == 0:
+        print(json.dumps({"metric": "cpu rank check: 16^3 gaussian scene at 32x32 on the CPU oracle", "value": world * 1000.0 / ms,
+                          "unit": "frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "f32", "data": "synthetic", "config": {"workload": "cpu rank check", "parallelism": "replicas"}}),
+              flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     apply_scene_defaults(args)
+    spawned = spawn_ranks(args)
+    if spawned is not None:
+        return spawned
     if args.impl == "reference":
         return run_reference_batch(args) if args.scene == "batch" else run_reference(args)
+
+    import datetime
 
     import numpy as np
     import torch
@@ -1190,11 +1270,14 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
+    dev = "cpu" if args.cpu_check else "cuda"
+    if not args.cpu_check:
+        torch.cuda.set_device(local)
     if world > 1:
-        import datetime
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        if args.cpu_check:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+        else:
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
     def barrier():
         if world > 1:
@@ -1203,9 +1286,15 @@ def main():
     def max_over_ranks(v: float) -> float:
         if world == 1:
             return v
-        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        t = torch.tensor([v], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    if args.cpu_check:
+        rc = run_cpu_check(args, world, rank, barrier, max_over_ranks)
+        if world > 1:
+            dist.destroy_process_group()
+        return rc
 
     if args.scene == "sweep":
         return run_sweep(args)
@@ -1357,18 +1446,71 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             o = oracle_for(args, sc)
-            frame_s, sps, rows, merge_s, band_s, cs, threads = cpu_sample(args, o, args.cpu_rows)
+            if args.cpu_rows > 0:
+                frame_s, sps, rows, merge_s, band_s, cs, threads = cpu_sample(args, o, args.cpu_rows)
+                sample = (f"full merge ({merge_s:.2f} s) + {rows} of {args.height} rows ({band_s:.2f} s), "
+                          "extrapolated to a frame")
+            else:
+                # whole frames, one untimed; a handful of seconds each on a multi-core host
+                cpu_frame(o)
+                runs = [cpu_frame(o) for _ in range(3)]
+                frame_s = sum(r[0] for r in runs) / len(runs)
+                sps = sorted(r[1] for r in runs)[1]
+                threads = runs[0][5]
+                sample = (f"3 whole frames (merge {runs[0][2]:.2f} s + all {args.height} rows "
+                          f"{runs[0][3]:.2f} s each), mean")
             cpu = {
                 "value": 1.0 / frame_s,
                 "unit": "frames/s",
                 "cores": threads,
                 "kind": "port",
-                "sample": f"full merge ({merge_s:.2f} s) + {rows} of {args.height} rows ({band_s:.2f} s), extrapolated to a frame",
+                "sample": sample,
                 "gsamples_per_s": sps / 1e9,
             }
             del o
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "frames/s", "cores": None, "kind": "port", "sample": f"failed: {ex}"}
+
+    # the metric's second half: the learned path against the plain renderers, on the
+    # same four 512^3 sources at the same resolution (every rank, like the timed region)
+    learned = None
+    if args.scene == "precision" and args.renderer == "combined" and args.sources == 4 and not args.no_learned:
+        import copy
+
+        la = copy.copy(args)
+        la.scene = "learned"
+        apply_scene_defaults(la)
+        try:
+            ll = run_learned(la, world, rank, local, barrier, max_over_ranks, emit=False)
+        except SystemExit as ex:  # trained weights missing
+            ll = {"error": str(ex)}
+        if rank == 0 and ll is not None and "error" not in ll:
+            draw_ms = sum(v for k, v in acc.items() if k != "update")
+            learned = {
+                "value": ll["value"],
+                "unit": "frames/s",
+                "ms_per_step": ll["ms_per_step"],
+                "frames": ll["steps"],
+                "what": "960x540 step 1.0 per-source BF16 render + U-Net to 1920x1080, the plain 1920x1080 step 0.5 "
+                        "render every 16th frame as judge, fallback below 40 dB; orbiting camera over one resident "
+                        "timestep (no per-frame source update)",
+                "plain_per_source_bf16_fps": ll["plain_fps"],
+                "speedup_vs_plain_per_source_bf16": ll["speedup_vs_plain"],
+                "plain_combined_fps": fps,
+                "speedup_vs_plain_combined": ll["value"] / fps,
+                "plain_combined_draw_fps": world * 1000.0 / draw_ms if draw_ms > 0 else None,
+                "speedup_vs_plain_combined_draw": ll["value"] * draw_ms / (world * 1000.0) if draw_ms > 0 else None,
+                "note": "plain_combined_fps is this line's value (merge + draw every frame); plain_combined_draw_fps "
+                        "leaves the merge out, like the learned and per-source frames",
+                "psnr_db": ll["psnr_db"],
+                "fallback_frames": ll["fallback_frames"],
+                "phases_ms": ll["phases_ms"],
+                "half_render_roofline": {k: ll["roofline"][k] for k in ("achieved", "peak", "unit", "frac", "kernel_ms")},
+                "unet": {k: ll["roofline"]["unet"][k] for k in ("achieved", "peak", "unit", "frac", "kernel_ms")},
+                "clocks": ll["clocks"],
+            }
+        elif rank == 0 and ll is not None:
+            learned = ll
 
     if rank == 0:
         line = {
@@ -1393,6 +1535,7 @@ def main():
             "e2e": e2e,
             "stream": stream_line,
             "sortlast_blend": blend_line,
+            "learned": learned,
             "clocks": clocks,
             "gpu_launches": launches,
         }

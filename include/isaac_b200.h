@@ -306,7 +306,12 @@ isaacb_status isaacb_batch_get_launch_count(isaacb_batch* batch, uint32_t* launc
  * matrix dw[(tap*c_in+ci)][roundup(c_out,16)] (forward gather form).
  *
  * `error_flag` (optional, device int) is set when a bounded wait inside the
- * kernel gave up.  Asynchronous on `stream`; errors via isaacb_last_error(NULL). */
+ * kernel gave up.  Asynchronous on `stream`; errors via isaacb_last_error(NULL).
+ *
+ * `wait_check_us` (forward only; 0 for normal use) checks the failure path: the
+ * kernel, before any copy or MMA, waits that many microseconds on an mbarrier
+ * that nothing arrives at, sets error_flag, releases its TMEM and returns
+ * without writing the output. */
 typedef struct isaacb_conv_args
 {
     const void* x;
@@ -322,6 +327,7 @@ typedef struct isaacb_conv_args
     uint32_t out_h, out_w, c_out;
     uint32_t ksize, stride, pad;
     int32_t transposed, relu, accumulate;
+    uint32_t wait_check_us;
 } isaacb_conv_args;
 
 isaacb_status isaacb_conv_forward(const isaacb_conv_args* args, void* stream);
@@ -365,6 +371,11 @@ isaacb_status isaacb_recon_train_step(
 isaacb_status isaacb_recon_infer(isaacb_recon* recon, const uint8_t* low, uint32_t h, uint32_t w, uint8_t* out, void* stream);
 /* Reads and clears the flag the kernels raise when a bounded wait gave up. */
 isaacb_status isaacb_recon_error(isaacb_recon* recon, int32_t* flag);
+/* Checks the failure path: the first convolution of the next inference or
+ * training step runs the wait check of isaacb_conv_args.wait_check_us with this
+ * budget (microseconds, > 0), so that step raises the flag isaacb_recon_error
+ * reads and its output is not meaningful; later calls run normally. */
+isaacb_status isaacb_recon_arm_wait_check(isaacb_recon* recon, uint32_t budget_us);
 /* The method without the network: bilinear x2 alone (2h x 2w RGBA8). */
 isaacb_status isaacb_upsample_bilinear2(const uint8_t* low, uint32_t h, uint32_t w, uint8_t* out, void* stream);
 /* Adds the sum of squared byte differences of two RGBA8 images to *sum_dev. */

@@ -102,6 +102,7 @@ class ConvArgs(C.Structure):
         ("transposed", C.c_int32),
         ("relu", C.c_int32),
         ("accumulate", C.c_int32),
+        ("wait_check_us", C.c_uint32),
     ]
 
 
@@ -182,6 +183,7 @@ SIGNATURES = {
     "isaacb_recon_train_step": (_i32, [_P, _P, _P, _P, _u32, _u32, _u32, _f, _P, _P, _P]),
     "isaacb_recon_infer": (_i32, [_P, _P, _u32, _u32, _P, _P]),
     "isaacb_recon_error": (_i32, [_P, _i32p]),
+    "isaacb_recon_arm_wait_check": (_i32, [_P, _u32]),
     "isaacb_upsample_bilinear2": (_i32, [_P, _u32, _u32, _P, _P]),
     "isaacb_image_sq_error": (_i32, [_P, _P, C.c_uint64, _P, _P]),
     "isaacb_composite": (_i32, [_i32, _P, _P, _u32, _u32, _u32, _u32, _P, _P]),

@@ -22,6 +22,9 @@ namespace isaacb
         int ks, stride, pad, transposed;
         int relu, accumulate;
         int* errorFlag;
+        // failure-detection check: non-zero = before any copy or MMA, wait this many ns on
+        // an mbarrier that nothing arrives at, raise errorFlag, release TMEM and return
+        unsigned long long waitCheckNs;
     };
 
     // weight gradient (see recon_gemm.cu)

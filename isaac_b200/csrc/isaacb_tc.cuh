@@ -145,10 +145,11 @@ namespace isaacb
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
             return t;
         }
-        // bounded wait for the phase with the given parity to complete: false once about one
-        // second of wall time has passed (checked between probes, whatever each probe's own
-        // suspension limit is) or after 2^26 probes, whichever comes first
-        __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+        // bounded wait for the phase with the given parity to complete: false once `budgetNs`
+        // of wall time (about one second by default) has passed (checked between probes,
+        // whatever each probe's own suspension limit is) or after 2^26 probes, whichever
+        // comes first
+        __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t budgetNs = 1000000000ull)
         {
             if(mbar_try(bar, parity))
                 return true;
@@ -157,7 +158,7 @@ namespace isaacb
             {
                 if(mbar_try(bar, parity))
                     return true;
-                if(global_ns() - t0 > 1000000000ull)
+                if(global_ns() - t0 > budgetNs)
                     return false;
             }
             return false;

@@ -197,11 +197,51 @@ namespace isaacb
         return v;
     }
 
-    // CombinedIsoRenderKernel (lib/isaac/isaac_iso_kernel.hpp:25-128).  The march
-    // samples alpha with the fast path and skips bricks whose alpha bytes are all
-    // <= 127 (a trilinear value there is below the 0.5 threshold); when a hit
-    // follows skipped samples, the previous sample's value is evaluated for the
-    // depth interpolation.  Hit colour and gradient use the exact sampler.
+    // Interpolated alpha byte (0..255 scale) of the iso alpha quads at the reference's
+    // sample position pos = startU + stepVec * i, with the reference's arithmetic: the
+    // position and c = pos - 0.5 rounded as separate operations, floor/fraction of the
+    // unclamped c, CLAMP on the texel indices and the z -> y -> x lerp order of
+    // Sampler/trilinear (lib/isaac/isaac_texture.hpp:140-305, isaac_helper.hpp:124-144).
+    template<bool LINEAR>
+    __device__ __forceinline__ float iso_alpha_exact(const FrameParams& p, const March& m, int i)
+    {
+        const Geom& g = p.g;
+        const float3 pos = march_pos(m, i);
+        if(!LINEAR)
+        {
+            const int ax = iclamp(f2i(pos.x), 0, g.ls[0] - 1) + 1, ay = iclamp(f2i(pos.y), 0, g.ls[1] - 1) + 1,
+                      az = iclamp(f2i(pos.z), 0, g.ls[2] - 1) + 1;
+            const int brick = ((az >> 3) * g.nb[1] + (ay >> 3)) * g.nb[0] + (ax >> 3);
+            const uint32_t slot
+                = uint32_t(brick) * uint32_t(kSlotsPerBrick) + uint32_t((ax & 7) | ((ay & 7) << 3) | ((az & 7) << 6));
+            return byte_f(__ldg(p.isoAQ + slot), 0);
+        }
+        const float cx = pos.x - 0.5f, cy = pos.y - 0.5f, cz = pos.z - 0.5f;
+        const float flx = floorf(cx), fly = floorf(cy), flz = floorf(cz);
+        const float fx = cx - flx, fy = cy - fly, fz = cz - flz;
+        // a footprint whose base lies below -1 or above L-1 reads clamped texels only; the
+        // quad at base -1 (L-1) holds exactly those values
+        const int ax = iclamp(f2i(flx), -1, g.ls[0] - 1) + 1, ay = iclamp(f2i(fly), -1, g.ls[1] - 1) + 1,
+                  az = iclamp(f2i(flz), -1, g.ls[2] - 1) + 1;
+        const int brick = ((az >> 3) * g.nb[1] + (ay >> 3)) * g.nb[0] + (ax >> 3);
+        const uint32_t slot
+            = uint32_t(brick) * uint32_t(kSlotsPerBrick) + uint32_t((ax & 7) | ((ay & 7) << 3) | ((az & 7) << 6));
+        const uint32_t A = __ldg(p.isoAQ + slot), B = __ldg(p.isoAQ + slot + 64);
+        return tri_q(fx, fy, fz, byte_f(A, 0), byte_f(A, 1), byte_f(A, 2), byte_f(A, 3), byte_f(B, 0), byte_f(B, 1),
+                     byte_f(B, 2), byte_f(B, 3));
+    }
+
+    // CombinedIsoRenderKernel (lib/isaac/isaac_iso_kernel.hpp:25-128).  The march reads
+    // alpha with the fast sampler and skips bricks whose alpha bytes are all <= 127 (a
+    // trilinear value there is below the 0.5 threshold).  The fast sampler (fused
+    // position, 8-weight trilinear) differs from the reference's arithmetic by far less
+    // than kIsoMargin bytes, so a sample further than that below the threshold is a
+    // miss for both; any other sample is evaluated again with the reference's arithmetic
+    // (iso_alpha_exact), which decides the hit.  At the hit, the previous sample's value
+    // for the depth interpolation is the exact one too, and value / 255 is a division as
+    // in the reference.  So hit, depth, colour and normal follow the reference's float
+    // operations exactly.
+    constexpr float kIsoMargin = 0.125f; // alpha bytes
     template<bool LINEAR>
     __global__ void __launch_bounds__(256) k_iso(const __grid_constant__ FrameParams p)
     {
@@ -220,13 +260,10 @@ namespace isaacb
                     const March m = march_setup(ray, p.g, p.v.scale, p.step);
                     const float off = LINEAR ? 0.5f : 0.0f;
                     const float c0x = m.startU.x - off, c0y = m.startU.y - off, c0z = m.startU.z - off;
-                    const float inv255 = 1.0f / 255.0f;
                     bool hit = false;
                     float depth = ray.endDepth;
                     float4 hitColor = make_float4(0, 0, 0, 0);
                     float3 hitNormal = f3(0, 0, 0);
-                    float oldValue = 0.0f;
-                    bool oldKnown = true;
                     int curBrick = -1;
                     bool skip = false;
                     int i = m.startSteps;
@@ -242,31 +279,13 @@ namespace isaacb
                             curBrick = brick;
                             skip = __ldg(p.isoFlag + brick) <= 127;
                         }
-                        if(skip)
-                        {
-                            oldKnown = false;
+                        if(skip || a < 127.5f - kIsoMargin)
                             continue;
-                        }
-                        const float value = a * inv255;
-                        if(!oldKnown)
-                        {
-                            int b2;
-                            const float fj = float(i - 1);
-                            oldValue = (i == m.startSteps)
-                                ? 0.0f
-                                : iso_alpha_fast<LINEAR>(
-                                      p,
-                                      fmaf(m.stepVec.x, fj, c0x),
-                                      fmaf(m.stepVec.y, fj, c0y),
-                                      fmaf(m.stepVec.z, fj, c0z),
-                                      b2)
-                                    * inv255;
-                        }
-                        const float tmp = oldValue;
-                        oldValue = value;
-                        oldKnown = true;
+                        const float value = iso_alpha_exact<LINEAR>(p, m, i) / 255.0f;
                         if(value < 0.5f)
                             continue;
+                        // the reference's previous value: 0 before the first sample
+                        const float tmp = i == m.startSteps ? 0.0f : iso_alpha_exact<LINEAR>(p, m, i - 1) / 255.0f;
                         const bool first = ray.isClipped && i == m.startSteps;
                         const float t = fi * m.stepU;
                         if(first)

@@ -484,6 +484,7 @@ struct isaacb_recon
     float* gradHost = nullptr; // device staging for the flat gradient
     unsigned long long* sqErr = nullptr;
     int32_t* errorFlag = nullptr;
+    unsigned long long waitCheckNs = 0; // armed failure-path check for the next convolution
     int step = 0;
     // per-level sizes for the current call
     int lh[4], lw[4];
@@ -569,6 +570,8 @@ namespace
         p.pad = d.pad;
         p.relu = d.relu;
         p.errorFlag = R->errorFlag;
+        p.waitCheckNs = R->waitCheckNs;
+        R->waitCheckNs = 0;
         return launch_conv_gemm(p, s);
     }
 
@@ -930,6 +933,14 @@ extern "C"
         if(cudaMemcpy(flag, R->errorFlag, sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
             return ISAACB_CUDA_ERROR;
         cudaMemset(R->errorFlag, 0, sizeof(int32_t));
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_recon_arm_wait_check(isaacb_recon* R, uint32_t budget_us)
+    {
+        if(!R || budget_us == 0)
+            return fail_r(ISAACB_INVALID_ARG, "isaacb_recon_arm_wait_check: bad arguments");
+        R->waitCheckNs = 1000ull * budget_us;
         return ISAACB_OK;
     }
 

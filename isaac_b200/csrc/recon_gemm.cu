@@ -128,6 +128,18 @@ namespace isaacb
             __syncthreads();
             tc::fence_after_sync();
             const uint32_t tmem = sTmem;
+            if(p.waitCheckNs != 0)
+            {
+                // failure-detection check: sDone has had no arrival, so this bounded wait
+                // runs out; no copy or MMA is in flight when the TMEM is released
+                if(tid == 0 && !tc::mbar_wait(&sDone, 0, p.waitCheckNs) && p.errorFlag)
+                    atomicExch(p.errorFlag, 1);
+                tc::fence_before_sync();
+                __syncthreads();
+                if(tid < 32)
+                    tc::tmem_dealloc(tmem, cols);
+                return;
+            }
 
             const int P = p.B * p.Ho * p.Wo;
             const int nTiles = (P + kTileM - 1) / kTileM;
@@ -412,6 +424,18 @@ namespace isaacb
             __syncthreads();
             tc::fence_after_sync();
             const uint32_t tmem = sTmem;
+            if(p.waitCheckNs != 0)
+            {
+                // failure-detection check: sDrain has had no arrival, so this bounded wait
+                // runs out; no copy or MMA is in flight when the TMEM is released
+                if(tid == 0 && !tc::mbar_wait(&sDrain, 0, p.waitCheckNs) && p.errorFlag)
+                    atomicExch(p.errorFlag, 1);
+                tc::fence_before_sync();
+                __syncthreads();
+                if(warp == 0)
+                    tc::tmem_dealloc(tmem, cols);
+                return;
+            }
             const int tilesPerRow = (p.Wo + kTileM - 1) / kTileM;
             const int nTiles = p.B * p.Ho * tilesPerRow;
 
@@ -922,6 +946,7 @@ extern "C"
         p.relu = a->relu ? 1 : 0;
         p.accumulate = a->accumulate ? 1 : 0;
         p.errorFlag = a->error_flag;
+        p.waitCheckNs = 1000ull * a->wait_check_us;
         if(!launch_conv_gemm(p, (cudaStream_t) stream))
         {
             set_global_error("isaacb_conv_forward: weights do not fit in shared memory");

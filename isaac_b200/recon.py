@@ -117,9 +117,15 @@ class Reconstructor:
         return out
 
     def error_flag(self) -> int:
+        """Reads and clears the flag a bounded wait in the kernels raises when it gives up."""
         f = C.c_int32()
         check(self.lib.isaacb_recon_error(self.handle, C.byref(f)))
         return int(f.value)
+
+    def arm_wait_check(self, budget_us: int):
+        """The next inference or training step's first convolution checks the failure path:
+        a wait of ``budget_us`` on a barrier nothing arrives at, which raises the flag."""
+        check(self.lib.isaacb_recon_arm_wait_check(self.handle, int(budget_us)))
 
 
 def bilinear2(low, out=None):

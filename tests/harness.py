@@ -39,6 +39,8 @@ class Scene:
     storage: list = field(default_factory=list)  # per volume source: 0 f32, 1 bf16, 2 f16
     scale: tuple = (1.0, 1.0, 1.0)
     transfer_size: int = 1024
+    P: object = None  # explicit projection and modelview; None: scenes.camera(camera_seed)
+    MV: object = None
 
 
 def gaussian_pair(n=32, fb=(64, 48), seed=1, **kw) -> Scene:
@@ -116,7 +118,10 @@ def build_gpu(s: Scene):
 
 def _apply_settings(s: Scene, t, oracle: bool):
     n = len(s.volumes) + len(s.particles)
-    P, MV = scenes.camera(s.fb[0], s.fb[1], seed=s.camera_seed, distance=s.camera_distance)
+    if s.P is not None:
+        P, MV = s.P, s.MV
+    else:
+        P, MV = scenes.camera(s.fb[0], s.fb[1], seed=s.camera_seed, distance=s.camera_distance)
     if oracle:
         for i in range(n):
             if i < len(s.functions) and s.functions[i]:
@@ -161,6 +166,41 @@ def _apply_settings(s: Scene, t, oracle: bool):
         t.setDitherMode(s.dither_mode)
         t.setBackgroundColor(s.background)
         t.setCamera(P, MV)
+
+
+def config_scene(scene: str, renderer: str = "combined", dtype: str = "f32") -> Scene:
+    """The benchmark's own scene of one configuration (``bench.build_scene``), generated
+    on the GPU from the same seeds, as a harness Scene with float32 host arrays.
+
+    ``scene``: "gaussian" (128^3 scalar + curl -> 512x512), "full" (3 x 256^3 sources,
+    1M particles, iso, 2 clipping planes, SSAO -> 1920x1080) or "precision" (4 x 512^3
+    spectral sources -> 1920x1080)."""
+    import argparse
+
+    import bench
+
+    args = argparse.Namespace(scene=scene, size=512, sources=4, width=1920, height=1080, renderer=renderer,
+                              dtype=dtype)
+    bench.apply_scene_defaults(args)
+    sc = bench.build_scene(args, "cuda")
+    n = args.size
+    s = Scene(n=(n, n, n), fb=(args.width, args.height))
+    s.volumes = [(t.cpu().numpy(), True) for t, _ in sc.volumes]
+    if sc.particles is not None:
+        off, pos, attr, radius, cells = sc.particles
+        s.particles = [(off.cpu().numpy(), pos.cpu().numpy(), attr.cpu().numpy(), None, radius)]
+        s.particle_cells = tuple(cells)
+    s.functions = list(sc.functions)
+    s.transfer = list(sc.transfer)
+    s.iso = list(sc.iso)
+    s.clips = list(sc.clips)
+    s.ao = (bool(sc.ao), 0.5, False)
+    s.P, s.MV = sc.P, sc.MV
+    if renderer == "per_source":
+        s.optimized = False
+        s.storage = [{"f32": 0, "bf16": 1, "f16": 2}[dtype]] * len(s.volumes)
+    del sc
+    return s
 
 
 def image_diff(a: np.ndarray, b: np.ndarray) -> dict:
