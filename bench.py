@@ -53,6 +53,8 @@ def parse_args():
         "sweep: ray-march speed of both renderers against the view angle (a diagnostic, one JSON line per yaw)",
     )
     ap.add_argument("--timesteps", type=int, default=4, help="batch scene: timesteps (contexts)")
+    ap.add_argument("--autotune-step", action="store_true",
+                    help="learned scene: also pick the half-size step by measurement under the 40 dB judge")
     ap.add_argument("--shift", type=float, default=0.05, help="batch scene: advection per timestep, fraction of the box")
     ap.add_argument("--no-autotune", action="store_true", help="batch scene: keep the default launch shape")
     ap.add_argument("--size", type=int, default=512, help="edge of each cubic source volume")
@@ -61,10 +63,19 @@ def parse_args():
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--renderer", default="combined", choices=["combined", "per_source"])
     ap.add_argument("--dtype", default="f32", choices=["f32", "bf16", "f16"], help="per-source renderer bricks")
+    ap.add_argument(
+        "--learned-renderer",
+        default="per_source",
+        choices=["per_source", "combined"],
+        help="learned scene: the renderer of the half-size and judge frames (per_source: BF16 bricks)",
+    )
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-stream", action="store_true", help="skip the streamed-frame measurement")
     ap.add_argument("--no-learned", action="store_true", help="precision scene: skip the learned-path record")
+    ap.add_argument("--ao-samples", type=int, default=0,
+                    help="full scene: SSAO taps on a spiral (0 = the reference's 7x7 grid at 10 px)")
+    ap.add_argument("--ao-radius", type=float, default=8.0, help="full scene: radius of the SSAO spiral in pixels")
     ap.add_argument(
         "--cpu-check",
         action="store_true",
@@ -173,7 +184,8 @@ def apply_scene_defaults(args):
     if args.scene == "gaussian":
         args.size, args.width, args.height, args.sources = 128, 512, 512, 2
     elif args.scene == "learned":
-        args.renderer, args.dtype, args.sources = "per_source", "bf16", 4
+        args.renderer, args.sources = args.learned_renderer, 4
+        args.dtype = "bf16" if args.renderer == "per_source" else "f32"
     elif args.scene == "full":
         args.size, args.sources = 256, 3
         args.width = args.width or 1920
@@ -260,6 +272,8 @@ def make_viz(args, sc):
     for c in sc.clips:
         viz.addClipping(*c)
     viz.setAmbientOcclusion(sc.ao, 0.5)
+    if sc.ao and args.ao_samples:
+        viz.setAmbientOcclusionPattern(args.ao_samples, args.ao_radius)
     viz.setInterpolation(True)
     viz.setStep(0.5)
     viz.setCamera(sc.P, sc.MV)
@@ -406,8 +420,9 @@ def run_reference(args):
 
 def metric_name(args):
     if args.scene == "learned":
+        what = "BF16 bricks" if args.renderer == "per_source" else "f32 sources, combined renderer"
         return (
-            f"fps @{args.width}x{args.height}, {args.sources}x{args.size}^3 BF16 bricks: learned path "
+            f"fps @{args.width}x{args.height}, {args.sources}x{args.size}^3 {what}: learned path "
             f"({args.width // 2}x{args.height // 2} step 1.0 + U-Net, judged every 16th frame) vs plain step 0.5"
         )
     if args.scene == "batch":
@@ -419,7 +434,9 @@ def metric_name(args):
         return f"fps @{args.width}x{args.height}, {args.sources}x{args.size}^3 f32 sources, plain GPU ray-caster"
     if args.scene == "gaussian":
         return "fps @512x512, 128^3 scalar + curl sources, plain GPU ray-caster"
-    return f"fps @{args.width}x{args.height}, 3x256^3 sources + 1M particles, iso, 2 clip planes, SSAO"
+    ao = (f"SSAO {args.ao_samples} samples within {args.ao_radius:g} px" if args.ao_samples
+          else "SSAO (7x7 grid at 10 px)")
+    return f"fps @{args.width}x{args.height}, 3x256^3 sources + 1M particles, iso, 2 clip planes, {ao}"
 
 
 def config_of(args):
@@ -431,16 +448,18 @@ def config_of(args):
         f"{args.size}^3 float32 spectral sources, 16 views of uneven resolution",
     }
     if args.scene == "learned":
+        how = ("as BF16 bricks (per-source renderer)" if args.renderer == "per_source"
+               else "merged into the RGBA8 texture (combined renderer)")
         return {
-            "workload": f"learned reconstruction: {args.sources} x {args.size}^3 spectral sources as BF16 bricks "
-            f"(per-source renderer), {args.width // 2}x{args.height // 2} at step 1.0 + 4-level U-Net -> "
+            "workload": f"learned reconstruction: {args.sources} x {args.size}^3 spectral sources {how}, "
+            f"{args.width // 2}x{args.height // 2} at step 1.0 + 4-level U-Net -> "
             f"{args.width}x{args.height}; plain {args.width}x{args.height} step 0.5 every 16th frame as judge, "
             "fallback below 40 dB; orbiting camera over one timestep",
             "scene": "learned",
             "sources": args.sources,
             "volume": args.size,
             "framebuffer": [args.width, args.height],
-            "renderer": "per_source (bf16 bricks)",
+            "renderer": "per_source (bf16 bricks)" if args.renderer == "per_source" else "combined",
             "parallelism": "replicas",
             "l2": "inputs larger than L2 (sources and bricks are > 126 MB)",
         }
@@ -857,7 +876,7 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks, emit=True):
     from isaac_b200.recon_train import PairRenderer
 
     W, H = args.width, args.height
-    pr = PairRenderer(args.size, W, H)
+    pr = PairRenderer(args.size, W, H, renderer=args.renderer)
     pr.set_timestep(0)
     tfs = [scenes.transfer_4point(0.7 * i) for i in range(args.sources)]
     n_frames = max(16, (args.steps + 15) // 16 * 16)
@@ -866,9 +885,10 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks, emit=True):
     pr.full.update()
     pr.low.update()
     net = recon.Reconstructor(1, H // 2, W // 2, seed=1)
-    if not recon.WEIGHTS.exists():
-        raise SystemExit(f"trained weights missing: {recon.WEIGHTS} (python -m isaac_b200.recon_train)")
-    net.load()
+    wpath = recon.weights_for(args.renderer)
+    if not wpath.exists():
+        raise SystemExit(f"trained weights missing: {wpath} (python -m isaac_b200.recon_train --renderer {args.renderer})")
+    net.load(wpath)
     jr = recon.JudgedRenderer(pr.full, pr.low, net, judge_every=16, threshold=40.0)
     full = torch.empty((H, W, 4), dtype=torch.uint8, device="cuda")
 
@@ -929,6 +949,19 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks, emit=True):
     learned_ms = timed(learned)
     clocks = clk.stop()
     judged = [p for _, p in jr.judged[-(n_frames // 16):]]
+    fallback_frames = jr.fallback_frames
+
+    # the half-size step picked by the autotuner (time under the judge's PSNR constraint),
+    # then the learned frames timed again with it; the step goes back to 1.0 afterwards
+    step_tune = None
+    if args.autotune_step:
+        step_tune = jr.autotune_step(cams[::4][:8])
+        jr.count, jr.judged, jr.fallback, jr.fallback_frames = 0, [], False, 0
+        step_tune["value"] = world * 1000.0 / timed(learned)
+        step_tune["unit"] = "frames/s"
+        step_tune["fallback_frames"] = jr.fallback_frames
+        pr.low.setStep(1.0)
+        jr.count, jr.judged, jr.fallback, jr.fallback_frames = 0, [], False, 0
 
     # phases of one learned frame (events on the launch stream)
     # (over the same orbit of cameras as the timed frames: the samples per frame follow
@@ -950,18 +983,21 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks, emit=True):
     peaks = measured_peaks_all()
     # the dominant kernel of a learned frame is the half-size per-source march (64 B per
     # sample with 4 BF16 sources); the U-Net's tensor-core figures ride along
-    half_gbs = half_samples * 64 / (half_ms * 1e-3) / 1e9 if half_ms > 0 else None
+    bps = 64 if args.renderer == "per_source" else 32
+    half_gbs = half_samples * bps / (half_ms * 1e-3) / 1e9 if half_ms > 0 else None
     unet_tflops = flops / (net_ms * 1e-3) / 1e12 if net_ms > 0 else None
     roofline = {
         "bound": "hbm",
-        "kernel": "k_shade_volume_per_source_n (half-size per-source BF16 march, 960x540, step 1.0)",
+        "kernel": ("k_shade_volume_per_source_n (half-size per-source BF16 march, 960x540, step 1.0)"
+                   if args.renderer == "per_source" else "k_shade_volume (half-size combined march, 960x540, step 1.0)"),
         "achieved": half_gbs,
         "peak": peaks["hbm_gbs"],
         "peak_kind": "measured",
         "unit": "GB/s",
         "frac": half_gbs / peaks["hbm_gbs"] if half_gbs else None,
-        "traffic": recorded_traffic(f"learned_half_{args.size}_{W // 2}x{H // 2}"),
-        "algorithmic_bytes_per_sample": 64,
+        "traffic": recorded_traffic(f"learned_half_{args.size}_{W // 2}x{H // 2}"
+                                    + ("" if args.renderer == "per_source" else "_combined")),
+        "algorithmic_bytes_per_sample": bps,
         "samples_per_launch": half_samples,
         "kernel_ms": half_ms,
         "unet": {
@@ -1000,7 +1036,7 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks, emit=True):
             o = oracle_for(args, sc)
             frame_s, sps, rows, merge_s, band_s, cs, threads = cpu_sample(args, o, args.cpu_rows)
             cpu = {"value": 1.0 / frame_s, "unit": "frames/s", "cores": threads, "kind": "port",
-                   "sample": f"plain per-source BF16 path: brick update ({merge_s:.2f} s) + {rows} of {H} rows "
+                   "sample": f"plain {args.renderer} path: update ({merge_s:.2f} s) + {rows} of {H} rows "
                    f"({band_s:.2f} s), extrapolated to a frame"}
             del o, sc
         except Exception as ex:  # the baseline is reported, never required
@@ -1020,7 +1056,7 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks, emit=True):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "bf16",
+            "dtype": "bf16" if args.renderer == "per_source" else "f32",
             "data": "synthetic (seeded spectral fields); network trained on renderer-made pairs",
             "config": config_of(args),
             "plain_fps": plain_fps,
@@ -1030,7 +1066,8 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks, emit=True):
                         "bilinear_mean": float(np.mean(bil_psnr)), "bilinear_min": float(np.min(bil_psnr)),
                         "frames_at_or_above_40db": float(np.mean(np.array(rec_psnr) >= 40.0)),
                         "judged_in_timed_run": judged},
-            "fallback_frames": jr.fallback_frames,
+            "fallback_frames": fallback_frames,
+            "step_autotune": step_tune,
             "samples_per_frame": {"full": full_samples, "half": half_samples},
             "phases_ms": {"half_render": half_ms, "unet": net_ms},
             "roofline": roofline,
@@ -1472,45 +1509,50 @@ def main():
             cpu = {"value": None, "unit": "frames/s", "cores": None, "kind": "port", "sample": f"failed: {ex}"}
 
     # the metric's second half: the learned path against the plain renderers, on the
-    # same four 512^3 sources at the same resolution (every rank, like the timed region)
-    learned = None
+    # same four 512^3 sources at the same resolution (every rank, like the timed region):
+    # the half-size and judge frames drawn by the per-source renderer from BF16 bricks
+    # (the learned configuration) and by the combined renderer (this line's renderer)
+    learned = {}
     if args.scene == "precision" and args.renderer == "combined" and args.sources == 4 and not args.no_learned:
         import copy
 
-        la = copy.copy(args)
-        la.scene = "learned"
-        apply_scene_defaults(la)
-        try:
-            ll = run_learned(la, world, rank, local, barrier, max_over_ranks, emit=False)
-        except SystemExit as ex:  # trained weights missing
-            ll = {"error": str(ex)}
-        if rank == 0 and ll is not None and "error" not in ll:
-            draw_ms = sum(v for k, v in acc.items() if k != "update")
-            learned = {
+        draw_ms = sum(v for k, v in acc.items() if k != "update")
+        for lr_name in ("per_source", "combined"):
+            la = copy.copy(args)
+            la.scene, la.learned_renderer = "learned", lr_name
+            apply_scene_defaults(la)
+            try:
+                ll = run_learned(la, world, rank, local, barrier, max_over_ranks, emit=False)
+            except SystemExit as ex:  # trained weights missing
+                ll = {"error": str(ex)}
+            if rank != 0 or ll is None:
+                continue
+            if "error" in ll:
+                learned[lr_name] = ll
+                continue
+            learned[lr_name] = {
                 "value": ll["value"],
                 "unit": "frames/s",
                 "ms_per_step": ll["ms_per_step"],
                 "frames": ll["steps"],
-                "what": "960x540 step 1.0 per-source BF16 render + U-Net to 1920x1080, the plain 1920x1080 step 0.5 "
+                "what": f"960x540 step 1.0 {lr_name} render + U-Net to 1920x1080, the plain {lr_name} 1920x1080 step 0.5 "
                         "render every 16th frame as judge, fallback below 40 dB; orbiting camera over one resident "
                         "timestep (no per-frame source update)",
-                "plain_per_source_bf16_fps": ll["plain_fps"],
-                "speedup_vs_plain_per_source_bf16": ll["speedup_vs_plain"],
+                "plain_same_renderer_fps": ll["plain_fps"],
+                "speedup_vs_plain_same_renderer": ll["speedup_vs_plain"],
                 "plain_combined_fps": fps,
                 "speedup_vs_plain_combined": ll["value"] / fps,
                 "plain_combined_draw_fps": world * 1000.0 / draw_ms if draw_ms > 0 else None,
                 "speedup_vs_plain_combined_draw": ll["value"] * draw_ms / (world * 1000.0) if draw_ms > 0 else None,
                 "note": "plain_combined_fps is this line's value (merge + draw every frame); plain_combined_draw_fps "
-                        "leaves the merge out, like the learned and per-source frames",
+                        "leaves the merge out, like the learned and plain_same_renderer frames",
                 "psnr_db": ll["psnr_db"],
                 "fallback_frames": ll["fallback_frames"],
                 "phases_ms": ll["phases_ms"],
-                "half_render_roofline": {k: ll["roofline"][k] for k in ("achieved", "peak", "unit", "frac", "kernel_ms")},
+                "half_render_roofline": {k: ll["roofline"][k] for k in ("kernel", "achieved", "peak", "unit", "frac", "kernel_ms")},
                 "unet": {k: ll["roofline"]["unet"][k] for k in ("achieved", "peak", "unit", "frac", "kernel_ms")},
                 "clocks": ll["clocks"],
             }
-        elif rank == 0 and ll is not None:
-            learned = ll
 
     if rank == 0:
         line = {
@@ -1535,7 +1577,7 @@ def main():
             "e2e": e2e,
             "stream": stream_line,
             "sortlast_blend": blend_line,
-            "learned": learned,
+            "learned": learned or None,
             "clocks": clocks,
             "gpu_launches": launches,
         }

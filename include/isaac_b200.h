@@ -143,6 +143,15 @@ isaacb_status isaacb_set_step(isaacb_ctx* ctx, float step);
 isaacb_status isaacb_set_interpolation(isaacb_ctx* ctx, int32_t enabled);
 isaacb_status isaacb_set_renderer(isaacb_ctx* ctx, int32_t renderer);
 isaacb_status isaacb_set_ao(isaacb_ctx* ctx, int32_t enabled, float weight, int32_t filter);
+/* SSAO tap pattern (no reference counterpart; the reference always tests the 7x7
+ * grid of taps 10 px apart, lib/isaac/isaac_ssao_kernel.hpp:38-184).  samples = 0
+ * restores that grid.  1..32 samples on a golden-angle spiral filling a disc of
+ * `radius` pixels (1..127), rounded to whole pixels; a tap occludes when its depth
+ * is below the pixel's, and ao = clamp(occluded / (samples * 42/48), 0, 1), the
+ * grid's normalisation per tap.  isaacb_get_ao_pattern returns the count and the
+ * (x, y) offsets (2 * samples ints). */
+isaacb_status isaacb_set_ao_pattern(isaacb_ctx* ctx, uint32_t samples, float radius);
+isaacb_status isaacb_get_ao_pattern(isaacb_ctx* ctx, uint32_t* samples, int32_t* offsets);
 isaacb_status isaacb_set_render_mode(isaacb_ctx* ctx, int32_t mode);
 isaacb_status isaacb_set_dither_mode(isaacb_ctx* ctx, int32_t mode);
 /* Storage type of the per-source renderer's bricks (no reference counterpart;

@@ -9,12 +9,16 @@
  * Differences from the reference class:
  *  - no alpaka host/accelerator/stream objects, no server URL/port, no MPI;
  *    an optional cudaStream_t replaces the alpaka stream;
- *  - the field-source list must be empty (advection is not part of this path);
+ *  - field sources (FieldSourceList, float3 vector fields that are advected) become
+ *    the last volume sources of the context, after every plain volume source, and
+ *    are flagged with isaacb_set_field_source -- the merge order of the reference;
+ *    advection runs with the combined renderer;
  *  - glm vector types are replaced by isaacb::float_dim<N> and isaacb::int3v,
  *    which have the same component names (x, y, z, w) and operator[];
  *  - a volume source may expose `const float* linearData() const` (x-fastest,
- *    featureDim floats per voxel); then its memory is read in place instead of
- *    gathered through operator[] every frame.
+ *    featureDim floats per voxel, guardSize cells on every side); then its memory
+ *    is read in place instead of gathered through operator[] every frame.  A
+ *    gathered source is copied without its guard cells.
  */
 #ifndef ISAAC_B200_HPP
 #define ISAAC_B200_HPP
@@ -236,8 +240,9 @@ namespace isaacb
         class Controller = DefaultController>
     class IsaacVisualization
     {
-        static_assert(std::tuple_size<FieldSourceList>::value == 0, "field sources (advection) are not supported");
-        static constexpr int nVol = int(std::tuple_size<VolumeSourceList>::value);
+        static constexpr int nPlain = int(std::tuple_size<VolumeSourceList>::value);
+        static constexpr int nField = int(std::tuple_size<FieldSourceList>::value);
+        static constexpr int nVol = nPlain + nField; // field sources follow the plain ones
         static constexpr int nPart = int(std::tuple_size<ParticleList>::value);
         static constexpr int nTotal = nVol + nPart;
 
@@ -265,10 +270,10 @@ namespace isaacb
             , local_(localSize)
             , localParticle_(localParticleSize)
             , volumeSources_(volumeSources)
+            , fieldSources_(fieldSources)
             , particleSources_(particleSources)
             , stream_(stream)
         {
-            (void) fieldSources;
             isaacb_desc d{};
             d.framebuffer[0] = fb_[0];
             d.framebuffer[1] = fb_[1];
@@ -287,7 +292,15 @@ namespace isaacb
                 using S = std::decay_t<decltype(s)>;
                 d.feature_dim[I] = uint32_t(S::featureDim);
                 d.persistent[I] = S::persistent ? 1u : 0u;
-                d.guard_size[I] = uint32_t(S::guardSize);
+                // memory read in place keeps its guard cells; a gathered copy is the interior
+                d.guard_size[I] = detail::has_linear_data<S>::value ? uint32_t(S::guardSize) : 0u;
+            });
+            detail::for_each(fieldSources_, [&](auto I, auto& s) {
+                using S = std::decay_t<decltype(s)>;
+                static_assert(S::featureDim == 3, "a field source is a float3 vector field");
+                d.feature_dim[nPlain + I] = 3u;
+                d.persistent[nPlain + I] = S::persistent ? 1u : 0u;
+                d.guard_size[nPlain + I] = detail::has_linear_data<S>::value ? uint32_t(S::guardSize) : 0u;
             });
             detail::for_each(particleSources_, [&](auto I, auto& s) {
                 using S = std::decay_t<decltype(s)>;
@@ -295,6 +308,8 @@ namespace isaacb
                 d.persistent[nVol + I] = 1u;
             });
             detail::check(isaacb_create(&d, &ctx_), nullptr, "isaacb_create");
+            for(int i = nPlain; i < nVol; ++i)
+                detail::check(isaacb_set_field_source(ctx_, uint32_t(i), 1), ctx_, "field source");
             for(int i = 0; i < nTotal; ++i)
                 functions[i].source = "idem";
             staging_.fill(nullptr);
@@ -365,6 +380,15 @@ namespace isaacb
                 "render optimization");
         }
         void setAmbientOcclusion(bool enabled, float weight) { detail::check(isaacb_set_ao(ctx_, enabled, weight, 0), ctx_, "ao"); }
+        // "advection step", "advection weight", "advection seeding period", "advection
+        // seeding duration", "seed points" (lib/isaac.hpp:1636-1662)
+        void setAdvection(float stepFactor, float historyWeight, int seedingPeriod, int seedingDuration, int seedPoints)
+        {
+            detail::check(
+                isaacb_set_advection(ctx_, stepFactor, historyWeight, seedingPeriod, seedingDuration, seedPoints),
+                ctx_,
+                "advection");
+        }
         void setRenderMode(int m) { detail::check(isaacb_set_render_mode(ctx_, m), ctx_, "render mode"); }
         void setDitherMode(int m) { detail::check(isaacb_set_dither_mode(ctx_, m), ctx_, "dither mode"); }
         void setBackgroundColor(std::array<float, 4> rgba)
@@ -467,36 +491,36 @@ namespace isaacb
         // source update hooks (lib/isaac.hpp:249-290), gathers, particle lists, camera
         void prepare(void* pointer)
         {
-            const size_t nvox = size_t(local_[0]) * local_[1] * local_[2];
-            detail::for_each(volumeSources_, [&](auto I, auto& s) {
-                using S = std::decay_t<decltype(s)>;
-                s.update(true, pointer);
-                if constexpr(detail::has_linear_data<S>::value)
-                {
-                    detail::check(isaacb_set_source(ctx_, I, s.linearData()), ctx_, "set source");
-                }
-                else
-                {
-                    if(!staging_[I])
-                        detail::cuda(
-                            cudaMalloc(&staging_[I], nvox * S::featureDim * sizeof(float)),
-                            "staging allocation");
-                    detail::gather_volume<S><<<148 * 8, 256, 0, stream_>>>(
-                        s,
-                        staging_[I],
-                        int(local_[0]),
-                        int(local_[1]),
-                        int(local_[2]));
-                    detail::cuda(cudaGetLastError(), "gather launch");
-                    detail::check(isaacb_set_source(ctx_, I, staging_[I]), ctx_, "set source");
-                }
-            });
+            detail::for_each(volumeSources_, [&](auto I, auto& s) { prepareVolume(int(I), s, pointer); });
+            detail::for_each(fieldSources_, [&](auto I, auto& s) { prepareVolume(nPlain + int(I), s, pointer); });
             detail::for_each(particleSources_, [&](auto I, auto& s) {
                 using S = std::decay_t<decltype(s)>;
                 s.update(true, pointer);
                 gatherParticles<S>(I, s);
             });
             detail::check(isaacb_set_camera(ctx_, projection.data(), modelview.data()), ctx_, "camera");
+        }
+
+        // the source's update hook, then its memory in place (linearData) or gathered
+        // through its device operator[] into a staging buffer
+        template<class S>
+        void prepareVolume(int I, S& s, void* pointer)
+        {
+            s.update(true, pointer);
+            if constexpr(detail::has_linear_data<S>::value)
+            {
+                detail::check(isaacb_set_source(ctx_, uint32_t(I), s.linearData()), ctx_, "set source");
+            }
+            else
+            {
+                const size_t nvox = size_t(local_[0]) * local_[1] * local_[2];
+                if(!staging_[I])
+                    detail::cuda(cudaMalloc(&staging_[I], nvox * S::featureDim * sizeof(float)), "staging allocation");
+                detail::gather_volume<S>
+                    <<<148 * 8, 256, 0, stream_>>>(s, staging_[I], int(local_[0]), int(local_[1]), int(local_[2]));
+                detail::cuda(cudaGetLastError(), "gather launch");
+                detail::check(isaacb_set_source(ctx_, uint32_t(I), staging_[I]), ctx_, "set source");
+            }
         }
 
         template<class S>
@@ -540,6 +564,7 @@ namespace isaacb
         std::array<uint32_t, 2> fb_;
         std::array<uint32_t, 3> local_, localParticle_;
         VolumeSourceList& volumeSources_;
+        FieldSourceList& fieldSources_;
         ParticleList& particleSources_;
         cudaStream_t stream_;
         isaacb_ctx* ctx_ = nullptr;

@@ -140,6 +140,8 @@ SIGNATURES = {
     "isaacb_set_interpolation": (_i32, [_P, _i32]),
     "isaacb_set_renderer": (_i32, [_P, _i32]),
     "isaacb_set_ao": (_i32, [_P, _i32, _f, _i32]),
+    "isaacb_set_ao_pattern": (_i32, [_P, _u32, _f]),
+    "isaacb_get_ao_pattern": (_i32, [_P, _P, _P]),
     "isaacb_set_render_mode": (_i32, [_P, _i32]),
     "isaacb_set_dither_mode": (_i32, [_P, _i32]),
     "isaacb_set_storage": (_i32, [_P, _u32, _i32]),

@@ -299,12 +299,15 @@ struct isaacb_ctx
     int aoEnabled = 0;
     float aoWeight = 0.5f;
     int aoFilter = 0;
+    int aoSamples = 0; // 0: the reference's 7x7 grid
+    int8_t aoOffsets[2 * kMaxAoSamples] = {};
     int renderMode = 0;
     int ditherMode = 1;
     float bg[4] = {0, 0, 0, 0};
     double proj[16]{}, mv[16]{};
     bool cameraSet = false;
     const float* src[kMaxSources]{};
+    float* compact[kMaxSources]{}; // compact interior copies of guarded sources
     ParticleSrc part[kMaxSources]{};
     bool partSet[kMaxSources]{};
     bool counting = false;
@@ -605,6 +608,33 @@ namespace
         return ISAACB_OK;
     }
 
+    // A source with guard cells is read through a compact copy of its interior: the
+    // combined renderer and min/max read only the interior (MergeToCombinedTextureKernel
+    // and MinMaxKernel iterate over the local size, lib/isaac/isaac_common_kernel.hpp:
+    // 716-719, lib/isaac/isaac_min_max_kernel.hpp:35-38), which is what every kernel
+    // here indexes.
+    const float* source_data(const isaacb_ctx* c, int s)
+    {
+        return c->desc.guard_size[s] != 0 ? c->compact[s] : c->src[s];
+    }
+    isaacb_status compact_guarded(isaacb_ctx* c, cudaStream_t st)
+    {
+        for(int s = 0; s < c->nVol; ++s)
+        {
+            const int g = int(c->desc.guard_size[s]);
+            if(g == 0 || !c->src[s])
+                continue;
+            const int fd = int(c->desc.feature_dim[s]);
+            if(!c->compact[s])
+                ISAACB_CUDA(c, cudaMalloc(&c->compact[s], size_t(c->g.ls[0]) * c->g.ls[1] * c->g.ls[2] * fd * sizeof(float)),
+                            "compact source allocation");
+            launch_compact_guarded(c->src[s], c->compact[s], c->g.ls[0], c->g.ls[1], c->g.ls[2], g, fd, st);
+            ISAACB_CUDA(c, cudaGetLastError(), "compact guarded source");
+            c->updateLaunches++;
+        }
+        return ISAACB_OK;
+    }
+
     // the merge's launch parameters from a context's state (no launch, no stream work)
     void prepare_merge(isaacb_ctx* c, MergeParams& p)
     {
@@ -618,7 +648,7 @@ namespace
         p.totalWeight = 0.0f;
         for(int s = 0; s < c->nVol; ++s)
         {
-            p.src[s] = c->src[s];
+            p.src[s] = source_data(c, s);
             p.fdim[s] = int32_t(c->desc.feature_dim[s]);
             p.chain[s] = c->chain[s];
             p.chainIdem[s] = (c->chain[s].op[0] == OP_IDEM && c->chain[s].op[1] == OP_IDEM && c->chain[s].op[2] == OP_IDEM) ? 1 : 0;
@@ -705,8 +735,8 @@ extern "C"
         {
             if(d->feature_dim[s] < 1 || d->feature_dim[s] > 4)
                 return fail(nullptr, ISAACB_INVALID_ARG, "isaacb_create: feature_dim must be 1..4");
-            if(d->guard_size[s] != 0)
-                return fail(nullptr, ISAACB_INVALID_ARG, "isaacb_create: guard_size must be 0");
+            if(d->guard_size[s] > 64 || (s >= d->n_volume_sources && d->guard_size[s] != 0))
+                return fail(nullptr, ISAACB_INVALID_ARG, "isaacb_create: guard_size must be 0..64 (0 for particle sources)");
         }
         isaacb_ctx* c = new isaacb_ctx;
         c->desc = *d;
@@ -810,6 +840,8 @@ extern "C"
     {
         if(!c)
             return ISAACB_OK;
+        for(float* q : c->compact)
+            cudaFree(q);
         cudaFree(c->lutDev);
         cudaFree(c->lutPre);
         cudaFree(c->psPre);
@@ -964,6 +996,33 @@ extern "C"
         c->aoFilter = filter != 0;
         return ISAACB_OK;
     }
+    isaacb_status isaacb_set_ao_pattern(isaacb_ctx* c, uint32_t samples, float radius)
+    {
+        if(!c || samples > uint32_t(kMaxAoSamples) || (samples > 0 && !(radius >= 1.0f && radius <= 127.0f)))
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_ao_pattern: samples 0..32, radius 1..127 px");
+        // a golden-angle spiral filling the disc evenly: tap k at radius r*sqrt((k+0.5)/n),
+        // angle k * pi * (3 - sqrt(5)), rounded to whole pixels
+        const double golden = 3.14159265358979323846 * (3.0 - std::sqrt(5.0));
+        for(uint32_t k = 0; k < samples; ++k)
+        {
+            const double r = double(radius) * std::sqrt((double(k) + 0.5) / double(samples));
+            const double a = golden * double(k);
+            c->aoOffsets[2 * k] = int8_t(std::lround(r * std::cos(a)));
+            c->aoOffsets[2 * k + 1] = int8_t(std::lround(r * std::sin(a)));
+        }
+        c->aoSamples = int(samples);
+        return ISAACB_OK;
+    }
+    isaacb_status isaacb_get_ao_pattern(isaacb_ctx* c, uint32_t* samples, int32_t* offsets)
+    {
+        if(!c || !samples)
+            return ISAACB_INVALID_ARG;
+        *samples = uint32_t(c->aoSamples);
+        if(offsets)
+            for(int k = 0; k < 2 * c->aoSamples; ++k)
+                offsets[k] = c->aoOffsets[k];
+        return ISAACB_OK;
+    }
     isaacb_status isaacb_set_render_mode(isaacb_ctx* c, int32_t m)
     {
         if(!c)
@@ -985,6 +1044,8 @@ extern "C"
             return fail(c, ISAACB_INVALID_ARG, "isaacb_set_field_source: bad source");
         if(enabled && c->desc.feature_dim[s] != 3)
             return fail(c, ISAACB_INVALID_ARG, "isaacb_set_field_source: a field source is a float3 vector field");
+        if(enabled && c->desc.guard_size[s] != 0)
+            return fail(c, ISAACB_INVALID_ARG, "isaacb_set_field_source: field sources take no guard cells here");
         bool f[kMaxSources];
         for(int k = 0; k < c->nVol; ++k)
             f[k] = c->field[k];
@@ -1198,6 +1259,9 @@ extern "C"
         c->updateLaunches = 0;
         if(c->renderer == ISAACB_RENDERER_COMBINED)
         {
+            r = compact_guarded(c, st);
+            if(r != ISAACB_OK)
+                return r;
             if(!c->advectedThisFrame)
             {
                 r = advect_fields(c, st);
@@ -1237,8 +1301,16 @@ extern "C"
         else
         {
             for(int k = 0; k < c->nVol; ++k)
+            {
                 if(c->field[k] && (c->weight[k] != 0.0f || c->iso[k] != 0.0f))
                     return fail(c, ISAACB_INVALID_ARG, "isaacb_update: field sources are merged by the combined renderer only");
+                // the reference's per-source sampler clamps a guarded persistent source's
+                // coordinates to [-guard, ...] computed on an unsigned size
+                // (lib/isaac/isaac_volume_kernel.hpp:206-214), which lands every sample
+                // on the far corner; guarded sources take the combined renderer here
+                if(c->desc.guard_size[k] != 0 && (c->weight[k] != 0.0f || c->iso[k] != 0.0f))
+                    return fail(c, ISAACB_INVALID_ARG, "isaacb_update: guarded sources need the combined renderer");
+            }
             for(int k = 0; k < ISAACB_TIMING_SLOTS; ++k)
                 c->evUsed[k] = false;
             if(c->timing)
@@ -1306,6 +1378,8 @@ extern "C"
         p.renderMode = c->renderMode;
         p.aoWeight = c->aoWeight;
         p.aoFilter = c->aoFilter;
+        p.aoSamples = c->aoSamples;
+        std::memcpy(p.aoOffsets, c->aoOffsets, sizeof(p.aoOffsets));
         p.totalWeightAll = 0.0f;
         for(int s = 0; s < c->nTotal; ++s)
             p.totalWeightAll += c->weight[s];
@@ -1446,6 +1520,11 @@ extern "C"
         if(!c || !mn || !mx)
             return fail(c, ISAACB_INVALID_ARG, "isaacb_minmax: null argument");
         cudaStream_t st = (cudaStream_t) stream;
+        {
+            const isaacb_status r = compact_guarded(c, st);
+            if(r != ISAACB_OK)
+                return r;
+        }
         for(int s = 0; s < c->nTotal; ++s)
         {
             MinMaxParams p{};
@@ -1458,7 +1537,7 @@ extern "C"
             {
                 if(!c->src[s])
                     return fail(c, ISAACB_NOT_READY, "isaacb_minmax: source without memory");
-                p.src = c->src[s];
+                p.src = source_data(c, s);
                 p.particle = 0;
             }
             else
@@ -1736,6 +1815,8 @@ namespace
                 for(int s = 0; s < c->nVol; ++s)
                     if(!c->src[s] && (c->weight[s] != 0.0f || c->iso[s] != 0.0f))
                         return batch_fail(ISAACB_NOT_READY, "isaacb_batch: a source has no memory");
+                if(compact_guarded(c, st) != ISAACB_OK)
+                    return batch_fail(ISAACB_CUDA_ERROR, std::string("isaacb_batch: ") + c->lastError);
                 MergeParams p{};
                 prepare_merge(c, p);
                 if(capture)

@@ -16,6 +16,7 @@ namespace isaacb
     constexpr int kMaxSources = 16;
     constexpr int kMaxFunctors = 3;
     constexpr int kMaxClip = 16;
+    constexpr int kMaxAoSamples = 32; // taps of the configurable SSAO pattern
     // Quad-packed apron brick: 8x8 (x,y) slots x 9 z-planes.  Slot (lx,ly,lz) of
     // brick (bx,by,bz) holds the four texels (x0,y0),(x0+1,y0),(x0,y0+1),(x0+1,y0+1)
     // of plane z, with x0 = 8bx-1+lx, y0 = 8by-1+ly, z = 8bz-1+lz, each clamped to

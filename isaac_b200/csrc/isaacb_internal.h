@@ -116,6 +116,9 @@ namespace isaacb
         void* out; // slots of ncomp*4 elements, component major
     };
     void launch_source_bricks(const SourceBrickParams& p, cudaStream_t s);
+    // interior of a source with `guard` cells per side ((X+2g)(Y+2g)(Z+2g) voxels, x fastest)
+    // into a compact X*Y*Z copy, fdim floats per voxel
+    void launch_compact_guarded(const float* src, float* dst, int X, int Y, int Z, int guard, int fdim, cudaStream_t s);
 
     // quad bricks -> linear RGBA8 (diagnostics)
     void launch_unbrick(const Geom& g, const uint4* volQ, uint32_t* out, cudaStream_t s);
@@ -176,6 +179,10 @@ namespace isaacb
         int32_t renderMode;
         float aoWeight;
         int32_t aoFilter;
+        // SSAO taps: 0 = the reference's 7x7 grid at 10 px; else aoSamples pixel offsets
+        // (x, y pairs in aoOffsets), normalised by aoSamples * 42/48 like the grid's 42
+        int32_t aoSamples;
+        int8_t aoOffsets[2 * kMaxAoSamples];
         float totalWeightAll;
         int32_t skipEmpty; // the volume march checks per-brick emptiness
         const float4* lut;

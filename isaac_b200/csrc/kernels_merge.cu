@@ -716,6 +716,29 @@ namespace isaacb
             dst[i] = gclamp(src[i] * 30.0f, 0.0f, 1.0f);
     }
 
+    // one thread per float of the compact copy: consecutive threads read consecutive
+    // floats of one guarded row
+    __global__ void __launch_bounds__(256)
+        k_compact_guarded(const float* __restrict__ src, float* __restrict__ dst, int X, int Y, int Z, int g, int fd)
+    {
+        const size_t rowF = size_t(X) * fd;
+        const size_t n = rowF * Y * Z;
+        const size_t gx = size_t(X + 2 * g), gy = size_t(Y + 2 * g);
+        for(size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        {
+            const size_t row = i / rowF, k = i - row * rowF;
+            const size_t y = row % Y, z = row / Y;
+            dst[i] = __ldg(src + (((z + g) * gy + (y + g)) * gx + g) * fd + k);
+        }
+    }
+
+    void launch_compact_guarded(const float* src, float* dst, int X, int Y, int Z, int guard, int fdim, cudaStream_t s)
+    {
+        const size_t n = size_t(X) * Y * Z * fdim;
+        const size_t blocks = std::min<size_t>((n + 255) / 256, size_t(148) * 32);
+        k_compact_guarded<<<unsigned(blocks), 256, 0, s>>>(src, dst, X, Y, Z, guard, fdim);
+    }
+
     void launch_noise(const NoiseParams& p, float* noise, float* tmp, cudaStream_t s)
     {
         const size_t n = size_t(p.LX) * p.LY * p.LZ;

@@ -349,17 +349,34 @@ namespace isaacb
         const size_t o = pix(p, px, py);
         const float ref = p.depth[o];
         float occ = 0.0f;
-        for(int i = -3; i <= 3; ++i)
+        float ao;
+        if(p.aoSamples == 0)
         {
-            const int x = iclamp(px + i * 10, 0, p.v.W - 1);
-            for(int j = -3; j <= 3; ++j)
+            for(int i = -3; i <= 3; ++i)
             {
-                const int y = iclamp(py + j * 10, 0, p.v.H - 1);
+                const int x = iclamp(px + i * 10, 0, p.v.W - 1);
+                for(int j = -3; j <= 3; ++j)
+                {
+                    const int y = iclamp(py + j * 10, 0, p.v.H - 1);
+                    if(__ldg(p.depth + pix(p, x, y)) < ref)
+                        occ += 1.0f;
+                }
+            }
+            ao = gclamp(occ / 42.0f, 0.0f, 1.0f);
+        }
+        else
+        {
+            // the configurable pattern (no reference counterpart): the same occlusion
+            // test over aoSamples taps, CLAMP at the frame border
+            for(int k = 0; k < p.aoSamples; ++k)
+            {
+                const int x = iclamp(px + p.aoOffsets[2 * k], 0, p.v.W - 1);
+                const int y = iclamp(py + p.aoOffsets[2 * k + 1], 0, p.v.H - 1);
                 if(__ldg(p.depth + pix(p, x, y)) < ref)
                     occ += 1.0f;
             }
+            ao = gclamp(occ / (float(p.aoSamples) * (42.0f / 48.0f)), 0.0f, 1.0f);
         }
-        const float ao = gclamp(occ / 42.0f, 0.0f, 1.0f);
         p.ao[o] = ao;
         if(p.aoFilter)
         {

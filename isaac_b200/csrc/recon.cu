@@ -206,21 +206,9 @@ namespace
         }
     }
 
-    // bilinear x2 of the half-size frame at full-size pixel (X, Y), aligned with the
-    // renderer's pixel positions: even pixels copy, odd ones average two neighbours
     __device__ __forceinline__ float4 bilinear2(const uchar4* __restrict__ low, int h, int w, int X, int Y)
     {
-        const int ya = Y >> 1, yb = min((Y + 1) >> 1, h - 1);
-        const int xa = X >> 1, xb = min((X + 1) >> 1, w - 1);
-        const float wy = (Y & 1) ? 0.5f : 0.0f, wx = (X & 1) ? 0.5f : 0.0f;
-        const uchar4 a = __ldg(low + size_t(ya) * w + xa), b = __ldg(low + size_t(ya) * w + xb);
-        const uchar4 c = __ldg(low + size_t(yb) * w + xa), d = __ldg(low + size_t(yb) * w + xb);
-        auto mix = [&](float va, float vb, float vc, float vd) {
-            const float r0 = va * (1.0f - wx) + vb * wx;
-            const float r1 = vc * (1.0f - wx) + vd * wx;
-            return (r0 * (1.0f - wy) + r1 * wy) / 255.0f;
-        };
-        return make_float4(mix(a.x, b.x, c.x, d.x), mix(a.y, b.y, c.y, d.y), mix(a.z, b.z, c.z, d.z), mix(a.w, b.w, c.w, d.w));
+        return bilinear2_rgba(low, h, w, X, Y);
     }
 
     // per half-size pixel: the 4 full-size predictions, their squared error against the
@@ -297,30 +285,6 @@ namespace
         }
     }
 
-    // the reconstructed full-size frame, RGBA8 (round to nearest, clamped)
-    __global__ void k_frame(const uint8_t* __restrict__ low, const float* __restrict__ r, uint8_t* __restrict__ out, int h, int w)
-    {
-        const size_t n = size_t(h) * w;
-        for(size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
-        {
-            const int x = int(i % w), y = int(i / w);
-            const uchar4* lo = reinterpret_cast<const uchar4*>(low);
-            const float4* rp = reinterpret_cast<const float4*>(r + i * 16);
-#pragma unroll
-            for(int s = 0; s < 4; ++s)
-            {
-                const int X = 2 * x + (s & 1), Y = 2 * y + (s >> 1);
-                const float4 bl = bilinear2(lo, h, w, X, Y);
-                const float4 q = rp[s];
-                auto byte = [](float v) {
-                    return uint8_t(__float2int_rn(fminf(fmaxf(v * 255.0f, 0.0f), 255.0f)));
-                };
-                reinterpret_cast<uchar4*>(out)[size_t(Y) * (2 * w) + X]
-                    = make_uchar4(byte(bl.x + q.x), byte(bl.y + q.y), byte(bl.z + q.z), byte(bl.w + q.w));
-            }
-        }
-    }
-
     // the method without the network: bilinear x2 alone, RGBA8
     __global__ void k_bilinear_frame(const uint8_t* __restrict__ low, uint8_t* __restrict__ out, int h, int w)
     {
@@ -329,10 +293,7 @@ namespace
         {
             const int X = int(i % (2 * w)), Y = int(i / (2 * w));
             const float4 bl = bilinear2(reinterpret_cast<const uchar4*>(low), h, w, X, Y);
-            auto byte = [](float v) {
-                return uint8_t(__float2int_rn(fminf(fmaxf(v * 255.0f, 0.0f), 255.0f)));
-            };
-            reinterpret_cast<uchar4*>(out)[i] = make_uchar4(byte(bl.x), byte(bl.y), byte(bl.z), byte(bl.w));
+            reinterpret_cast<uchar4*>(out)[i] = make_uchar4(unit_byte(bl.x), unit_byte(bl.y), unit_byte(bl.z), unit_byte(bl.w));
         }
     }
 
@@ -477,6 +438,7 @@ struct isaacb_recon
     bf16* act[kLayers] = {}; // outputs (OUT: unused, see r)
     bf16* dpre[kLayers] = {}; // gradient with respect to each layer's pre-activation output
     bf16* cat[kLayers] = {}; // concatenated inputs
+    float* upPart = nullptr; // inference: W_coarse * coarse of a concatenating layer, FP32
     bf16* dcat = nullptr; // gradient of a concatenated input (largest one)
     bf16* x = nullptr;
     float* r = nullptr; // OUT, FP32
@@ -597,6 +559,86 @@ namespace
                     kDefs[d.fine].cout);
             }
             if(!conv_layer(R, L, B, s))
+                return false;
+        }
+        return true;
+    }
+
+    // One image, inference only.  A concatenating 1x1 layer runs as two GEMMs: W_coarse *
+    // coarse at the coarse level into FP32, then W_fine * fine with that partial, upsampled
+    // to the nearest coarse pixel, added before the bias-and-ReLU (a 1x1 convolution
+    // commutes with nearest upsampling), so the concatenated tensor is never formed.  The
+    // output layer writes the RGBA8 frame (bilinear x2 + residual) in its epilogue.  The
+    // sums are the training forward's, in another order (FP32).
+    bool forward_infer(isaacb_recon* R, const uint8_t* low, uint8_t* out, cudaStream_t s)
+    {
+        for(int L = 0; L < kLayers; ++L)
+        {
+            const LayerDef& d = kDefs[L];
+            if(d.src == -2)
+            {
+                const int lf = kLevel[d.fine], lc = kLevel[d.coarse];
+                const int c1 = kDefs[d.coarse].cout, c2 = kDefs[d.fine].cout;
+                ConvGemmParams pc{};
+                pc.x = R->act[d.coarse];
+                pc.w = R->wf[L];
+                pc.wStride = R->T.Kpad[L];
+                pc.yf = R->upPart;
+                pc.B = 1;
+                pc.H = pc.Ho = R->lh[lc];
+                pc.W = pc.Wo = R->lw[lc];
+                pc.Cg = c1;
+                pc.Cout = d.cout;
+                pc.Npad = R->T.Npad[L];
+                pc.Kpad = round_up(c1, 64);
+                pc.ks = 1;
+                pc.stride = 1;
+                pc.errorFlag = R->errorFlag;
+                ConvGemmParams pf = pc;
+                pf.x = R->act[d.fine];
+                pf.w = R->wf[L] + c1;
+                pf.yf = nullptr;
+                pf.y = R->act[L];
+                pf.bias = R->bias[L];
+                pf.relu = d.relu;
+                pf.H = pf.Ho = R->lh[lf];
+                pf.W = pf.Wo = R->lw[lf];
+                pf.Cg = c2;
+                pf.Kpad = round_up(c2, 64);
+                pf.upPart = R->upPart;
+                pf.upH = R->lh[lc];
+                pf.upW = R->lw[lc];
+                if(!row_tiles_apply(pc) || !row_tiles_apply(pf))
+                    return false;
+                if(!launch_conv_gemm(pc, s) || !launch_conv_gemm(pf, s))
+                    return false;
+                continue;
+            }
+            if(L == kLayers - 1)
+            {
+                ConvGemmParams p{};
+                p.x = R->act[d.src];
+                p.w = R->wf[L];
+                p.bias = R->bias[L];
+                p.B = 1;
+                p.H = p.Ho = R->lh[0];
+                p.W = p.Wo = R->lw[0];
+                p.Cg = R->T.cg[L];
+                p.Cout = d.cout;
+                p.Npad = R->T.Npad[L];
+                p.Kpad = R->T.Kpad[L];
+                p.ks = 1;
+                p.stride = 1;
+                p.errorFlag = R->errorFlag;
+                p.frameOut = out;
+                p.frameLow = low;
+                if(d.cout != 16 || !row_tiles_apply(p))
+                    return false;
+                if(!launch_conv_gemm(p, s))
+                    return false;
+                continue;
+            }
+            if(!conv_layer(R, L, 1, s))
                 return false;
         }
         return true;
@@ -754,7 +796,7 @@ extern "C"
         level_sizes(R->maxH, R->maxW, mh, mw);
         bool ok = true;
         int off = 0;
-        size_t maxCat = 0;
+        size_t maxCat = 0, maxUp = 0;
         for(int L = 0; L < kLayers && ok; ++L)
         {
             const LayerDef& d = kDefs[L];
@@ -783,6 +825,7 @@ extern "C"
             {
                 ok = ok && dalloc(R, R->cat[L], pix * d.cin);
                 maxCat = std::max(maxCat, pix * d.cin);
+                maxUp = std::max(maxUp, size_t(R->maxBatch) * mh[kLevel[d.coarse]] * mw[kLevel[d.coarse]] * d.cout);
             }
             if(ok && conv_gemm_smem(R->T.Npad[L], R->T.Kpad[L]) > 227 * 1024)
                 ok = false;
@@ -791,6 +834,7 @@ extern "C"
         R->total = off;
         const size_t pix0 = size_t(R->maxBatch) * mh[0] * mw[0];
         ok = ok && dalloc(R, R->dcat, maxCat) && dalloc(R, R->x, pix0 * 16) && dalloc(R, R->r, pix0 * 16);
+        ok = ok && dalloc(R, R->upPart, maxUp);
         ok = ok && dalloc(R, R->master, size_t(off)) && dalloc(R, R->adamM, size_t(off)) && dalloc(R, R->adamV, size_t(off));
         ok = ok && dalloc(R, R->lossSum, 1) && dalloc(R, R->gradHost, size_t(off)) && dalloc(R, R->sqErr, 1) && dalloc(R, R->errorFlag, 1);
         if(!ok)
@@ -917,9 +961,8 @@ extern "C"
         level_sizes(int(h), int(w), R->lh, R->lw);
         const size_t pix0 = size_t(h) * w;
         k_input<<<grid_for(pix0), 256, 0, s>>>(low, nullptr, 1, int(h), int(w), R->x);
-        if(!forward(R, 1, s))
+        if(!forward_infer(R, low, out, s))
             return fail_r(ISAACB_INVALID_ARG, "isaacb_recon_infer: layer does not fit");
-        k_frame<<<grid_for(pix0), 256, 0, s>>>(low, R->r, out, int(h), int(w));
         const cudaError_t e = cudaGetLastError();
         if(e != cudaSuccess)
             return fail_r(ISAACB_CUDA_ERROR, std::string("isaacb_recon_infer: ") + cudaGetErrorString(e));

@@ -112,13 +112,14 @@ namespace isaacb
             bool abortLocal = false, aborted = false;
             // the whole packed weight matrix, canonical K-major: core (n/8, k/8) at (n/8)*Kpad*16 + (k/8)*128
             {
+                const size_t wStride = p.wStride ? size_t(p.wStride) : size_t(p.Kpad);
                 const int kb = p.Kpad / 8;
                 const int pieces = p.Npad * kb;
                 for(int i = tid; i < pieces; i += kThreads)
                 {
                     const int n = i / kb, k8 = i - n * kb;
                     const uint32_t dst = sB + uint32_t(n >> 3) * uint32_t(p.Kpad) * 16u + uint32_t(k8) * 128u + uint32_t(n & 7) * 16u;
-                    tc::cp_async16(dst, p.w + size_t(n) * p.Kpad + size_t(k8) * 8, 16);
+                    tc::cp_async16(dst, p.w + size_t(n) * wStride + size_t(k8) * 8, 16);
                 }
                 tc::cp_async_commit();
                 tc::cp_async_wait<0>();
@@ -408,13 +409,14 @@ namespace isaacb
                 tc::mbar_init_fence();
             }
             {
+                const size_t wStride = p.wStride ? size_t(p.wStride) : size_t(p.Kpad);
                 const int kb = p.Kpad / 8;
                 const int pieces = p.Npad * kb;
                 for(int i = tid; i < pieces; i += kRowThreads)
                 {
                     const int n = i / kb, k8 = i - n * kb;
                     const uint32_t dst = sB + uint32_t(n >> 3) * uint32_t(p.Kpad) * 16u + uint32_t(k8) * 128u + uint32_t(n & 7) * 16u;
-                    tc::cp_async16(dst, p.w + size_t(n) * p.Kpad + size_t(k8) * 8, 16);
+                    tc::cp_async16(dst, p.w + size_t(n) * wStride + size_t(k8) * 8, 16);
                 }
                 tc::cp_async_commit();
                 tc::cp_async_wait<0>();
@@ -562,58 +564,97 @@ namespace isaacb
                     const int x = xt * kTileM + tid;
                     const bool valid = x < p.Wo;
                     const size_t pix = size_t(row) * p.Wo + x;
-                    for(int c0 = 0; c0 < p.Npad; c0 += 8)
+                    const int y = row % p.Ho, b = row / p.Ho;
+                    const float* up = nullptr;
+                    if(p.upPart && valid)
+                        up = p.upPart
+                            + ((size_t(b) * p.upH + min(y >> 1, p.upH - 1)) * p.upW + min(x >> 1, p.upW - 1)) * p.Cout;
+                    // 16 accumulator columns per TMEM wait
+                    for(int c16 = 0; c16 < p.Npad; c16 += 16)
                     {
-                        float v[8];
-                        tc::tmem_ld8(tmem + uint32_t(a) * half + (lane0 << 16) + uint32_t(c0), v);
+                        float v[2][8];
+                        const uint32_t ta = tmem + uint32_t(a) * half + (lane0 << 16) + uint32_t(c16);
+                        tc::tmem_ld8(ta, v[0]);
+                        tc::tmem_ld8(ta + 8u, v[1]);
                         tc::tmem_wait_ld();
-                        if(!valid || c0 >= p.Cout)
+                        if(!valid)
                             continue;
-                        const size_t o = pix * p.Cout + c0;
-                        if(p.bias)
-                        {
 #pragma unroll
-                            for(int k = 0; k < 8; ++k)
-                                v[k] += __ldg(p.bias + c0 + k);
-                        }
-                        if(p.relu)
+                        for(int hh = 0; hh < 2; ++hh)
                         {
-#pragma unroll
-                            for(int k = 0; k < 8; ++k)
-                                v[k] = fmaxf(v[k], 0.0f);
-                        }
-                        if(p.mask)
-                        {
-                            float mk[8];
-                            unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(p.mask + o)), mk);
-#pragma unroll
-                            for(int k = 0; k < 8; ++k)
-                                v[k] = mk[k] > 0.0f ? v[k] : 0.0f;
-                        }
-                        if(p.yf)
-                        {
-                            float4* dst = reinterpret_cast<float4*>(p.yf + o);
-                            if(p.accumulate)
+                            const int c0 = c16 + 8 * hh;
+                            if(c0 >= p.Cout)
+                                break;
+                            float(&w)[8] = v[hh];
+                            const size_t o = pix * p.Cout + c0;
+                            if(p.bias)
                             {
-                                const float4 u = dst[0], w = dst[1];
-                                v[0] += u.x, v[1] += u.y, v[2] += u.z, v[3] += u.w;
-                                v[4] += w.x, v[5] += w.y, v[6] += w.z, v[7] += w.w;
-                            }
-                            dst[0] = make_float4(v[0], v[1], v[2], v[3]);
-                            dst[1] = make_float4(v[4], v[5], v[6], v[7]);
-                        }
-                        else
-                        {
-                            uint4* dst = reinterpret_cast<uint4*>(p.y + o);
-                            if(p.accumulate)
-                            {
-                                float u[8];
-                                unpack_bf16x8(*dst, u);
 #pragma unroll
                                 for(int k = 0; k < 8; ++k)
-                                    v[k] += u[k];
+                                    w[k] += __ldg(p.bias + c0 + k);
                             }
-                            *dst = pack_bf16x8(v);
+                            if(up)
+                            {
+                                const float4 u0 = __ldg(reinterpret_cast<const float4*>(up + c0));
+                                const float4 u1 = __ldg(reinterpret_cast<const float4*>(up + c0) + 1);
+                                w[0] += u0.x, w[1] += u0.y, w[2] += u0.z, w[3] += u0.w;
+                                w[4] += u1.x, w[5] += u1.y, w[6] += u1.z, w[7] += u1.w;
+                            }
+                            if(p.relu)
+                            {
+#pragma unroll
+                                for(int k = 0; k < 8; ++k)
+                                    w[k] = fmaxf(w[k], 0.0f);
+                            }
+                            if(p.mask)
+                            {
+                                float mk[8];
+                                unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(p.mask + o)), mk);
+#pragma unroll
+                                for(int k = 0; k < 8; ++k)
+                                    w[k] = mk[k] > 0.0f ? w[k] : 0.0f;
+                            }
+                            if(p.frameOut)
+                            {
+                                // channels 4s..4s+3 are the residual of full-size pixel s of the
+                                // 2x2 block: X = 2x + (s & 1), Y = 2y + (s >> 1)
+                                const uchar4* lo = reinterpret_cast<const uchar4*>(p.frameLow) + size_t(b) * p.Ho * p.Wo;
+                                uchar4* fo = reinterpret_cast<uchar4*>(p.frameOut) + size_t(b) * 4 * p.Ho * p.Wo;
+#pragma unroll
+                                for(int q = 0; q < 2; ++q)
+                                {
+                                    const int sp = c0 / 4 + q;
+                                    const int X = 2 * x + (sp & 1), Y = 2 * y + (sp >> 1);
+                                    const float4 bl = bilinear2_rgba(lo, p.Ho, p.Wo, X, Y);
+                                    fo[size_t(Y) * (2 * p.Wo) + X] = make_uchar4(unit_byte(bl.x + w[4 * q]), unit_byte(bl.y + w[4 * q + 1]),
+                                                                                 unit_byte(bl.z + w[4 * q + 2]), unit_byte(bl.w + w[4 * q + 3]));
+                                }
+                            }
+                            else if(p.yf)
+                            {
+                                float4* dst = reinterpret_cast<float4*>(p.yf + o);
+                                if(p.accumulate)
+                                {
+                                    const float4 u = dst[0], t2 = dst[1];
+                                    w[0] += u.x, w[1] += u.y, w[2] += u.z, w[3] += u.w;
+                                    w[4] += t2.x, w[5] += t2.y, w[6] += t2.z, w[7] += t2.w;
+                                }
+                                dst[0] = make_float4(w[0], w[1], w[2], w[3]);
+                                dst[1] = make_float4(w[4], w[5], w[6], w[7]);
+                            }
+                            else
+                            {
+                                uint4* dst = reinterpret_cast<uint4*>(p.y + o);
+                                if(p.accumulate)
+                                {
+                                    float u[8];
+                                    unpack_bf16x8(*dst, u);
+#pragma unroll
+                                    for(int k = 0; k < 8; ++k)
+                                        w[k] += u[k];
+                                }
+                                *dst = pack_bf16x8(w);
+                            }
                         }
                     }
                     tc::fence_before_sync();

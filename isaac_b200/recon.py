@@ -20,6 +20,13 @@ from . import _lib
 from ._lib import check
 
 WEIGHTS = Path(__file__).resolve().parent / "data" / "recon_unet.f32"
+# trained on pairs of the combined (pre-classified RGBA8) renderer
+WEIGHTS_COMBINED = Path(__file__).resolve().parent / "data" / "recon_unet_combined.f32"
+
+
+def weights_for(renderer: str) -> Path:
+    """The trained weights for half-size frames of the given renderer ("per_source" or "combined")."""
+    return WEIGHTS_COMBINED if renderer == "combined" else WEIGHTS
 
 
 def _torch():
@@ -213,6 +220,49 @@ class JudgedRenderer:
             return self.full
         return self.rec
 
+    def autotune_step(self, cameras, steps=(1.0, 1.25, 1.5, 2.0), margin_db: float = 3.0, repeat: int = 3) -> dict:
+        """Step schedule of the half-size render, picked by measurement under the judge's
+        quality constraint.  For every candidate step (cells) the half-size render plus the
+        network is timed (CUDA events, ``repeat`` passes over ``cameras``) and its PSNR
+        against the plain full-size frame measured on each camera.  A candidate qualifies
+        when every camera is at or above ``threshold + margin_db``; the fastest qualifying
+        one is set on the half-size view (the first candidate when none qualifies) and the
+        report returned.  The plain frames are the judge's own, so the choice keeps the
+        learned path above the fallback threshold on these views."""
+        torch = _torch()
+        fulls = []
+        for P, MV in cameras:
+            self.full_viz.setCamera(P, MV)
+            f = torch.empty_like(self.full)
+            self.full_viz.render(f)
+            fulls.append(f)
+        results = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for st in steps:
+            self.low_viz.setStep(st)
+            ps = []
+            for (P, MV), f in zip(cameras, fulls):
+                self.low_viz.setCamera(P, MV)
+                self.low_viz.render(self.half)
+                self.net.infer(self.half, self.rec)
+                ps.append(self.measure(self.rec, f))
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(repeat):
+                for P, MV in cameras:
+                    self.low_viz.setCamera(P, MV)
+                    self.low_viz.render(self.half)
+                    self.net.infer(self.half, self.rec)
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / (repeat * len(cameras))
+            results.append({"step": st, "ms": ms, "psnr_min": min(ps), "psnr_mean": sum(ps) / len(ps),
+                            "qualifies": min(ps) >= self.threshold + margin_db})
+        ok = [r for r in results if r["qualifies"]]
+        best = min(ok, key=lambda r: r["ms"]) if ok else results[0]
+        self.low_viz.setStep(best["step"])
+        return {"chosen_step": best["step"], "margin_db": margin_db, "candidates": results}
+
 
 # (ksize, stride, pad, c_in, c_out, output level) of the network's convolutions
 LAYER_SHAPES = [
@@ -256,10 +306,18 @@ def _main(argv=None):
         net.load(Path(a.weights))
     g = torch.Generator(device="cuda").manual_seed(1)
     low = torch.randint(0, 256, (a.height, a.width, 4), dtype=torch.uint8, device="cuda", generator=g)
-    for _ in range(a.repeat):
-        net.infer(low)
+    out = torch.empty((2 * a.height, 2 * a.width, 4), dtype=torch.uint8, device="cuda")
+    net.infer(low, out)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
-    print("ok", net.error_flag())
+    e0.record()
+    for _ in range(a.repeat):
+        net.infer(low, out)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(a.repeat, 1)
+    print(f"ok error_flag={net.error_flag()} ms_per_inference={ms:.4f} "
+          f"tflops={inference_flops(a.height, a.width) / (ms * 1e-3) / 1e12:.1f}")
     return 0
 
 

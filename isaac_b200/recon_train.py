@@ -7,11 +7,12 @@ random 4-8 point transfer functions at full size (step 0.5) and half size
 (step 1.0).  Aligned crops of each frame pair (a half-size crop of c x c and
 the full-size crop of 2c x 2c at twice its origin) are the training pairs.
 
-    python -m isaac_b200.recon_train --pairs 20000 --timesteps 64 --steps 4000
+    python -m isaac_b200.recon_train --pairs 20000 --timesteps 64 --steps 4000 [--renderer combined]
 
-writes the FP32 weights to isaac_b200/data/recon_unet.f32 (the default the
-judged renderer loads) and prints one JSON line with the losses and the
-held-out PSNRs of the reconstruction and of bilinear upsampling.
+writes the FP32 weights to isaac_b200/data/recon_unet.f32 (per-source renderer)
+or recon_unet_combined.f32 (combined renderer), the defaults the judged renderer
+loads, and prints one JSON line with the losses and the held-out PSNRs of the
+reconstruction and of bilinear upsampling.
 """
 
 from __future__ import annotations
@@ -25,15 +26,24 @@ from pathlib import Path
 import numpy as np
 
 from . import scenes
-from .recon import WEIGHTS, Reconstructor, bilinear2, psnr
+from .recon import Reconstructor, bilinear2, psnr, weights_for
 
 SEEDS = (6, 7, 8, 9)
 SLOPES = (-5.0 / 3.0, -2.0, -3.0, -11.0 / 3.0)
 
 
-def random_transfer(rng: np.random.Generator) -> dict:
+def random_transfer(rng: np.random.Generator, sharp: float = 0.35) -> dict:
     """4-8 control points over [0, 1024]; colours uniform, alpha mostly low so
-    the volume stays translucent, with an occasional opaque band."""
+    the volume stays translucent, with an occasional opaque band.  With
+    probability ``sharp`` a near-iso function instead: low alpha except one narrow
+    opaque band (4-40 keys wide) around a random key, which renders as thin
+    surfaces and sharp edges, where a half-size frame loses the most."""
+    if rng.random() < sharp:
+        k = int(rng.integers(60, 964))
+        wd = int(rng.integers(2, 21))
+        lo = (float(rng.random()), float(rng.random()), float(rng.random()), float(rng.uniform(0.0, 0.08)))
+        hi = (float(rng.random()), float(rng.random()), float(rng.random()), float(rng.uniform(0.7, 1.0)))
+        return {0: lo, k - wd: lo, k: hi, k + wd: lo, 1024: lo}
     n = int(rng.integers(4, 9))
     keys = np.sort(rng.choice(np.arange(1, 1024), size=n - 2, replace=False))
     keys = [0] + [int(k) for k in keys] + [1024]
@@ -51,18 +61,25 @@ def random_camera(w: int, h: int, rng: np.random.Generator):
 
 
 class PairRenderer:
-    """A full-size and a half-size view of the same four BF16 sources.
+    """A full-size and a half-size view of the same four sources.
 
-    ``step`` is the full-size ray step; the half-size view marches at twice
-    it.  Both visualizations read the same device fields, which ``set_timestep``
-    overwrites in place."""
+    ``renderer``: "per_source" draws with the per-source renderer from BF16 bricks
+    (transfer functions applied per sample); "combined" with the default renderer
+    from the merged RGBA8 texture (transfer functions baked in by the merge, so a
+    transfer-function change re-merges).  ``step`` is the full-size ray step; the
+    half-size view marches at twice it.  Both visualizations read the same device
+    fields, which ``set_timestep`` overwrites in place."""
 
-    def __init__(self, size: int = 512, width: int = 1920, height: int = 1080, step: float = 0.5, shift: float = 0.05):
+    def __init__(self, size: int = 512, width: int = 1920, height: int = 1080, step: float = 0.5, shift: float = 0.05,
+                 renderer: str = "per_source"):
         import torch
 
         from . import IsaacVisualization, VolumeSource
 
+        if renderer not in ("per_source", "combined"):
+            raise ValueError(f"renderer must be per_source or combined, not {renderer!r}")
         self.size, self.width, self.height, self.step, self.shift = size, width, height, step, shift
+        self.renderer = renderer
         self.fields = [torch.empty((size, size, size), dtype=torch.float32, device="cuda") for _ in SEEDS]
         vols = [VolumeSource(f"src{i}", f, feature_dim=1, persistent=True) for i, f in enumerate(self.fields)]
         n = (size, size, size)
@@ -70,12 +87,14 @@ class PairRenderer:
         self.low = IsaacVisualization("half", (width // 2, height // 2), n, n, (1, 1, 1), (0, 0, 0), vols, [])
         self._keep = vols
         for v, st in ((self.full, step), (self.low, 2 * step)):
-            v.setRenderOptimization(False)
-            for i in range(len(SEEDS)):
-                v.setStorage(i, 1)  # BF16 bricks
+            if renderer == "per_source":
+                v.setRenderOptimization(False)
+                for i in range(len(SEEDS)):
+                    v.setStorage(i, 1)  # BF16 bricks
             v.setInterpolation(True)
             v.setStep(st)
         self.timestep = None
+        self.dirty = True
 
     def set_timestep(self, t: int):
         import torch
@@ -94,6 +113,8 @@ class PairRenderer:
                 v.setTransferPoints(i, tf)
             v.updateTransfer()
             v.setCamera(P, MV)
+        if self.renderer == "combined":
+            self.dirty = True  # the merged texture holds the transfer functions
 
     def render(self, full_out, low_out, update: bool = True):
         """Both frames into (H, W, 4) / (H/2, W/2, 4) uint8 CUDA tensors."""
@@ -200,10 +221,12 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--eval-views", type=int, default=16)
-    ap.add_argument("--out", default=str(WEIGHTS))
+    ap.add_argument("--renderer", default="per_source", choices=["per_source", "combined"])
+    ap.add_argument("--out", default=None, help="weights file (default: the renderer's)")
     a = ap.parse_args(argv)
+    a.out = a.out or str(weights_for(a.renderer))
 
-    pr = PairRenderer(a.size, a.width, a.height)
+    pr = PairRenderer(a.size, a.width, a.height, renderer=a.renderer)
     low, high = make_pairs(pr, a.pairs, a.timesteps, a.crop, a.seed)
     net = Reconstructor(a.batch, a.crop, a.crop, seed=a.seed)
     hist, secs = train(net, low, high, a.steps, a.batch, a.lr, a.seed + 1)
@@ -214,7 +237,8 @@ def main(argv=None):
     # held-out views: another camera and transfer-function stream, timesteps between the trained ones
     rec, bil = evaluate(pr, infer_net, a.eval_views, a.seed + 1000, a.timesteps)
     line = {
-        "pairs": a.pairs, "timesteps": a.timesteps, "crop": a.crop, "steps": a.steps, "batch": a.batch,
+        "renderer": a.renderer, "pairs": a.pairs, "timesteps": a.timesteps, "crop": a.crop, "steps": a.steps,
+        "batch": a.batch,
         "train_seconds": secs, "loss_first": hist[0] if hist else None, "loss_last": hist[-1] if hist else None,
         "psnr_recon_db": {"mean": float(np.mean(rec)), "min": float(np.min(rec))},
         "psnr_bilinear_db": {"mean": float(np.mean(bil)), "min": float(np.min(bil))},

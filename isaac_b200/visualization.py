@@ -54,15 +54,17 @@ def _cm_mul(a: np.ndarray, b: np.ndarray) -> np.ndarray:
 class VolumeSource:
     """A volume source over device memory: ``data`` is a CUDA tensor of shape
     (Z, Y, X, featureDim) or (Z, Y, X), float32, x fastest -- what the reference
-    reads through ``operator[]`` (example/example.cpp:36-143)."""
+    reads through ``operator[]`` (example/example.cpp:36-143).  With ``guard_size``
+    g > 0 the tensor holds g guard cells on every side, (Z+2g, Y+2g, X+2g[, f]), as
+    a simulation's field with ghost cells does; the combined renderer and min/max
+    read its interior."""
 
-    guardSize = 0
-
-    def __init__(self, name: str, data, feature_dim: int | None = None, persistent: bool = True):
+    def __init__(self, name: str, data, feature_dim: int | None = None, persistent: bool = True, guard_size: int = 0):
         self._name = name
         self.data = data
         self.featureDim = int(feature_dim if feature_dim is not None else (data.shape[-1] if data.dim() == 4 else 1))
         self.persistent = bool(persistent)
+        self.guardSize = int(guard_size)
 
     def getName(self) -> str:
         return self._name
@@ -312,6 +314,19 @@ class IsaacVisualization:
     def setAmbientOcclusion(self, enabled: bool, weight: float = 0.5, filter: bool = False):
         self.ambientOcclusion = {"isEnabled": bool(enabled), "weight": float(weight)}
         check(self.lib.isaacb_set_ao(self.ctx, int(enabled), float(weight), int(filter)), self.ctx)
+
+    def setAmbientOcclusionPattern(self, samples: int = 0, radius: float = 8.0):
+        """SSAO taps (no reference counterpart): 0 = the reference's 7x7 grid 10 px apart;
+        1..32 samples on a golden-angle spiral within ``radius`` pixels."""
+        check(self.lib.isaacb_set_ao_pattern(self.ctx, int(samples), float(radius)), self.ctx)
+
+    def ambientOcclusionPattern(self) -> np.ndarray:
+        """The (x, y) pixel offsets of the SSAO taps, shape (samples, 2); empty for the grid."""
+        n = C.c_uint32(0)
+        check(self.lib.isaacb_get_ao_pattern(self.ctx, C.byref(n), None), self.ctx)
+        out = np.zeros(2 * max(n.value, 1), dtype=np.int32)
+        check(self.lib.isaacb_get_ao_pattern(self.ctx, C.byref(n), C.c_void_p(out.ctypes.data)), self.ctx)
+        return out[: 2 * n.value].reshape(-1, 2)
 
     def setRenderMode(self, mode: int):
         self.renderMode = int(mode)

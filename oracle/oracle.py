@@ -135,6 +135,7 @@ class Oracle:
         n_volume,
         transfer_size=1024,
         f64=False,
+        guard=None,
     ):
         self.lib = load()
         self.W, self.H = (int(v) for v in framebuffer)
@@ -158,7 +159,7 @@ class Oracle:
             int(n - n_volume),
             _iarr(feature_dims),
             _iarr([int(p) for p in persistent]),
-            _iarr([0] * n),
+            _iarr(list(guard) if guard is not None else [0] * n),
         )
         if not self.ctx:
             raise ValueError("oracle: bad configuration")

@@ -2,13 +2,16 @@
 // of the reference's example (example/example.cpp:36-228): a scalar source read in
 // place (linearData), a vector source read only through its device operator[], and
 // a particle source behind getIterator(cell).  Reads a scene file, renders one
-// frame, writes the frame and the per-source min/max.
+// frame, writes the frame and the per-source min/max.  With --field the vector source
+// is a field source (the reference's FieldSourceList) with advection, and the frame
+// written is the third of three.
 //
-// usage: frontend_example <scene.bin> <out.bin>
+// usage: frontend_example <scene.bin> <out.bin> [--field]
 #include "isaac_b200.hpp"
 
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 using isaacb::float_dim;
@@ -85,6 +88,10 @@ static T* upload(const std::vector<T>& h)
     return d;
 }
 
+template<bool Field>
+int run(ScalarSource& sc, VectorSource& ve, ParticleSourceCells& ps, int n, int W, int H, int PX, int PY, int PZ,
+        const std::array<double, 16>& P, const std::array<double, 16>& MV, const char* outPath);
+
 int main(int argc, char** argv)
 {
     if(argc < 3)
@@ -111,13 +118,19 @@ int main(int argc, char** argv)
     fread(attr.data(), sizeof(float), 3 * np, f);
     fclose(f);
 
-    std::tuple<ScalarSource, VectorSource> volumes{
-        ScalarSource{upload(scalar), n, n},
-        VectorSource{upload(vec), n, n}};
-    std::tuple<> fields;
-    std::tuple<ParticleSourceCells> particles{ParticleSourceCells{upload(off), upload(pos), upload(attr), PX, PY}};
+    ScalarSource sc{upload(scalar), n, n};
+    VectorSource ve{upload(vec), n, n};
+    ParticleSourceCells ps{upload(off), upload(pos), upload(attr), PX, PY};
+    const bool field = argc > 3 && std::string(argv[3]) == "--field";
+    return field ? run<true>(sc, ve, ps, n, W, H, PX, PY, PZ, P, MV, argv[2])
+                 : run<false>(sc, ve, ps, n, W, H, PX, PY, PZ, P, MV, argv[2]);
+}
 
-    using Viz = isaacb::IsaacVisualization<decltype(volumes), decltype(fields), decltype(particles)>;
+template<bool Field, class Volumes, class Fields, class Particles>
+static int render(Volumes& volumes, Fields& fields, Particles& particles, int n, int W, int H, int PX, int PY, int PZ,
+                  const std::array<double, 16>& P, const std::array<double, 16>& MV, const char* outPath)
+{
+    using Viz = isaacb::IsaacVisualization<Volumes, Fields, Particles>;
     Viz viz(
         "frontend",
         {uint32_t(W), uint32_t(H)},
@@ -138,13 +151,40 @@ int main(int argc, char** argv)
     viz.setInterpolation(true);
     viz.setIsoThreshold(0, 0.45f);
     viz.setCamera(P, MV);
-    const uint8_t* frame = viz.doVisualization();
+    const uint8_t* frame = nullptr;
+    if(Field)
+    {
+        viz.setAdvection(1.0f, 0.95f, 1, 1, 40);
+        for(int k = 0; k < 3; ++k)
+            frame = viz.doVisualization();
+    }
+    else
+        frame = viz.doVisualization();
     auto mm = viz.minMax();
-    FILE* o = fopen(argv[2], "wb");
+    FILE* o = fopen(outPath, "wb");
     fwrite(frame, 1, size_t(W) * H * 4, o);
     fwrite(mm.first.data(), sizeof(float), 3, o);
     fwrite(mm.second.data(), sizeof(float), 3, o);
     fclose(o);
     printf("frontend ok\n");
     return 0;
+}
+
+template<bool Field>
+int run(ScalarSource& sc, VectorSource& ve, ParticleSourceCells& ps, int n, int W, int H, int PX, int PY, int PZ,
+        const std::array<double, 16>& P, const std::array<double, 16>& MV, const char* outPath)
+{
+    std::tuple<ParticleSourceCells> particles{ps};
+    if constexpr(Field)
+    {
+        std::tuple<ScalarSource> volumes{sc};
+        std::tuple<VectorSource> fields{ve};
+        return render<true>(volumes, fields, particles, n, W, H, PX, PY, PZ, P, MV, outPath);
+    }
+    else
+    {
+        std::tuple<ScalarSource, VectorSource> volumes{sc, ve};
+        std::tuple<> fields;
+        return render<false>(volumes, fields, particles, n, W, H, PX, PY, PZ, P, MV, outPath);
+    }
 }

@@ -41,6 +41,7 @@ class Scene:
     transfer_size: int = 1024
     P: object = None  # explicit projection and modelview; None: scenes.camera(camera_seed)
     MV: object = None
+    guard: list = field(default_factory=list)  # per volume source: guard cells per side (arrays include them)
 
 
 def gaussian_pair(n=32, fb=(64, 48), seed=1, **kw) -> Scene:
@@ -71,9 +72,10 @@ def build_oracle(s: Scene, f64: bool = False) -> O.Oracle:
         (1 if p[2].ndim == 1 else p[2].shape[-1]) for p in s.particles
     ]
     pers = [int(p) for _, p in s.volumes] + [1] * len(s.particles)
+    guard = [s.guard[i] if i < len(s.guard) else 0 for i in range(nvol)] + [0] * len(s.particles)
     o = O.Oracle(
         s.fb, s.global_n or s.n, s.n, s.particle_cells, s.position, s.scale, fdims, pers, nvol,
-        transfer_size=s.transfer_size, f64=f64
+        transfer_size=s.transfer_size, f64=f64, guard=guard
     )
     for i, (v, _) in enumerate(s.volumes):
         dt = s.storage[i] if i < len(s.storage) else 0
@@ -93,7 +95,8 @@ def build_gpu(s: Scene):
     vols = []
     for i, (v, pers) in enumerate(s.volumes):
         t = torch.from_numpy(np.ascontiguousarray(v)).cuda()
-        vols.append(VolumeSource(f"src{i}", t, feature_dim=1 if v.ndim == 3 else v.shape[-1], persistent=pers))
+        vols.append(VolumeSource(f"src{i}", t, feature_dim=1 if v.ndim == 3 else v.shape[-1], persistent=pers,
+                                 guard_size=s.guard[i] if i < len(s.guard) else 0))
     parts = []
     for j, p in enumerate(s.particles):
         off, pos, attr, radii, cr = p

@@ -72,7 +72,14 @@ def test_create_rejects_bad_descriptors_without_gpu():
     d.feature_dim[0] = 5
     assert lib.isaacb_create(C.byref(d), C.byref(ctx)) == _lib.INVALID_ARG
     d.feature_dim[0] = 1
-    d.guard_size[0] = 1
+    d.guard_size[0] = 65  # guard cells: 0..64 per side
+    assert lib.isaacb_create(C.byref(d), C.byref(ctx)) == _lib.INVALID_ARG
+    assert b"guard_size" in lib.isaacb_last_error(None)
+    d.guard_size[0] = 0
+    d.n_particle_sources = 1
+    d.local_particle_size[:] = (2, 2, 2)
+    d.feature_dim[1] = 1
+    d.guard_size[1] = 1  # particle sources have no guard
     assert lib.isaacb_create(C.byref(d), C.byref(ctx)) == _lib.INVALID_ARG
 
 

@@ -58,10 +58,28 @@ def error_row(img: np.ndarray, ref64: np.ndarray) -> dict:
     }
 
 
+# Per-row bounds on the GPU frame against FP64 (max LSB, mean LSB, min PSNR dB), set from
+# the measured table with margin.  The full-feature row is dominated by threshold
+# decisions -- iso hits at local maxima of the field near the threshold, particle
+# silhouettes and the SSAO depth comparisons they feed -- that FP32 and FP64 arithmetic
+# take differently at a few hundred pixels; the FP32 oracle shows the same error.
+BOUNDS = {
+    "gaussian_128_512px_combined": (3, 0.02, 60.0),
+    "full_feature_256_1080p_combined": (255, 0.6, 33.0),
+    "precision_512_1080p_combined": (3, 0.02, 60.0),
+    "precision_512_1080p_per_source_f32": (3, 0.02, 60.0),
+    "precision_512_1080p_per_source_bf16": (3, 0.03, 60.0),
+    "precision_512_1080p_per_source_f16": (3, 0.02, 60.0),
+}
+
+
 def _record(name, got, ref32, ref64, **extra):
     row = {"gpu": error_row(got, ref64), "oracle_fp32": error_row(ref32, ref64)}
     row.update(extra)
     TABLE[name] = row
+    mx, mean, psnr = BOUNDS[name]
+    g = row["gpu"]
+    assert g["max"] <= mx and g["mean"] <= mean and g["psnr_db"] >= psnr, (name, row)
     return row
 
 

@@ -1,6 +1,8 @@
 """The C++ front end (include/isaac_b200.hpp) used as a simulation would use it:
 compiled with nvcc into tests/cpp/frontend_example.cu, fed a seeded scene, and
-checked against the CPU oracle (frame within the parity bar, min/max bit-exact)."""
+checked against the CPU oracle (frame within the parity bar, min/max bit-exact).
+With a field source (the reference's FieldSourceList), the vector source is
+advected and the third frame is compared."""
 
 import os
 import shutil
@@ -27,7 +29,8 @@ def _compile(tmp):
     return exe
 
 
-def test_cpp_frontend_matches_oracle(tmp_path):
+@pytest.mark.parametrize("field", [False, True], ids=["volume_sources", "field_source"])
+def test_cpp_frontend_matches_oracle(tmp_path, field):
     B.build()
     n, W, H = 32, 64, 48
     cells = (8, 8, 8)
@@ -46,7 +49,8 @@ def test_cpp_frontend_matches_oracle(tmp_path):
         attr.numpy().tofile(f)
     exe = _compile(str(tmp_path))
     out_file = tmp_path / "out.bin"
-    r = subprocess.run([exe, str(scene_file), str(out_file)], capture_output=True, text=True)
+    r = subprocess.run([exe, str(scene_file), str(out_file)] + (["--field"] if field else []), capture_output=True,
+                       text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     raw = np.fromfile(out_file, dtype=np.uint8)
     frame = raw[: W * H * 4].reshape(H, W, 4)
@@ -65,6 +69,11 @@ def test_cpp_frontend_matches_oracle(tmp_path):
     s.iso = [0.45, 0.0]
     o = build_oracle(s)
     o.set_camera(P, MV)
+    if field:
+        o.set_field(1)
+        o.set_advection(1.0, 0.95, 1, 1, 40)
+        for _ in range(2):
+            o.frame()
     ref = o.frame()
     assert_image_parity(frame, ref)
     rmn, rmx = o.minmax()
