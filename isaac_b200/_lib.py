@@ -186,6 +186,7 @@ SIGNATURES = {
     "isaacb_recon_infer": (_i32, [_P, _P, _u32, _u32, _P, _P]),
     "isaacb_recon_error": (_i32, [_P, _i32p]),
     "isaacb_recon_arm_wait_check": (_i32, [_P, _u32]),
+    "isaacb_conv_set_producer": (_i32, [_i32]),
     "isaacb_upsample_bilinear2": (_i32, [_P, _u32, _u32, _P, _P]),
     "isaacb_image_sq_error": (_i32, [_P, _P, C.c_uint64, _P, _P]),
     "isaacb_composite": (_i32, [_i32, _P, _P, _u32, _u32, _u32, _u32, _P, _P]),

@@ -116,6 +116,43 @@ class IsaacBatch:
     def launchGraph(self):
         check(self.lib.isaacb_batch_launch_graph(self.handle, self._stream()))
 
+    def autotune_step(self, steps=(0.5, 0.75, 1.0, 1.5), threshold_db: float = 40.0, repeat: int = 3) -> dict:
+        """Step schedule under a quality constraint: every view is rendered at step 0.5
+        (the reference's default) as the judge, then at each candidate step; a candidate
+        qualifies when every view's PSNR against its judge frame is at or above
+        ``threshold_db``, and the fastest qualifying candidate (render time by CUDA
+        events over ``repeat`` launches) is set on every visualization.  Frames at a
+        larger step are not bit-identical to the reference's step; the report says how
+        far they are."""
+        from .recon import psnr
+
+        torch = _torch()
+        for v in self.vis:
+            v.setStep(0.5)
+        self.render(update=False)
+        judge = [f.clone() for f in self.frames]
+        acc = torch.zeros(1, dtype=torch.int64, device="cuda")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        results = []
+        for st in steps:
+            for v in self.vis:
+                v.setStep(st)
+            self.render(update=False)
+            ps = [psnr(f, j, acc) for f, j in zip(self.frames, judge)]
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(repeat):
+                self.render(update=False)
+            e1.record()
+            e1.synchronize()
+            results.append({"step": st, "ms": e0.elapsed_time(e1) / repeat, "psnr_min": min(ps),
+                            "psnr_mean": sum(ps) / len(ps), "qualifies": min(ps) >= threshold_db})
+        ok = [r for r in results if r["qualifies"]]
+        best = min(ok, key=lambda r: r["ms"]) if ok else results[0]
+        for v in self.vis:
+            v.setStep(best["step"])
+        return {"chosen_step": best["step"], "threshold_db": threshold_db, "candidates": results}
+
     def autotune(self) -> tuple[BatchConfig, float]:
         """Time every tile shape, CTA count and skipping choice; keep the fastest."""
         best = BatchConfig()

@@ -164,6 +164,53 @@ namespace isaacb
             return false;
         }
 
+        // one arrival that also expects `bytes` of asynchronous (TMA) transactions
+        __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
+        {
+            asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(
+                             smem_addr(bar)),
+                         "r"(bytes)
+                         : "memory");
+        }
+        // tiled TMA loads of a box at integer coordinates (innermost first) into shared
+        // memory, completing `bytes` on the mbarrier; no multicast.  dst 128-byte aligned;
+        // the innermost coordinate times the element size a multiple of 16 bytes.
+        __device__ __forceinline__ void tma_load_4d(uint32_t dst, const void* tmap, int c0, int c1, int c2, int c3, uint64_t* bar)
+        {
+            asm volatile(
+                "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(
+                    dst),
+                "l"(tmap),
+                "r"(c0),
+                "r"(c1),
+                "r"(c2),
+                "r"(c3),
+                "r"(smem_addr(bar))
+                : "memory");
+        }
+        __device__ __forceinline__ void tma_load_5d(
+            uint32_t dst,
+            const void* tmap,
+            int c0,
+            int c1,
+            int c2,
+            int c3,
+            int c4,
+            uint64_t* bar)
+        {
+            asm volatile(
+                "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(
+                    dst),
+                "l"(tmap),
+                "r"(c0),
+                "r"(c1),
+                "r"(c2),
+                "r"(c3),
+                "r"(c4),
+                "r"(smem_addr(bar))
+                : "memory");
+        }
+
         __device__ __forceinline__ void mbar_arrive(uint64_t* bar)
         {
             asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" ::"r"(smem_addr(bar)) : "memory");

@@ -28,6 +28,8 @@
 #include "isaacb_conv.h"
 #include "isaacb_tc.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <algorithm>
 #include <string>
@@ -352,27 +354,34 @@ namespace isaacb
         // consecutive 16-byte rows, and consecutive output pixels are consecutive
         // entries of a run (of a parity plane for stride 2).  Warp roles:
         //   warps 0-3  epilogue (TMEM lane = pixel), double-buffered accumulators
-        //   warps 4-7  producers: cp.async of the halo, arrival on the stage's mbarrier
+        //   warps 4-7  producers: cp.async of the halo, arrival on the stage's mbarrier;
+        //              with TMA one thread of warp 4 issues one tiled bulk-tensor load per
+        //              run (a box of 8 channels x the run's pixels) instead
         //   warp 8     one thread issues the MMAs and commits them
         constexpr int kRowThreads = 288;
 
         struct RowGeom
         {
             int S; // stride: 1 or 2
-            int HWp; // entries per run (per parity plane for stride 2)
+            int HWp; // entries between runs (per parity plane for stride 2)
+            int HWn; // entries a run needs (<= HWp; HWp is padded to 8 for TMA destinations)
             int stages; // halo buffers: 1 or 2
         };
 
-        __host__ __device__ inline RowGeom row_geom(int stride, int ks, int pad, int stages)
+        __host__ __device__ inline RowGeom row_geom(int stride, int ks, int pad, int stages, bool tma = false)
         {
             RowGeom g;
             g.S = stride;
-            g.HWp = stride == 1 ? kTileM + 2 * pad : kTileM + (ks - 1) / 2 + 1;
+            g.HWn = stride == 1 ? kTileM + 2 * pad : kTileM + (ks - 1) / 2 + 1;
+            // a TMA destination starts on a 128-byte boundary: runs of a multiple of 8 entries
+            g.HWp = tma ? (g.HWn + 7) / 8 * 8 : g.HWn;
             g.stages = stages;
             return g;
         }
 
-        __global__ void __launch_bounds__(kRowThreads, 1) k_conv_row(const __grid_constant__ ConvGemmParams p, const RowGeom rg)
+        template<bool TMA>
+        __global__ void __launch_bounds__(kRowThreads, 1)
+            k_conv_row(const __grid_constant__ ConvGemmParams p, const RowGeom rg, const __grid_constant__ CUtensorMap tmap)
         {
             extern __shared__ unsigned char dsm[];
             __shared__ uint32_t sTmem;
@@ -400,7 +409,7 @@ namespace isaacb
             {
                 for(int s = 0; s < 2; ++s)
                 {
-                    tc::mbar_init(&sFull[s], 128);
+                    tc::mbar_init(&sFull[s], TMA ? 1 : 128);
                     tc::mbar_init(&sEmpty[s], 1);
                     tc::mbar_init(&sAccFull[s], 1);
                     tc::mbar_init(&sAccEmpty[s], 128);
@@ -441,7 +450,52 @@ namespace isaacb
             const int tilesPerRow = (p.Wo + kTileM - 1) / kTileM;
             const int nTiles = p.B * p.Ho * tilesPerRow;
 
-            if(warp >= 4 && warp < 8)
+            if(TMA && warp >= 4 && warp < 8)
+            {
+                // entry (ty, chunk j, parity q, idx) holds input column S*x0 - pad + S*idx + q:
+                // one box per run.  Stride 1: map (C, W, H, B), box (8, HWn, 1, 1) at
+                // (8j, x0 - pad, row, b).  Stride 2: map (C, 2, W/2, H, B), the column split
+                // into its parity and half, box (8, 1, HWn, 1, 1) at (8j, c & 1, c >> 1, row,
+                // b) with c = 2*x0 - pad + q.  Rows and columns outside the image read zeros.
+                if(tid == 128)
+                {
+                    const uint32_t txBytes = uint32_t(ks * nC * S * rg.HWn) * 16u;
+                    int i = 0;
+                    for(int tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++i)
+                    {
+                        const int s = i % NS, n = i / NS;
+                        if(n >= 1 && !tc::mbar_wait(&sEmpty[s], uint32_t(n - 1) & 1u))
+                        {
+                            if(p.errorFlag)
+                                atomicExch(p.errorFlag, 1);
+                            break;
+                        }
+                        const int xt = tile % tilesPerRow;
+                        const int row = tile / tilesPerRow;
+                        const int y = row % p.Ho, b = row / p.Ho;
+                        const int x0 = xt * kTileM;
+                        const uint32_t st = sH + uint32_t(s) * haloBytes;
+                        tc::mbar_arrive_expect_tx(&sFull[s], txBytes);
+                        for(int ty = 0; ty < ks; ++ty)
+                        {
+                            const int iy = p.transposed ? y + pad - ty : S * y - pad + ty;
+                            for(int j = 0; j < nC; ++j)
+                                for(int q = 0; q < S; ++q)
+                                {
+                                    const uint32_t dst = st + uint32_t((ty * nC + j) * S + q) * runBytes;
+                                    if(S == 1)
+                                        tc::tma_load_4d(dst, &tmap, 8 * j, x0 - pad, iy, b, &sFull[s]);
+                                    else
+                                    {
+                                        const int c = 2 * x0 - pad + q;
+                                        tc::tma_load_5d(dst, &tmap, 8 * j, c & 1, c >> 1, iy, b, &sFull[s]);
+                                    }
+                                }
+                        }
+                    }
+                }
+            }
+            else if(warp >= 4 && warp < 8)
             {
                 // producers: entry (ty, chunk j, parity q, idx) holds input column S*x0 - pad + S*idx + q
                 const int pt = tid - 128;
@@ -860,30 +914,97 @@ namespace isaacb
         return p.Cg % 16 == 0 && p.Npad <= 256
             && ((p.stride == 1 && 2 * p.pad == p.ks - 1) || (p.stride == 2 && !p.transposed && p.ks <= 3 && p.pad <= 1));
     }
-    size_t conv_row_smem(const ConvGemmParams& p, int stages)
+    size_t conv_row_smem(const ConvGemmParams& p, int stages, bool tma = false)
     {
-        const RowGeom g = row_geom(p.stride, p.ks, p.pad, stages);
+        const RowGeom g = row_geom(p.stride, p.ks, p.pad, stages, tma);
         return size_t(p.Npad) * p.Kpad * 2 + size_t(stages) * p.ks * (p.Cg / 8) * g.S * g.HWp * 16 + 128;
     }
+
+    namespace
+    {
+        PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+        {
+            static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+            static bool tried = false;
+            if(!tried)
+            {
+                tried = true;
+                void* f = nullptr;
+                cudaDriverEntryPointQueryResult q{};
+                if(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess
+                   && q == cudaDriverEntryPointSuccess)
+                    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+            }
+            return fn;
+        }
+
+        // The tensor map of a row-tile convolution's input for the TMA producer (layouts at
+        // k_conv_row); false when the input does not fit one (then the cp.async producer runs)
+        bool encode_row_map(const ConvGemmParams& p, const RowGeom& g, CUtensorMap& m)
+        {
+            auto enc = tensor_map_encoder();
+            if(!enc || (reinterpret_cast<uintptr_t>(p.x) & 15u) != 0 || p.Cg % 8 != 0)
+                return false;
+            const cuuint64_t C = cuuint64_t(p.Cg), W = cuuint64_t(p.W), H = cuuint64_t(p.H), B = cuuint64_t(p.B);
+            cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+            CUresult r;
+            if(g.S == 1)
+            {
+                cuuint64_t dims[4] = {C, W, H, B};
+                cuuint64_t strides[3] = {C * 2, W * C * 2, H * W * C * 2};
+                cuuint32_t box[4] = {8, cuuint32_t(g.HWn), 1, 1};
+                r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(p.x), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            }
+            else
+            {
+                if(p.W % 2 != 0)
+                    return false; // the parity split views W as (W/2, 2)
+                cuuint64_t dims[5] = {C, 2, W / 2, H, B};
+                cuuint64_t strides[4] = {C * 2, 2 * C * 2, W * C * 2, H * W * C * 2};
+                cuuint32_t box[5] = {8, 1, cuuint32_t(g.HWn), 1, 1};
+                r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16*>(p.x), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            }
+            return r == CUDA_SUCCESS;
+        }
+
+        template<bool TMA>
+        void launch_row(const ConvGemmParams& p, int stages, const CUtensorMap& m, cudaStream_t s)
+        {
+            const size_t smem = conv_row_smem(p, stages, TMA);
+            cudaFuncSetAttribute(k_conv_row<TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            cudaFuncSetAttribute(k_conv_row<TMA>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+            const int tiles = p.B * p.Ho * ((p.Wo + kTileM - 1) / kTileM);
+            int perSm = ctas_per_sm(k_conv_row<TMA>, kRowThreads, smem);
+            while(perSm > 1 && perSm * 2 * int(tmem_columns(p.Npad)) > 512)
+                --perSm;
+            const int slots = num_sms() * perSm;
+            k_conv_row<TMA><<<tiles < slots ? tiles : slots, kRowThreads, smem, s>>>(
+                p,
+                row_geom(p.stride, p.ks, p.pad, stages, TMA),
+                m);
+        }
+    } // namespace
+
+    bool g_rowTma = true; // the TMA producer where the input allows it
 
     bool launch_conv_gemm(const ConvGemmParams& p, cudaStream_t s)
     {
         if(row_tiles_apply(p))
         {
             int stages = 2;
-            if(conv_row_smem(p, 2) > 227 * 1024)
+            if(conv_row_smem(p, 2, true) > 227 * 1024)
                 stages = 1;
-            if(conv_row_smem(p, stages) <= 227 * 1024)
+            if(conv_row_smem(p, stages, true) <= 227 * 1024)
             {
-                const size_t smem = conv_row_smem(p, stages);
-                cudaFuncSetAttribute(k_conv_row, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-                cudaFuncSetAttribute(k_conv_row, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-                const int tiles = p.B * p.Ho * ((p.Wo + kTileM - 1) / kTileM);
-                int perSm = ctas_per_sm(k_conv_row, kRowThreads, smem);
-                while(perSm > 1 && perSm * 2 * int(tmem_columns(p.Npad)) > 512)
-                    --perSm;
-                const int slots = num_sms() * perSm;
-                k_conv_row<<<tiles < slots ? tiles : slots, kRowThreads, smem, s>>>(p, row_geom(p.stride, p.ks, p.pad, stages));
+                CUtensorMap m{};
+                if(g_rowTma && encode_row_map(p, row_geom(p.stride, p.ks, p.pad, stages, true), m))
+                    launch_row<true>(p, stages, m, s);
+                else
+                    launch_row<false>(p, stages, m, s);
                 return true;
             }
         }
@@ -999,6 +1120,12 @@ extern "C"
             set_global_error(std::string("isaacb_conv_forward: ") + cudaGetErrorString(e));
             return ISAACB_CUDA_ERROR;
         }
+        return ISAACB_OK;
+    }
+
+    isaacb_status isaacb_conv_set_producer(int32_t tma)
+    {
+        g_rowTma = tma != 0;
         return ISAACB_OK;
     }
 

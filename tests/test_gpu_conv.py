@@ -105,3 +105,35 @@ def test_conv_forward_dgrad_wgrad(case):
     _close(got, ref_mat, 2e-3, "wgrad")
     torch.cuda.synchronize()
     assert int(flag.item()) == 0
+
+
+@pytest.mark.parametrize("case", CASES, ids=[str(c) for c in CASES])
+def test_tma_and_cp_async_producers_agree(case):
+    """The row-tile kernel loads its halo with tiled TMA copies where the input allows
+    (stride 1; stride 2 with an even width) and with cp.async gathers otherwise; both
+    fill the same shared-memory runs, so the outputs are bit-identical."""
+    B, H, W, Ci, Co, ks, s, pad = case
+    rng = np.random.default_rng(7)
+    Ho, Wo = R.out_size(H, ks, s, pad), R.out_size(W, ks, s, pad)
+    x = _bf16(rng.standard_normal((B, H, W, Ci)).astype(np.float32))
+    w = R.round_bf16((rng.standard_normal((Co, ks, ks, Ci)) / np.sqrt(ks * ks * Ci)).astype(np.float32))
+    wd, wt = _bf16(R.pack_weights(w)), _bf16(R.pack_weights_transposed(w))
+    dy = _bf16(rng.standard_normal((B, Ho, Wo, Co)).astype(np.float32))
+    lib = _lib.load()
+    outs = []
+    try:
+        for tma in (1, 0):
+            _lib.check(lib.isaacb_conv_set_producer(tma))
+            yf = torch.zeros((B, Ho, Wo, Co), dtype=torch.float32, device="cuda")
+            _run("isaacb_conv_forward", x=x.data_ptr(), w=wd.data_ptr(), y_f32=yf.data_ptr(), batch=B, in_h=H, in_w=W,
+                 c_in=Ci, out_h=Ho, out_w=Wo, c_out=Co, ksize=ks, stride=s, pad=pad)
+            dx = torch.zeros((B, H, W, Ci), dtype=torch.float32, device="cuda")
+            if s == 1:
+                _run("isaacb_conv_forward", x=dy.data_ptr(), w=wt.data_ptr(), y_f32=dx.data_ptr(), batch=B, in_h=Ho,
+                     in_w=Wo, c_in=Co, out_h=H, out_w=W, c_out=Ci, ksize=ks, stride=s, pad=pad, transposed=1)
+            torch.cuda.synchronize()
+            outs.append((yf.cpu(), dx.cpu()))
+    finally:
+        _lib.check(lib.isaacb_conv_set_producer(1))
+    assert torch.equal(outs[0][0], outs[1][0])
+    assert torch.equal(outs[0][1], outs[1][1])

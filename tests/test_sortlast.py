@@ -6,6 +6,7 @@ by the oracle.  The frame heights do not divide by the world size."""
 
 import os
 import socket
+import time
 
 import numpy as np
 import pytest
@@ -90,3 +91,47 @@ def test_gloo_ranks_composite_like_the_oracle(tmp_path, world, h, w, distances, 
         got = np.load(tmp_path / f"rank{r}.npy")
         assert got.shape == (h, w, 4)
         assert np.array_equal(got, ref)
+
+
+def _failing_rank_main(rank, world, port, out_dir):
+    """Rank 1 leaves between frames (it raises after one composite); the survivors'
+    next composite must end with an error from the short process-group timeout instead
+    of waiting for good."""
+    import datetime
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import torch.distributed as dist
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    comp = S.SortLastCompositor(blend=_oracle_blend)
+    frame = torch.from_numpy(_premultiplied(6, 4, seed=100 + rank))
+    comp.composite(frame, float(rank))  # a good frame first
+    if rank == 1:
+        os._exit(0)  # leaves between steps: nothing of it is in flight
+    t0 = time.time()
+    try:
+        comp.composite(frame, float(rank))
+        outcome = "completed"
+    except Exception as ex:  # the collective reports the missing rank
+        outcome = f"error:{type(ex).__name__}"
+    with open(os.path.join(out_dir, f"rank{rank}.txt"), "w") as f:
+        f.write(f"{outcome}\n{time.time() - t0:.1f}\n")
+    os._exit(0)
+
+
+def test_surviving_ranks_see_a_departed_rank_as_an_error(tmp_path):
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_failing_rank_main, args=(r, 3, port, str(tmp_path))) for r in range(3)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    alive = [p for p in procs if p.is_alive()]
+    for p in alive:
+        p.kill()
+    assert not alive, "a surviving rank waited for good"
+    for r in (0, 2):
+        outcome, secs = (tmp_path / f"rank{r}.txt").read_text().split("\n")[:2]
+        assert outcome.startswith("error"), outcome
+        assert float(secs) < 60.0
