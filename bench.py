@@ -89,6 +89,18 @@ def parse_args():
     return ap.parse_args()
 
 
+def json_safe(v):
+    """The record with every non-finite float (an infinite PSNR of identical frames, a NaN)
+    replaced by None, so that the line is strict JSON."""
+    if isinstance(v, float):
+        return v if math.isfinite(v) else None
+    if isinstance(v, dict):
+        return {k: json_safe(x) for k, x in v.items()}
+    if isinstance(v, (list, tuple)):
+        return [json_safe(x) for x in v]
+    return v
+
+
 def recorded_traffic(key: str):
     """DRAM bytes (read + write) of one launch of the line's dominant kernel, from a 1-pass
     ncu capture of the same workload recorded in profiles/traffic.json; None if absent."""
@@ -415,7 +427,7 @@ def run_reference(args):
         "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference CPU backend not buildable here (alpaka/Boost/glm/IceT/MPI absent); oracle/ CPU restatement timed instead",
     }
-    print(json.dumps(line), flush=True)
+    print(json.dumps(json_safe(line)), flush=True)
     return 0
 
 
@@ -599,7 +611,7 @@ def run_reference_batch(args):
         "e2e": {"value": v, "unit": "batch frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference CPU backend not buildable here (alpaka/Boost/glm/IceT/MPI absent); oracle/ CPU restatement timed instead",
     }
-    print(json.dumps(line), flush=True)
+    print(json.dumps(json_safe(line)), flush=True)
     return 0
 
 
@@ -806,7 +818,7 @@ def run_batch(args, world, rank, local, barrier, max_over_ranks):
             "clocks": clocks,
             "gpu_launches": args.steps * graph_launches,
         }
-        print(json.dumps(line), flush=True)
+        print(json.dumps(json_safe(line)), flush=True)
     batch.close()
     for v in vis:
         v.close()
@@ -879,7 +891,7 @@ def run_sweep(args):
         line["per_source_full"] = _sweep_time(pr.full, full)
         comb.setCamera(P, MV)
         line["combined_full"] = _sweep_time(comb, full)
-        print(json.dumps(line), flush=True)
+        print(json.dumps(json_safe(line)), flush=True)
     comb.close()
     return 0
 
@@ -1102,7 +1114,7 @@ def run_learned(args, world, rank, local, barrier, max_over_ranks, emit=True):
             "gpu_launches": None,
         }
         if emit:
-            print(json.dumps(line), flush=True)
+            print(json.dumps(json_safe(line)), flush=True)
     net.close()
     for v in (pr.full, pr.low):
         v.close()
@@ -1606,7 +1618,7 @@ def main():
             "clocks": clocks,
             "gpu_launches": launches,
         }
-        print(json.dumps(line), flush=True)
+        print(json.dumps(json_safe(line)), flush=True)
     viz.close()
     if world > 1:
         dist.destroy_process_group()

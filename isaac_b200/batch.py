@@ -145,8 +145,11 @@ class IsaacBatch:
                 self.render(update=False)
             e1.record()
             e1.synchronize()
-            results.append({"step": st, "ms": e0.elapsed_time(e1) / repeat, "psnr_min": min(ps),
-                            "psnr_mean": sum(ps) / len(ps), "qualifies": min(ps) >= threshold_db})
+            # an identical frame has infinite PSNR; the report keeps JSON-safe numbers (None)
+            fin = [x for x in ps if x != float("inf")]
+            results.append({"step": st, "ms": e0.elapsed_time(e1) / repeat, "psnr_min": min(fin) if fin else None,
+                            "psnr_mean": sum(fin) / len(fin) if fin else None, "identical_views": len(ps) - len(fin),
+                            "qualifies": min(ps) >= threshold_db})
         ok = [r for r in results if r["qualifies"]]
         best = min(ok, key=lambda r: r["ms"]) if ok else results[0]
         for v in self.vis:

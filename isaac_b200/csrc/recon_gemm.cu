@@ -354,11 +354,18 @@ namespace isaacb
         // consecutive 16-byte rows, and consecutive output pixels are consecutive
         // entries of a run (of a parity plane for stride 2).  Warp roles:
         //   warps 0-3  epilogue (TMEM lane = pixel), double-buffered accumulators
-        //   warps 4-7  producers: cp.async of the halo, arrival on the stage's mbarrier;
-        //              with TMA one thread of warp 4 issues one tiled bulk-tensor load per
-        //              run (a box of 8 channels x the run's pixels) instead
+        //   warps 4-7  producers: cp.async of the halo, arrival on the stage's mbarrier
         //   warp 8     one thread issues the MMAs and commits them
+        // With TMA the halo comes in one tiled bulk-tensor load per run (a box of 8 channels
+        // x the run's pixels) issued by one thread of warp 9, and warps 4-7 join the
+        // epilogue: warps 0-3 take the first half of the accumulator columns, warps 4-7 the
+        // second (a warp reads TMEM lanes 32*(w%4)..+31, so both groups see every pixel).
         constexpr int kRowThreads = 288;
+        template<bool TMA>
+        __host__ __device__ constexpr int row_threads()
+        {
+            return TMA ? 320 : kRowThreads;
+        }
 
         struct RowGeom
         {
@@ -380,11 +387,12 @@ namespace isaacb
         }
 
         template<bool TMA>
-        __global__ void __launch_bounds__(kRowThreads, 1)
+        __global__ void __launch_bounds__(row_threads<TMA>(), 1)
             k_conv_row(const __grid_constant__ ConvGemmParams p, const RowGeom rg, const __grid_constant__ CUtensorMap tmap)
         {
             extern __shared__ unsigned char dsm[];
             __shared__ uint32_t sTmem;
+            __shared__ float sBias[256];
             __shared__ __align__(8) uint64_t sFull[2];
             __shared__ __align__(8) uint64_t sEmpty[2];
             __shared__ __align__(8) uint64_t sAccFull[2];
@@ -412,7 +420,7 @@ namespace isaacb
                     tc::mbar_init(&sFull[s], TMA ? 1 : 128);
                     tc::mbar_init(&sEmpty[s], 1);
                     tc::mbar_init(&sAccFull[s], 1);
-                    tc::mbar_init(&sAccEmpty[s], 128);
+                    tc::mbar_init(&sAccEmpty[s], TMA ? 256 : 128);
                 }
                 tc::mbar_init(&sDrain, 1);
                 tc::mbar_init_fence();
@@ -421,13 +429,16 @@ namespace isaacb
                 const size_t wStride = p.wStride ? size_t(p.wStride) : size_t(p.Kpad);
                 const int kb = p.Kpad / 8;
                 const int pieces = p.Npad * kb;
-                for(int i = tid; i < pieces; i += kRowThreads)
+                for(int i = tid; i < pieces; i += row_threads<TMA>())
                 {
                     const int n = i / kb, k8 = i - n * kb;
                     const uint32_t dst = sB + uint32_t(n >> 3) * uint32_t(p.Kpad) * 16u + uint32_t(k8) * 128u + uint32_t(n & 7) * 16u;
                     tc::cp_async16(dst, p.w + size_t(n) * wStride + size_t(k8) * 8, 16);
                 }
                 tc::cp_async_commit();
+                // the per-channel bias, read by every epilogue thread for every pixel
+                for(int c = tid; c < p.Npad && c < 256; c += row_threads<TMA>())
+                    sBias[c] = (p.bias && c < p.Cout) ? __ldg(p.bias + c) : 0.0f;
                 tc::cp_async_wait<0>();
                 tc::fence_async_smem();
             }
@@ -450,14 +461,14 @@ namespace isaacb
             const int tilesPerRow = (p.Wo + kTileM - 1) / kTileM;
             const int nTiles = p.B * p.Ho * tilesPerRow;
 
-            if(TMA && warp >= 4 && warp < 8)
+            if(TMA && warp == 9)
             {
                 // entry (ty, chunk j, parity q, idx) holds input column S*x0 - pad + S*idx + q:
                 // one box per run.  Stride 1: map (C, W, H, B), box (8, HWn, 1, 1) at
                 // (8j, x0 - pad, row, b).  Stride 2: map (C, 2, W/2, H, B), the column split
                 // into its parity and half, box (8, 1, HWn, 1, 1) at (8j, c & 1, c >> 1, row,
                 // b) with c = 2*x0 - pad + q.  Rows and columns outside the image read zeros.
-                if(tid == 128)
+                if(lane == 0)
                 {
                     const uint32_t txBytes = uint32_t(ks * nC * S * rg.HWn) * 16u;
                     int i = 0;
@@ -495,7 +506,7 @@ namespace isaacb
                     }
                 }
             }
-            else if(warp >= 4 && warp < 8)
+            else if(!TMA && warp >= 4 && warp < 8)
             {
                 // producers: entry (ty, chunk j, parity q, idx) holds input column S*x0 - pad + S*idx + q
                 const int pt = tid - 128;
@@ -600,8 +611,11 @@ namespace isaacb
             }
             else
             {
-                // epilogue: thread = TMEM lane = pixel of the tile
-                const uint32_t lane0 = uint32_t(warp) * 32u;
+                // epilogue: thread = TMEM lane = pixel of the tile; with TMA two groups of four
+                // warps split the accumulator columns
+                const uint32_t lane0 = uint32_t(warp & 3) * 32u;
+                const int colsPer = TMA ? p.Npad / 2 : p.Npad; // a multiple of 8
+                const int cBeg = TMA ? (warp >> 2) * colsPer : 0;
                 int i = 0;
                 for(int tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++i)
                 {
@@ -615,7 +629,7 @@ namespace isaacb
                     tc::fence_after_sync();
                     const int xt = tile % tilesPerRow;
                     const int row = tile / tilesPerRow;
-                    const int x = xt * kTileM + tid;
+                    const int x = xt * kTileM + (tid & 127);
                     const bool valid = x < p.Wo;
                     const size_t pix = size_t(row) * p.Wo + x;
                     const int y = row % p.Ho, b = row / p.Ho;
@@ -623,13 +637,15 @@ namespace isaacb
                     if(p.upPart && valid)
                         up = p.upPart
                             + ((size_t(b) * p.upH + min(y >> 1, p.upH - 1)) * p.upW + min(x >> 1, p.upW - 1)) * p.Cout;
-                    // 16 accumulator columns per TMEM wait
-                    for(int c16 = 0; c16 < p.Npad; c16 += 16)
+                    // 16 accumulator columns per TMEM wait (8 where a column group ends)
+                    for(int c16 = cBeg; c16 < cBeg + colsPer; c16 += 16)
                     {
+                        const bool two = c16 + 16 <= cBeg + colsPer;
                         float v[2][8];
                         const uint32_t ta = tmem + uint32_t(a) * half + (lane0 << 16) + uint32_t(c16);
                         tc::tmem_ld8(ta, v[0]);
-                        tc::tmem_ld8(ta + 8u, v[1]);
+                        if(two)
+                            tc::tmem_ld8(ta + 8u, v[1]);
                         tc::tmem_wait_ld();
                         if(!valid)
                             continue;
@@ -637,7 +653,7 @@ namespace isaacb
                         for(int hh = 0; hh < 2; ++hh)
                         {
                             const int c0 = c16 + 8 * hh;
-                            if(c0 >= p.Cout)
+                            if(c0 >= p.Cout || (hh == 1 && !two))
                                 break;
                             float(&w)[8] = v[hh];
                             const size_t o = pix * p.Cout + c0;
@@ -645,7 +661,7 @@ namespace isaacb
                             {
 #pragma unroll
                                 for(int k = 0; k < 8; ++k)
-                                    w[k] += __ldg(p.bias + c0 + k);
+                                    w[k] += sBias[c0 + k];
                             }
                             if(up)
                             {
@@ -978,11 +994,11 @@ namespace isaacb
             cudaFuncSetAttribute(k_conv_row<TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
             cudaFuncSetAttribute(k_conv_row<TMA>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
             const int tiles = p.B * p.Ho * ((p.Wo + kTileM - 1) / kTileM);
-            int perSm = ctas_per_sm(k_conv_row<TMA>, kRowThreads, smem);
+            int perSm = ctas_per_sm(k_conv_row<TMA>, row_threads<TMA>(), smem);
             while(perSm > 1 && perSm * 2 * int(tmem_columns(p.Npad)) > 512)
                 --perSm;
             const int slots = num_sms() * perSm;
-            k_conv_row<TMA><<<tiles < slots ? tiles : slots, kRowThreads, smem, s>>>(
+            k_conv_row<TMA><<<tiles < slots ? tiles : slots, row_threads<TMA>(), smem, s>>>(
                 p,
                 row_geom(p.stride, p.ks, p.pad, stages, TMA),
                 m);

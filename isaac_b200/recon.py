@@ -256,7 +256,10 @@ class JudgedRenderer:
             e1.record()
             e1.synchronize()
             ms = e0.elapsed_time(e1) / (repeat * len(cameras))
-            results.append({"step": st, "ms": ms, "psnr_min": min(ps), "psnr_mean": sum(ps) / len(ps),
+            # an identical frame has infinite PSNR; the report keeps JSON-safe numbers (None)
+            fin = [x for x in ps if x != float("inf")]
+            results.append({"step": st, "ms": ms, "psnr_min": min(fin) if fin else None,
+                            "psnr_mean": sum(fin) / len(fin) if fin else None, "identical_views": len(ps) - len(fin),
                             "qualifies": min(ps) >= self.threshold + margin_db})
         ok = [r for r in results if r["qualifies"]]
         best = min(ok, key=lambda r: r["ms"]) if ok else results[0]

@@ -111,18 +111,24 @@ def test_short_training_beats_bilinear():
     assert min(gains) > 0.0 and float(np.mean(gains)) > 0.5, gains
 
 
-def test_trained_weights_beat_bilinear_on_held_out_views():
-    """The committed network (trained on 512^3 renders) against the method without it,
-    bilinear x2 of the same half-size render, on views it was not trained on: another
-    seed stream of cameras and transfer functions, a smaller volume and frame."""
-    from isaac_b200.recon import WEIGHTS
+@pytest.mark.parametrize("renderer", ["per_source", "combined"])
+def test_trained_weights_beat_bilinear_on_held_out_views(renderer):
+    """The committed network for each renderer (trained on 512^3 renders) against the
+    method without it, bilinear x2 of the same half-size render, on views it was not
+    trained on: another seed stream of cameras and transfer functions (near-iso ones
+    among them), a smaller volume and frame."""
+    from isaac_b200.recon import weights_for
     from isaac_b200.recon_train import PairRenderer, evaluate
 
-    pr = PairRenderer(size=256, width=640, height=360)
+    pr = PairRenderer(size=256, width=640, height=360, renderer=renderer)
     net = Reconstructor(1, 180, 320, seed=1)
-    net.load(WEIGHTS)
-    rec, bil = evaluate(pr, net, views=6, seed=4242, timesteps=64)
+    net.load(weights_for(renderer))
+    rec, bil = evaluate(pr, net, views=12, seed=4242, timesteps=64)
     gains = np.array(rec) - np.array(bil)
+    print(renderer, "recon", np.round(rec, 2).tolist(), "bilinear", np.round(bil, 2).tolist(), "gain", float(gains.mean()))
     assert net.error_flag() == 0
     assert min(rec) > 40.0, rec
-    assert gains.mean() > 0.1, (rec, bil)
+    # measured: 0.43 dB (per-source) and 0.33 dB (combined) on these 12 views; bilinear is
+    # already within a few dB of the 8-bit truncation floor on these smooth fields
+    assert gains.mean() > 0.2, (rec, bil)
+    assert (gains > -0.05).all(), (rec, bil)
