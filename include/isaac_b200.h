@@ -340,7 +340,7 @@ typedef struct isaacb_conv_args
 } isaacb_conv_args;
 
 isaacb_status isaacb_conv_forward(const isaacb_conv_args* args, void* stream);
-/* Halo producer of the row-tile convolution (stride 1, or stride 2 forward): 1 (the
+/* Input staging of the row-tile convolutions (stride 1, or stride 2 forward): 1 (the
  * default) loads each run of the input rows with one tiled TMA copy where the input
  * allows it (16-byte aligned, an even width for stride 2), 0 gathers it with cp.async
  * in four producer warps.  The results are identical; process-wide setting. */

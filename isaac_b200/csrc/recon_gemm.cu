@@ -386,6 +386,120 @@ namespace isaacb
             return g;
         }
 
+        // Epilogue of one 128-pixel output tile (row y of image b, column tile xt): this
+        // thread's pixel px, accumulator columns [cBeg, cBeg + colsPer) of the TMEM tile at
+        // tAcc (this warp's lanes); bias, the upsampled coarse partial, ReLU, mask, then the
+        // bf16 / FP32 store or the RGBA8 frame.
+        __device__ __forceinline__ void row_epilogue(
+            const ConvGemmParams& p,
+            uint32_t tAcc,
+            int xt,
+            int b,
+            int y,
+            int px,
+            int cBeg,
+            int colsPer,
+            const float* sBias)
+        {
+            const int x = xt * kTileM + px;
+            const bool valid = x < p.Wo;
+            const size_t pix = (size_t(b) * p.Ho + y) * p.Wo + x;
+            const float* up = nullptr;
+            if(p.upPart && valid)
+                up = p.upPart
+                    + ((size_t(b) * p.upH + min(y >> 1, p.upH - 1)) * p.upW + min(x >> 1, p.upW - 1)) * p.Cout;
+            // 16 accumulator columns per TMEM wait (8 where a column group ends)
+            for(int c16 = cBeg; c16 < cBeg + colsPer; c16 += 16)
+            {
+                const bool two = c16 + 16 <= cBeg + colsPer;
+                float v[2][8];
+                const uint32_t ta = tAcc + uint32_t(c16);
+                tc::tmem_ld8(ta, v[0]);
+                if(two)
+                    tc::tmem_ld8(ta + 8u, v[1]);
+                tc::tmem_wait_ld();
+                if(!valid)
+                    continue;
+#pragma unroll
+                for(int hh = 0; hh < 2; ++hh)
+                {
+                    const int c0 = c16 + 8 * hh;
+                    if(c0 >= p.Cout || (hh == 1 && !two))
+                        break;
+                    float(&w)[8] = v[hh];
+                    const size_t o = pix * p.Cout + c0;
+                    if(p.bias)
+                    {
+#pragma unroll
+                        for(int k = 0; k < 8; ++k)
+                            w[k] += sBias[c0 + k];
+                    }
+                    if(up)
+                    {
+                        const float4 u0 = __ldg(reinterpret_cast<const float4*>(up + c0));
+                        const float4 u1 = __ldg(reinterpret_cast<const float4*>(up + c0) + 1);
+                        w[0] += u0.x, w[1] += u0.y, w[2] += u0.z, w[3] += u0.w;
+                        w[4] += u1.x, w[5] += u1.y, w[6] += u1.z, w[7] += u1.w;
+                    }
+                    if(p.relu)
+                    {
+#pragma unroll
+                        for(int k = 0; k < 8; ++k)
+                            w[k] = fmaxf(w[k], 0.0f);
+                    }
+                    if(p.mask)
+                    {
+                        float mk[8];
+                        unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(p.mask + o)), mk);
+#pragma unroll
+                        for(int k = 0; k < 8; ++k)
+                            w[k] = mk[k] > 0.0f ? w[k] : 0.0f;
+                    }
+                    if(p.frameOut)
+                    {
+                        // channels 4s..4s+3 are the residual of full-size pixel s of the
+                        // 2x2 block: X = 2x + (s & 1), Y = 2y + (s >> 1)
+                        const uchar4* lo = reinterpret_cast<const uchar4*>(p.frameLow) + size_t(b) * p.Ho * p.Wo;
+                        uchar4* fo = reinterpret_cast<uchar4*>(p.frameOut) + size_t(b) * 4 * p.Ho * p.Wo;
+#pragma unroll
+                        for(int q = 0; q < 2; ++q)
+                        {
+                            const int sp = c0 / 4 + q;
+                            const int X = 2 * x + (sp & 1), Y = 2 * y + (sp >> 1);
+                            const float4 bl = bilinear2_rgba(lo, p.Ho, p.Wo, X, Y);
+                            fo[size_t(Y) * (2 * p.Wo) + X] = make_uchar4(unit_byte(bl.x + w[4 * q]), unit_byte(bl.y + w[4 * q + 1]),
+                                                                         unit_byte(bl.z + w[4 * q + 2]), unit_byte(bl.w + w[4 * q + 3]));
+                        }
+                    }
+                    else if(p.yf)
+                    {
+                        float4* dst = reinterpret_cast<float4*>(p.yf + o);
+                        if(p.accumulate)
+                        {
+                            const float4 u = dst[0], t2 = dst[1];
+                            w[0] += u.x, w[1] += u.y, w[2] += u.z, w[3] += u.w;
+                            w[4] += t2.x, w[5] += t2.y, w[6] += t2.z, w[7] += t2.w;
+                        }
+                        dst[0] = make_float4(w[0], w[1], w[2], w[3]);
+                        dst[1] = make_float4(w[4], w[5], w[6], w[7]);
+                    }
+                    else
+                    {
+                        uint4* dst = reinterpret_cast<uint4*>(p.y + o);
+                        if(p.accumulate)
+                        {
+                            float u[8];
+                            unpack_bf16x8(*dst, u);
+#pragma unroll
+                            for(int k = 0; k < 8; ++k)
+                                w[k] += u[k];
+                        }
+                        *dst = pack_bf16x8(w);
+                    }
+                }
+            }
+        }
+
         template<bool TMA>
         __global__ void __launch_bounds__(row_threads<TMA>(), 1)
             k_conv_row(const __grid_constant__ ConvGemmParams p, const RowGeom rg, const __grid_constant__ CUtensorMap tmap)
@@ -629,104 +743,8 @@ namespace isaacb
                     tc::fence_after_sync();
                     const int xt = tile % tilesPerRow;
                     const int row = tile / tilesPerRow;
-                    const int x = xt * kTileM + (tid & 127);
-                    const bool valid = x < p.Wo;
-                    const size_t pix = size_t(row) * p.Wo + x;
-                    const int y = row % p.Ho, b = row / p.Ho;
-                    const float* up = nullptr;
-                    if(p.upPart && valid)
-                        up = p.upPart
-                            + ((size_t(b) * p.upH + min(y >> 1, p.upH - 1)) * p.upW + min(x >> 1, p.upW - 1)) * p.Cout;
-                    // 16 accumulator columns per TMEM wait (8 where a column group ends)
-                    for(int c16 = cBeg; c16 < cBeg + colsPer; c16 += 16)
-                    {
-                        const bool two = c16 + 16 <= cBeg + colsPer;
-                        float v[2][8];
-                        const uint32_t ta = tmem + uint32_t(a) * half + (lane0 << 16) + uint32_t(c16);
-                        tc::tmem_ld8(ta, v[0]);
-                        if(two)
-                            tc::tmem_ld8(ta + 8u, v[1]);
-                        tc::tmem_wait_ld();
-                        if(!valid)
-                            continue;
-#pragma unroll
-                        for(int hh = 0; hh < 2; ++hh)
-                        {
-                            const int c0 = c16 + 8 * hh;
-                            if(c0 >= p.Cout || (hh == 1 && !two))
-                                break;
-                            float(&w)[8] = v[hh];
-                            const size_t o = pix * p.Cout + c0;
-                            if(p.bias)
-                            {
-#pragma unroll
-                                for(int k = 0; k < 8; ++k)
-                                    w[k] += sBias[c0 + k];
-                            }
-                            if(up)
-                            {
-                                const float4 u0 = __ldg(reinterpret_cast<const float4*>(up + c0));
-                                const float4 u1 = __ldg(reinterpret_cast<const float4*>(up + c0) + 1);
-                                w[0] += u0.x, w[1] += u0.y, w[2] += u0.z, w[3] += u0.w;
-                                w[4] += u1.x, w[5] += u1.y, w[6] += u1.z, w[7] += u1.w;
-                            }
-                            if(p.relu)
-                            {
-#pragma unroll
-                                for(int k = 0; k < 8; ++k)
-                                    w[k] = fmaxf(w[k], 0.0f);
-                            }
-                            if(p.mask)
-                            {
-                                float mk[8];
-                                unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(p.mask + o)), mk);
-#pragma unroll
-                                for(int k = 0; k < 8; ++k)
-                                    w[k] = mk[k] > 0.0f ? w[k] : 0.0f;
-                            }
-                            if(p.frameOut)
-                            {
-                                // channels 4s..4s+3 are the residual of full-size pixel s of the
-                                // 2x2 block: X = 2x + (s & 1), Y = 2y + (s >> 1)
-                                const uchar4* lo = reinterpret_cast<const uchar4*>(p.frameLow) + size_t(b) * p.Ho * p.Wo;
-                                uchar4* fo = reinterpret_cast<uchar4*>(p.frameOut) + size_t(b) * 4 * p.Ho * p.Wo;
-#pragma unroll
-                                for(int q = 0; q < 2; ++q)
-                                {
-                                    const int sp = c0 / 4 + q;
-                                    const int X = 2 * x + (sp & 1), Y = 2 * y + (sp >> 1);
-                                    const float4 bl = bilinear2_rgba(lo, p.Ho, p.Wo, X, Y);
-                                    fo[size_t(Y) * (2 * p.Wo) + X] = make_uchar4(unit_byte(bl.x + w[4 * q]), unit_byte(bl.y + w[4 * q + 1]),
-                                                                                 unit_byte(bl.z + w[4 * q + 2]), unit_byte(bl.w + w[4 * q + 3]));
-                                }
-                            }
-                            else if(p.yf)
-                            {
-                                float4* dst = reinterpret_cast<float4*>(p.yf + o);
-                                if(p.accumulate)
-                                {
-                                    const float4 u = dst[0], t2 = dst[1];
-                                    w[0] += u.x, w[1] += u.y, w[2] += u.z, w[3] += u.w;
-                                    w[4] += t2.x, w[5] += t2.y, w[6] += t2.z, w[7] += t2.w;
-                                }
-                                dst[0] = make_float4(w[0], w[1], w[2], w[3]);
-                                dst[1] = make_float4(w[4], w[5], w[6], w[7]);
-                            }
-                            else
-                            {
-                                uint4* dst = reinterpret_cast<uint4*>(p.y + o);
-                                if(p.accumulate)
-                                {
-                                    float u[8];
-                                    unpack_bf16x8(*dst, u);
-#pragma unroll
-                                    for(int k = 0; k < 8; ++k)
-                                        w[k] += u[k];
-                                }
-                                *dst = pack_bf16x8(w);
-                            }
-                        }
-                    }
+                    row_epilogue(p, tmem + uint32_t(a) * half + (lane0 << 16), xt, row / p.Ho, row % p.Ho, tid & 127, cBeg,
+                                 colsPer, sBias);
                     tc::fence_before_sync();
                     tc::mbar_arrive(&sAccEmpty[a]);
                 }
@@ -1006,7 +1024,6 @@ namespace isaacb
     } // namespace
 
     bool g_rowTma = true; // the TMA producer where the input allows it
-
     bool launch_conv_gemm(const ConvGemmParams& p, cudaStream_t s)
     {
         if(row_tiles_apply(p))

@@ -304,7 +304,7 @@ def _main(argv=None):
     ap.add_argument("--repeat", type=int, default=3)
     ap.add_argument("--weights", default=str(WEIGHTS))
     ap.add_argument("--producer", default="tma", choices=["tma", "cp_async"],
-                    help="halo producer of the row-tile convolutions")
+                    help="input staging of the row-tile convolutions")
     a = ap.parse_args(argv)
     check(_lib.load().isaacb_conv_set_producer(1 if a.producer == "tma" else 0))
     net = Reconstructor(1, a.height, a.width, seed=1)
