@@ -27,15 +27,12 @@ namespace isaacb
         // an mbarrier that nothing arrives at, raise errorFlag, release TMEM and return
         unsigned long long waitCheckNs;
         // row-tile kernel only (k_conv_row):
-        int wStride; // elements between weight rows; 0 = Kpad
-        // + up(upPart) before the ReLU: FP32 [B][upH][upW][Cout] read at the nearest
-        // coarse pixel (min(y/2, upH-1), min(x/2, upW-1)), or null
-        const float* upPart;
-        int upH, upW;
-        // Cout = 16 residual channels of a pixel-shuffled x2 frame: instead of y/yf, write
-        // the RGBA8 frame bilinear2(frameLow) + residual (2Ho x 2Wo), or null
-        uint8_t* frameOut;
-        const uint8_t* frameLow;
+        // implicit concatenation (cp.async producer, 1x1): the first upC input channels
+        // come from xUp, [B][upInH][upInW][upC], read at the nearest coarse pixel
+        // (min(y/2, upInH-1), min(x/2, upInW-1)); the other Cg - upC from x, whose pixels
+        // then hold Cg - upC channels; null = off
+        const __nv_bfloat16* xUp;
+        int upC, upInH, upInW;
     };
 
     // bilinear x2 of a half-size RGBA8 frame at full-size pixel (X, Y), aligned with the
@@ -76,7 +73,7 @@ namespace isaacb
     };
 
     size_t conv_gemm_smem(int Npad, int Kpad);
-    // the row-tile kernel takes this convolution (and then honours wStride, upPart, frameOut)
+    // the row-tile kernel takes this convolution (and then honours xUp)
     bool row_tiles_apply(const ConvGemmParams& p);
     size_t conv_wgrad_smem(int Npad);
     bool launch_conv_gemm(const ConvGemmParams& p, cudaStream_t s);

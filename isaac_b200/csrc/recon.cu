@@ -285,6 +285,28 @@ namespace
         }
     }
 
+    // the reconstructed full-size frame, RGBA8 (round to nearest, clamped): bilinear x2 of
+    // the half-size frame plus the pixel-shuffled residual (4 channels per full-size pixel)
+    __global__ void k_frame(const uint8_t* __restrict__ low, const float* __restrict__ r, uint8_t* __restrict__ out, int h, int w)
+    {
+        const size_t n = size_t(h) * w;
+        for(size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        {
+            const int x = int(i % w), y = int(i / w);
+            const uchar4* lo = reinterpret_cast<const uchar4*>(low);
+            const float4* rp = reinterpret_cast<const float4*>(r + i * 16);
+#pragma unroll
+            for(int s = 0; s < 4; ++s)
+            {
+                const int X = 2 * x + (s & 1), Y = 2 * y + (s >> 1);
+                const float4 bl = bilinear2(lo, h, w, X, Y);
+                const float4 q = rp[s];
+                reinterpret_cast<uchar4*>(out)[size_t(Y) * (2 * w) + X]
+                    = make_uchar4(unit_byte(bl.x + q.x), unit_byte(bl.y + q.y), unit_byte(bl.z + q.z), unit_byte(bl.w + q.w));
+            }
+        }
+    }
+
     // the method without the network: bilinear x2 alone, RGBA8
     __global__ void k_bilinear_frame(const uint8_t* __restrict__ low, uint8_t* __restrict__ out, int h, int w)
     {
@@ -438,7 +460,6 @@ struct isaacb_recon
     bf16* act[kLayers] = {}; // outputs (OUT: unused, see r)
     bf16* dpre[kLayers] = {}; // gradient with respect to each layer's pre-activation output
     bf16* cat[kLayers] = {}; // concatenated inputs
-    float* upPart = nullptr; // inference: W_coarse * coarse of a concatenating layer, FP32
     bf16* dcat = nullptr; // gradient of a concatenated input (largest one)
     bf16* x = nullptr;
     float* r = nullptr; // OUT, FP32
@@ -564,12 +585,10 @@ namespace
         return true;
     }
 
-    // One image, inference only.  A concatenating 1x1 layer runs as two GEMMs: W_coarse *
-    // coarse at the coarse level into FP32, then W_fine * fine with that partial, upsampled
-    // to the nearest coarse pixel, added before the bias-and-ReLU (a 1x1 convolution
-    // commutes with nearest upsampling), so the concatenated tensor is never formed.  The
-    // output layer writes the RGBA8 frame (bilinear x2 + residual) in its epilogue.  The
-    // sums are the training forward's, in another order (FP32).
+    // One image, inference only.  A concatenating 1x1 layer reads its two inputs in place:
+    // the row-tile producer gathers the coarse tensor's channels at the nearest coarse
+    // pixel and the fine tensor's after them, which is [up(coarse), fine] without the
+    // concatenated tensor ever being formed.  The sums are the training forward's.
     bool forward_infer(isaacb_recon* R, const uint8_t* low, uint8_t* out, cudaStream_t s)
     {
         for(int L = 0; L < kLayers; ++L)
@@ -577,40 +596,29 @@ namespace
             const LayerDef& d = kDefs[L];
             if(d.src == -2)
             {
+                // [up(coarse), fine] read in place by the producer (implicit concatenation)
                 const int lf = kLevel[d.fine], lc = kLevel[d.coarse];
-                const int c1 = kDefs[d.coarse].cout, c2 = kDefs[d.fine].cout;
-                ConvGemmParams pc{};
-                pc.x = R->act[d.coarse];
-                pc.w = R->wf[L];
-                pc.wStride = R->T.Kpad[L];
-                pc.yf = R->upPart;
-                pc.B = 1;
-                pc.H = pc.Ho = R->lh[lc];
-                pc.W = pc.Wo = R->lw[lc];
-                pc.Cg = c1;
-                pc.Cout = d.cout;
-                pc.Npad = R->T.Npad[L];
-                pc.Kpad = round_up(c1, 64);
-                pc.ks = 1;
-                pc.stride = 1;
-                pc.errorFlag = R->errorFlag;
-                ConvGemmParams pf = pc;
-                pf.x = R->act[d.fine];
-                pf.w = R->wf[L] + c1;
-                pf.yf = nullptr;
-                pf.y = R->act[L];
-                pf.bias = R->bias[L];
-                pf.relu = d.relu;
-                pf.H = pf.Ho = R->lh[lf];
-                pf.W = pf.Wo = R->lw[lf];
-                pf.Cg = c2;
-                pf.Kpad = round_up(c2, 64);
-                pf.upPart = R->upPart;
-                pf.upH = R->lh[lc];
-                pf.upW = R->lw[lc];
-                if(!row_tiles_apply(pc) || !row_tiles_apply(pf))
-                    return false;
-                if(!launch_conv_gemm(pc, s) || !launch_conv_gemm(pf, s))
+                ConvGemmParams p{};
+                p.x = R->act[d.fine];
+                p.xUp = R->act[d.coarse];
+                p.upC = kDefs[d.coarse].cout;
+                p.upInH = R->lh[lc];
+                p.upInW = R->lw[lc];
+                p.w = R->wf[L];
+                p.bias = R->bias[L];
+                p.y = R->act[L];
+                p.B = 1;
+                p.H = p.Ho = R->lh[lf];
+                p.W = p.Wo = R->lw[lf];
+                p.Cg = R->T.cg[L];
+                p.Cout = d.cout;
+                p.Npad = R->T.Npad[L];
+                p.Kpad = R->T.Kpad[L];
+                p.ks = 1;
+                p.stride = 1;
+                p.relu = d.relu;
+                p.errorFlag = R->errorFlag;
+                if(p.Cg != d.cin || !row_tiles_apply(p) || !launch_conv_gemm(p, s))
                     return false;
                 continue;
             }
@@ -630,12 +638,10 @@ namespace
                 p.ks = 1;
                 p.stride = 1;
                 p.errorFlag = R->errorFlag;
-                p.frameOut = out;
-                p.frameLow = low;
-                if(d.cout != 16 || !row_tiles_apply(p))
-                    return false;
+                p.yf = R->r;
                 if(!launch_conv_gemm(p, s))
                     return false;
+                k_frame<<<grid_for(size_t(R->lh[0]) * R->lw[0]), 256, 0, s>>>(low, R->r, out, R->lh[0], R->lw[0]);
                 continue;
             }
             if(!conv_layer(R, L, 1, s))
@@ -796,7 +802,7 @@ extern "C"
         level_sizes(R->maxH, R->maxW, mh, mw);
         bool ok = true;
         int off = 0;
-        size_t maxCat = 0, maxUp = 0;
+        size_t maxCat = 0;
         for(int L = 0; L < kLayers && ok; ++L)
         {
             const LayerDef& d = kDefs[L];
@@ -825,7 +831,6 @@ extern "C"
             {
                 ok = ok && dalloc(R, R->cat[L], pix * d.cin);
                 maxCat = std::max(maxCat, pix * d.cin);
-                maxUp = std::max(maxUp, size_t(R->maxBatch) * mh[kLevel[d.coarse]] * mw[kLevel[d.coarse]] * d.cout);
             }
             if(ok && conv_gemm_smem(R->T.Npad[L], R->T.Kpad[L]) > 227 * 1024)
                 ok = false;
@@ -834,7 +839,6 @@ extern "C"
         R->total = off;
         const size_t pix0 = size_t(R->maxBatch) * mh[0] * mw[0];
         ok = ok && dalloc(R, R->dcat, maxCat) && dalloc(R, R->x, pix0 * 16) && dalloc(R, R->r, pix0 * 16);
-        ok = ok && dalloc(R, R->upPart, maxUp);
         ok = ok && dalloc(R, R->master, size_t(off)) && dalloc(R, R->adamM, size_t(off)) && dalloc(R, R->adamV, size_t(off));
         ok = ok && dalloc(R, R->lossSum, 1) && dalloc(R, R->gradHost, size_t(off)) && dalloc(R, R->sqErr, 1) && dalloc(R, R->errorFlag, 1);
         if(!ok)

@@ -114,14 +114,13 @@ namespace isaacb
             bool abortLocal = false, aborted = false;
             // the whole packed weight matrix, canonical K-major: core (n/8, k/8) at (n/8)*Kpad*16 + (k/8)*128
             {
-                const size_t wStride = p.wStride ? size_t(p.wStride) : size_t(p.Kpad);
                 const int kb = p.Kpad / 8;
                 const int pieces = p.Npad * kb;
                 for(int i = tid; i < pieces; i += kThreads)
                 {
                     const int n = i / kb, k8 = i - n * kb;
                     const uint32_t dst = sB + uint32_t(n >> 3) * uint32_t(p.Kpad) * 16u + uint32_t(k8) * 128u + uint32_t(n & 7) * 16u;
-                    tc::cp_async16(dst, p.w + size_t(n) * wStride + size_t(k8) * 8, 16);
+                    tc::cp_async16(dst, p.w + size_t(n) * p.Kpad + size_t(k8) * 8, 16);
                 }
                 tc::cp_async_commit();
                 tc::cp_async_wait<0>();
@@ -388,8 +387,7 @@ namespace isaacb
 
         // Epilogue of one 128-pixel output tile (row y of image b, column tile xt): this
         // thread's pixel px, accumulator columns [cBeg, cBeg + colsPer) of the TMEM tile at
-        // tAcc (this warp's lanes); bias, the upsampled coarse partial, ReLU, mask, then the
-        // bf16 / FP32 store or the RGBA8 frame.
+        // tAcc (this warp's lanes); bias, ReLU, mask, then the bf16 / FP32 store.
         __device__ __forceinline__ void row_epilogue(
             const ConvGemmParams& p,
             uint32_t tAcc,
@@ -404,10 +402,6 @@ namespace isaacb
             const int x = xt * kTileM + px;
             const bool valid = x < p.Wo;
             const size_t pix = (size_t(b) * p.Ho + y) * p.Wo + x;
-            const float* up = nullptr;
-            if(p.upPart && valid)
-                up = p.upPart
-                    + ((size_t(b) * p.upH + min(y >> 1, p.upH - 1)) * p.upW + min(x >> 1, p.upW - 1)) * p.Cout;
             // 16 accumulator columns per TMEM wait (8 where a column group ends)
             for(int c16 = cBeg; c16 < cBeg + colsPer; c16 += 16)
             {
@@ -434,13 +428,6 @@ namespace isaacb
                         for(int k = 0; k < 8; ++k)
                             w[k] += sBias[c0 + k];
                     }
-                    if(up)
-                    {
-                        const float4 u0 = __ldg(reinterpret_cast<const float4*>(up + c0));
-                        const float4 u1 = __ldg(reinterpret_cast<const float4*>(up + c0) + 1);
-                        w[0] += u0.x, w[1] += u0.y, w[2] += u0.z, w[3] += u0.w;
-                        w[4] += u1.x, w[5] += u1.y, w[6] += u1.z, w[7] += u1.w;
-                    }
                     if(p.relu)
                     {
 #pragma unroll
@@ -455,23 +442,7 @@ namespace isaacb
                         for(int k = 0; k < 8; ++k)
                             w[k] = mk[k] > 0.0f ? w[k] : 0.0f;
                     }
-                    if(p.frameOut)
-                    {
-                        // channels 4s..4s+3 are the residual of full-size pixel s of the
-                        // 2x2 block: X = 2x + (s & 1), Y = 2y + (s >> 1)
-                        const uchar4* lo = reinterpret_cast<const uchar4*>(p.frameLow) + size_t(b) * p.Ho * p.Wo;
-                        uchar4* fo = reinterpret_cast<uchar4*>(p.frameOut) + size_t(b) * 4 * p.Ho * p.Wo;
-#pragma unroll
-                        for(int q = 0; q < 2; ++q)
-                        {
-                            const int sp = c0 / 4 + q;
-                            const int X = 2 * x + (sp & 1), Y = 2 * y + (sp >> 1);
-                            const float4 bl = bilinear2_rgba(lo, p.Ho, p.Wo, X, Y);
-                            fo[size_t(Y) * (2 * p.Wo) + X] = make_uchar4(unit_byte(bl.x + w[4 * q]), unit_byte(bl.y + w[4 * q + 1]),
-                                                                         unit_byte(bl.z + w[4 * q + 2]), unit_byte(bl.w + w[4 * q + 3]));
-                        }
-                    }
-                    else if(p.yf)
+                    if(p.yf)
                     {
                         float4* dst = reinterpret_cast<float4*>(p.yf + o);
                         if(p.accumulate)
@@ -540,14 +511,13 @@ namespace isaacb
                 tc::mbar_init_fence();
             }
             {
-                const size_t wStride = p.wStride ? size_t(p.wStride) : size_t(p.Kpad);
                 const int kb = p.Kpad / 8;
                 const int pieces = p.Npad * kb;
                 for(int i = tid; i < pieces; i += row_threads<TMA>())
                 {
                     const int n = i / kb, k8 = i - n * kb;
                     const uint32_t dst = sB + uint32_t(n >> 3) * uint32_t(p.Kpad) * 16u + uint32_t(k8) * 128u + uint32_t(n & 7) * 16u;
-                    tc::cp_async16(dst, p.w + size_t(n) * wStride + size_t(k8) * 8, 16);
+                    tc::cp_async16(dst, p.w + size_t(n) * p.Kpad + size_t(k8) * 8, 16);
                 }
                 tc::cp_async_commit();
                 // the per-channel bias, read by every epilogue thread for every pixel
@@ -648,7 +618,14 @@ namespace isaacb
                     {
                         const int iy = p.transposed ? y + pad - ty : S * y - pad + ty;
                         const bool rowOk = iy >= 0 && iy < p.H;
-                        const bf16* rowPtr = p.x + (size_t(b) * p.H + (rowOk ? iy : 0)) * p.W * p.Cg;
+                        // implicit concatenation: chunks below nUp come from the coarse tensor at
+                        // the nearest coarse pixel, the rest from x, whose pixels hold cX channels
+                        const int nUp = p.xUp ? p.upC / 8 : 0;
+                        const int cX = p.Cg - 8 * nUp;
+                        const bf16* rowPtr = p.x + (size_t(b) * p.H + (rowOk ? iy : 0)) * p.W * cX;
+                        const bf16* upRow = p.xUp
+                            ? p.xUp + (size_t(b) * p.upInH + min((rowOk ? iy : 0) >> 1, p.upInH - 1)) * p.upInW * p.upC
+                            : nullptr;
                         const uint32_t rowBase = st + uint32_t(ty * nC * S) * runBytes;
                         int j = pt % nC, c = pt / nC;
                         for(int g = pt; g < perRow; g += 128)
@@ -656,7 +633,9 @@ namespace isaacb
                             const int ix = S * x0 - pad + c;
                             const int q = c & (S - 1), idx = S == 1 ? c : (c >> 1);
                             const bool ok = rowOk && ix >= 0 && ix < p.W;
-                            const bf16* src = ok ? rowPtr + size_t(ix) * p.Cg + j * 8 : p.x;
+                            const bf16* src = !ok ? p.x
+                                : j < nUp ? upRow + size_t(min(ix >> 1, p.upInW - 1)) * p.upC + j * 8
+                                          : rowPtr + size_t(ix) * cX + (j - nUp) * 8;
                             tc::cp_async16(rowBase + uint32_t(j * S + q) * runBytes + uint32_t(idx) * 16u, src, ok ? 16u : 0u);
                             j += dj;
                             c += dc;
@@ -945,6 +924,8 @@ namespace isaacb
 
     bool row_tiles_apply(const ConvGemmParams& p)
     {
+        if(p.xUp && (p.ks != 1 || p.stride != 1 || p.upC % 8 != 0 || p.transposed))
+            return false;
         return p.Cg % 16 == 0 && p.Npad <= 256
             && ((p.stride == 1 && 2 * p.pad == p.ks - 1) || (p.stride == 2 && !p.transposed && p.ks <= 3 && p.pad <= 1));
     }
@@ -1034,7 +1015,7 @@ namespace isaacb
             if(conv_row_smem(p, stages, true) <= 227 * 1024)
             {
                 CUtensorMap m{};
-                if(g_rowTma && encode_row_map(p, row_geom(p.stride, p.ks, p.pad, stages, true), m))
+                if(g_rowTma && !p.xUp && encode_row_map(p, row_geom(p.stride, p.ks, p.pad, stages, true), m))
                     launch_row<true>(p, stages, m, s);
                 else
                     launch_row<false>(p, stages, m, s);
