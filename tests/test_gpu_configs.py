@@ -242,3 +242,89 @@ def test_zz_error_table():
             json.dump(TABLE, f, indent=1)
     if len(TABLE) < 6:
         pytest.skip(f"only {sorted(TABLE)} ran")
+
+
+# --------------------------------------------------------------------- batching, 16 views x 4 timesteps of 4 x 512^3
+def test_batch_16_views_at_config_size():
+    """The batching configuration at full size: 16 views of uneven resolution over 4
+    advected timesteps of the four 512^3 sources, in one persistent launch and as a
+    captured graph.  Every view equals the single-view render of its timestep's context
+    bit for bit, and a 256x256 view is within the parity bar of the oracle."""
+    import argparse
+
+    import bench
+    from isaac_b200 import scenes
+    from isaac_b200.batch import IsaacBatch
+
+    args = argparse.Namespace(scene="batch", size=512, sources=4, width=1920, height=1080, timesteps=4, shift=0.05,
+                              renderer="combined", dtype="f32", learned_renderer="per_source", ao_samples=0,
+                              ao_radius=8.0)
+    small = bench._small(args)
+    steps_sc = bench.build_batch_scenes(args, "cuda")
+    vis = [bench.make_viz(small, sc) for sc in steps_sc]
+    views = scenes.batch_views(timesteps=args.timesteps)
+    batch = IsaacBatch(vis, views)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        batch.render(update=True)
+        batch.capture(update=True)
+        batch.launchGraph()
+    stream.synchronize()
+    for i, (t, w, h, P, MV) in enumerate(views):
+        single = bench.make_viz(argparse.Namespace(**{**vars(small), "width": w, "height": h}), steps_sc[t])
+        single.setCamera(P, MV)
+        ref = single.doVisualization()
+        assert np.array_equal(batch.frames[i].cpu().numpy(), ref), i
+        if i == 0:
+            # the oracle on the same timestep's sources, 256x256
+            from harness import Scene
+
+            s = Scene(n=(512, 512, 512), fb=(w, h), volumes=[(f.cpu().numpy(), True) for f, _ in steps_sc[t].volumes])
+            s.transfer = list(steps_sc[t].transfer)
+            s.P, s.MV = P, MV
+            o = build_oracle(s)
+            assert_image_parity(ref, o.frame())
+            o.close()
+        single.close()
+    batch.close()
+    for v in vis:
+        v.close()
+
+
+# --------------------------------------------------------------------- learned reconstruction at 1920x1080
+@pytest.mark.parametrize("renderer", ["per_source", "combined"])
+def test_learned_path_at_config_size(renderer):
+    """The learned configuration at full size: the four 512^3 sources, 960x540 at step
+    1.0 reconstructed to 1920x1080 by the committed network, judged against the plain
+    1920x1080 step-0.5 render on an orbit of cameras: every frame at or above 40 dB (no
+    fallback) and the network at least as close as bilinear x2 on average."""
+    import math
+
+    from isaac_b200 import recon, scenes
+    from isaac_b200.recon_train import PairRenderer
+
+    W, H = 1920, 1080
+    pr = PairRenderer(512, W, H, renderer=renderer)
+    pr.set_timestep(0)
+    tfs = [scenes.transfer_4point(0.7 * i) for i in range(4)]
+    cams = [scenes.orbit_camera(W, H, yaw=2 * math.pi * k / 8.0, pitch=0.35, distance=2.4) for k in range(8)]
+    pr.set_view(*cams[0], tfs)
+    pr.full.update()
+    pr.low.update()
+    net = recon.Reconstructor(1, H // 2, W // 2, seed=1)
+    net.load(recon.weights_for(renderer))
+    jr = recon.JudgedRenderer(pr.full, pr.low, net, judge_every=1, threshold=40.0)
+    tmp = torch.empty((H, W, 4), dtype=torch.uint8, device="cuda")
+    gains = []
+    for P, MV in cams:
+        jr.setCamera(P, MV)
+        jr.frame()
+        p_rec = jr.judged[-1][1]
+        gains.append(p_rec - recon.psnr(recon.bilinear2(jr.half, tmp), jr.full))
+        assert p_rec >= 40.0, jr.judged
+    assert jr.fallback_frames == 0
+    assert float(np.mean(gains)) > 0.0, gains
+    assert net.error_flag() == 0
+    net.close()
+    for v in (pr.full, pr.low):
+        v.close()
