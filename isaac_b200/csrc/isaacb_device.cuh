@@ -644,12 +644,17 @@ namespace isaacb
     {
         return f2p_fma(a, b, negZero);
     }
-    // bytes (c, c+1) of w as an exact float pair: 2^23 + b bit patterns minus 2^23
-    __device__ __forceinline__ f2p ubyte_pair(uint32_t w, int c, f2p bias)
+    // bytes (c, c+1) of w as the exact float pair (b_c 2^-133, b_c+1 2^-133): the byte
+    // in bits 16-23 and zeros elsewhere, one byte permute per value and no add.  Below
+    // 128 the value is subnormal, from 128 on bit 23 is the exponent's lowest bit and
+    // the value is normal, and in both ranges it equals b 2^-133; zero stays zero.  The
+    // packed fma (no .ftz) takes subnormal operands as they are; with weights scaled by
+    // 2^64 every product and sum is a normal number, each the unscaled one times 2^-69.
+    __device__ __forceinline__ f2p ubyte_pair_tiny(uint32_t w, int c)
     {
-        const float lo = __int_as_float(int(__byte_perm(w, 0x4B000000u, 0x7440u + unsigned(c))));
-        const float hi = __int_as_float(int(__byte_perm(w, 0x4B000000u, 0x7440u + unsigned(c + 1))));
-        return f2p_add(f2p_make(lo, hi), bias);
+        const float lo = __int_as_float(int(__byte_perm(w, 0u, 0x4044u + 256u * unsigned(c))));
+        const float hi = __int_as_float(int(__byte_perm(w, 0u, 0x4044u + 256u * unsigned(c + 1))));
+        return f2p_make(lo, hi);
     }
 
     // pixel of a thread: a block of 256 threads covers 32x8 pixels and each warp an 8x4 tile

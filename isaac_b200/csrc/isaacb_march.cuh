@@ -35,6 +35,8 @@ namespace isaacb
     {
         const Geom& g = p.g;
         const float k = factor / 255.0f;
+        // trilinear samples come out scaled by 2^-69 (see the tap loop); 2^69 k is exact
+        const float kS = LINEAR ? k * 0x1p69f : k;
         const float off = LINEAR ? 0.5f : 0.0f;
         const float c0x = m.startU.x - off, c0y = m.startU.y - off, c0z = m.startU.z - off;
         const float svx = m.stepVec.x, svy = m.stepVec.y, svz = m.stepVec.z;
@@ -96,19 +98,25 @@ namespace isaacb
                 const uint4 A = __ldg(p.volQ + slot);
                 const uint4 B = __ldg(p.volQ + slot + 64);
                 const float fx = cx - (tx - 12582912.0f), fy = cy - (ty - 12582912.0f), fz = cz - (tz - 12582912.0f);
-                const float gx = 1.0f - fx, gy = 1.0f - fy, gz = 1.0f - fz;
+                // the z weights carry a factor 2^64 (exact: 2^64 - 2^64 fz is 1 - fz
+                // rounded, then scaled), so all eight weights are the unscaled ones times 2^64
+                const float fz64 = fz * 0x1p64f;
+                const float gx = 1.0f - fx, gy = 1.0f - fy, gz64 = 0x1p64f - fz64;
                 const float w00 = gx * gy, w10 = fx * gy, w01 = gx * fy, w11 = fx * fy;
-                const float wt[8] = {w00 * gz, w10 * gz, w01 * gz, w11 * gz, w00 * fz, w10 * fz, w01 * fz, w11 * fz};
+                const float wt[8] = {w00 * gz64, w10 * gz64, w01 * gz64, w11 * gz64,
+                                     w00 * fz64, w10 * fz64, w01 * fz64, w11 * fz64};
                 const uint32_t tap[8] = {A.x, A.y, A.z, A.w, B.x, B.y, B.z, B.w};
-                // (r,g) and (b,a) accumulate as packed FP32 pairs, one FFMA2 each per tap
-                const f2p bias = f2p_make(-8388608.0f, -8388608.0f);
+                // (r,g) and (b,a) accumulate as packed FP32 pairs, one FFMA2 each per tap,
+                // over the bytes as b 2^-133 (one byte permute, no bias add): every product
+                // and partial sum is the unscaled one times 2^-69, rounded the same way,
+                // and the 2^69 goes into the compositing factor
                 f2p rg = f2p_make(0.0f, 0.0f), ba = f2p_make(0.0f, 0.0f);
 #pragma unroll
                 for(int k = 0; k < 8; ++k)
                 {
                     const f2p wk = f2p_make(wt[k], wt[k]);
-                    rg = f2p_fma(ubyte_pair(tap[k], 0, bias), wk, rg);
-                    ba = f2p_fma(ubyte_pair(tap[k], 2, bias), wk, ba);
+                    rg = f2p_fma(ubyte_pair_tiny(tap[k], 0), wk, rg);
+                    ba = f2p_fma(ubyte_pair_tiny(tap[k], 2), wk, ba);
                 }
                 f2p_split(rg, r0, r1);
                 f2p_split(ba, r2, r3);
@@ -118,7 +126,7 @@ namespace isaacb
                 const uint32_t w = __ldg(q32 + size_t(slot) * 4);
                 r0 = ubyte_f(w, 0), r1 = ubyte_f(w, 1), r2 = ubyte_f(w, 2), r3 = ubyte_f(w, 3);
             }
-            const float s = (1.0f - color.w) * k;
+            const float s = (1.0f - color.w) * kS;
             color.x = fmaf(s, r0, color.x);
             color.y = fmaf(s, r1, color.y);
             color.z = fmaf(s, r2, color.z);
