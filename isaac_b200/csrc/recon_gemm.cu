@@ -372,6 +372,7 @@ namespace isaacb
             int HWp; // entries between runs (per parity plane for stride 2)
             int HWn; // entries a run needs (<= HWp; HWp is padded to 8 for TMA destinations)
             int stages; // halo buffers: 1 or 2
+            int rowB; // swizzled staging: bytes per staged pixel (Cg * 2 = 32, 64 or 128); 0 = chunked runs
         };
 
         __host__ __device__ inline RowGeom row_geom(int stride, int ks, int pad, int stages, bool tma = false)
@@ -382,6 +383,7 @@ namespace isaacb
             // a TMA destination starts on a 128-byte boundary: runs of a multiple of 8 entries
             g.HWp = tma ? (g.HWn + 7) / 8 * 8 : g.HWn;
             g.stages = stages;
+            g.rowB = 0;
             return g;
         }
 
@@ -489,8 +491,14 @@ namespace isaacb
             const int pad = p.pad, ks = p.ks, S = rg.S, HWp = rg.HWp, NS = rg.stages;
             const int nC = p.Cg / 8;
             const uint32_t runBytes = uint32_t(HWp) * 16u;
-            const uint32_t haloBytes = uint32_t(ks * nC * S) * runBytes;
-            const uint32_t sH = sB + uint32_t(p.Npad) * uint32_t(p.Kpad) * 2u;
+            // swizzled staging: each input row is HWp pixels of rowB bytes, the row buffers
+            // and the halo start on multiples of the swizzle pattern's period (8 rows)
+            const int rowB = rg.rowB;
+            const uint32_t swSpan = 8u * uint32_t(rowB);
+            const uint32_t rowPitch = rowB ? (uint32_t(HWp * rowB) + swSpan - 1u) / swSpan * swSpan : 0u;
+            const uint32_t haloBytes = rowB ? uint32_t(ks * S) * rowPitch : uint32_t(ks * nC * S) * runBytes;
+            const uint32_t wEnd = sB + uint32_t(p.Npad) * uint32_t(p.Kpad) * 2u;
+            const uint32_t sH = rowB ? (wEnd + swSpan - 1u) / swSpan * swSpan : wEnd;
             const uint32_t half = tmem_columns(p.Npad);
             const uint32_t cols = 2 * half;
             if(warp == 0)
@@ -551,10 +559,13 @@ namespace isaacb
                 // one box per run.  Stride 1: map (C, W, H, B), box (8, HWn, 1, 1) at
                 // (8j, x0 - pad, row, b).  Stride 2: map (C, 2, W/2, H, B), the column split
                 // into its parity and half, box (8, 1, HWn, 1, 1) at (8j, c & 1, c >> 1, row,
-                // b) with c = 2*x0 - pad + q.  Rows and columns outside the image read zeros.
+                // b) with c = 2*x0 - pad + q.  Swizzled staging (16-64 channels): one box of
+                // all channels per run, (C, HWp, 1, 1) at (0, x0 - pad, row, b) or
+                // (C, 1, HWp, 1, 1) at (0, c & 1, c >> 1, row, b), written with the map's
+                // 32/64/128-byte swizzle.  Rows and columns outside the image read zeros.
                 if(lane == 0)
                 {
-                    const uint32_t txBytes = uint32_t(ks * nC * S * rg.HWn) * 16u;
+                    const uint32_t txBytes = rowB ? uint32_t(ks * S * HWp * rowB) : uint32_t(ks * nC * S * rg.HWn) * 16u;
                     int i = 0;
                     for(int tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++i)
                     {
@@ -574,6 +585,19 @@ namespace isaacb
                         for(int ty = 0; ty < ks; ++ty)
                         {
                             const int iy = p.transposed ? y + pad - ty : S * y - pad + ty;
+                            if(rowB)
+                            {
+                                if(S == 1)
+                                    tc::tma_load_4d(st + uint32_t(ty) * rowPitch, &tmap, 0, x0 - pad, iy, b, &sFull[s]);
+                                else
+                                    for(int q = 0; q < 2; ++q)
+                                    {
+                                        const int c = 2 * x0 - pad + q;
+                                        tc::tma_load_5d(st + uint32_t(ty * 2 + q) * rowPitch, &tmap, 0, c & 1, c >> 1, iy, b,
+                                                        &sFull[s]);
+                                    }
+                                continue;
+                            }
                             for(int j = 0; j < nC; ++j)
                                 for(int q = 0; q < S; ++q)
                                 {
@@ -678,6 +702,32 @@ namespace isaacb
                         const uint64_t aBase = tc::smem_desc(st, lboA, 128u);
                         const uint64_t bBase = tc::smem_desc(sB, 128u, sboB);
                         uint32_t acc = 0;
+                        if(rowB)
+                        {
+                            // K-major A with the rows' own swizzle (layout 6 / 4 / 2 = 32 / 64 /
+                            // 128 bytes), 8-row groups swSpan apart; tap (ty, tx) starts idx0 rows
+                            // into run (ty, q) and each K step of 16 channels 32 bytes further.
+                            // The swizzle follows the absolute shared-memory address, as the TMA
+                            // copy wrote it, so the base-offset field stays 0.
+                            const uint64_t swDesc = (tc::smem_desc(0, 16u, swSpan) & ~uint64_t(0x3FFF))
+                                | (uint64_t(rowB == 32 ? 6 : rowB == 64 ? 4 : 2) << 61);
+                            for(int ty = 0; ty < ks; ++ty)
+                                for(int tx = 0; tx < ks; ++tx)
+                                {
+                                    const int col = p.transposed ? 2 * pad - tx : tx;
+                                    const int q = col & (S - 1), idx0 = S == 1 ? col : (col >> 1);
+                                    uint32_t addr = st + uint32_t(ty * S + q) * rowPitch + uint32_t(idx0 * rowB);
+                                    uint32_t bOff = uint32_t((ty * ks + tx) * p.Cg);
+                                    for(int jp = 0; jp < nC / 2; ++jp)
+                                    {
+                                        tc::mma_bf16(d, swDesc | uint64_t((addr >> 4) & 0x3FFFu), bBase + bOff, idesc, acc);
+                                        acc = 1;
+                                        addr += 32u;
+                                        bOff += 16u;
+                                    }
+                                }
+                        }
+                        else
                         for(int ty = 0; ty < ks; ++ty)
                             for(int tx = 0; tx < ks; ++tx)
                             {
@@ -929,9 +979,23 @@ namespace isaacb
         return p.Cg % 16 == 0 && p.Npad <= 256
             && ((p.stride == 1 && 2 * p.pad == p.ks - 1) || (p.stride == 2 && !p.transposed && p.ks <= 3 && p.pad <= 1));
     }
+    // Swizzled staging for the TMA producer: 16, 32 or 64 channels, each run (an input row,
+    // or one parity plane of it at stride 2) one box of Cg * 2-byte pixels, instead of one
+    // box per 8-channel chunk (the narrow chunk boxes kept the copy engine busy).  Returns
+    // the bytes per staged pixel, 0 where the chunked runs are used.
+    inline int swizzle_row_bytes(const ConvGemmParams& p)
+    {
+        return (p.Cg == 16 || p.Cg == 32 || p.Cg == 64) ? p.Cg * 2 : 0;
+    }
     size_t conv_row_smem(const ConvGemmParams& p, int stages, bool tma = false)
     {
         const RowGeom g = row_geom(p.stride, p.ks, p.pad, stages, tma);
+        const int rowB = tma ? swizzle_row_bytes(p) : 0;
+        if(rowB)
+        {
+            const size_t span = size_t(8) * rowB, pitch = (size_t(g.HWp) * rowB + span - 1) / span * span;
+            return size_t(p.Npad) * p.Kpad * 2 + span + size_t(stages) * p.ks * g.S * pitch + 128;
+        }
         return size_t(p.Npad) * p.Kpad * 2 + size_t(stages) * p.ks * (p.Cg / 8) * g.S * g.HWp * 16 + 128;
     }
 
@@ -963,7 +1027,33 @@ namespace isaacb
             const cuuint64_t C = cuuint64_t(p.Cg), W = cuuint64_t(p.W), H = cuuint64_t(p.H), B = cuuint64_t(p.B);
             cuuint32_t estr[5] = {1, 1, 1, 1, 1};
             CUresult r;
-            if(g.S == 1)
+            if(g.rowB)
+            {
+                const CUtensorMapSwizzle sw = g.rowB == 32 ? CU_TENSOR_MAP_SWIZZLE_32B
+                    : g.rowB == 64                         ? CU_TENSOR_MAP_SWIZZLE_64B
+                                                           : CU_TENSOR_MAP_SWIZZLE_128B;
+                if(g.S == 1)
+                {
+                    cuuint64_t dims[4] = {C, W, H, B};
+                    cuuint64_t strides[3] = {C * 2, W * C * 2, H * W * C * 2};
+                    cuuint32_t box[4] = {cuuint32_t(C), cuuint32_t(g.HWp), 1, 1};
+                    r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(p.x), dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                }
+                else
+                {
+                    if(p.W % 2 != 0)
+                        return false; // the parity split views W as (W/2, 2)
+                    cuuint64_t dims[5] = {C, 2, W / 2, H, B};
+                    cuuint64_t strides[4] = {C * 2, 2 * C * 2, W * C * 2, H * W * C * 2};
+                    cuuint32_t box[5] = {cuuint32_t(C), 1, cuuint32_t(g.HWp), 1, 1};
+                    r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16*>(p.x), dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                }
+            }
+            else if(g.S == 1)
             {
                 cuuint64_t dims[4] = {C, W, H, B};
                 cuuint64_t strides[3] = {C * 2, W * C * 2, H * W * C * 2};
@@ -987,7 +1077,7 @@ namespace isaacb
         }
 
         template<bool TMA>
-        void launch_row(const ConvGemmParams& p, int stages, const CUtensorMap& m, cudaStream_t s)
+        void launch_row(const ConvGemmParams& p, int stages, const CUtensorMap& m, cudaStream_t s, int rowB = 0)
         {
             const size_t smem = conv_row_smem(p, stages, TMA);
             cudaFuncSetAttribute(k_conv_row<TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
@@ -997,10 +1087,9 @@ namespace isaacb
             while(perSm > 1 && perSm * 2 * int(tmem_columns(p.Npad)) > 512)
                 --perSm;
             const int slots = num_sms() * perSm;
-            k_conv_row<TMA><<<tiles < slots ? tiles : slots, row_threads<TMA>(), smem, s>>>(
-                p,
-                row_geom(p.stride, p.ks, p.pad, stages, TMA),
-                m);
+            RowGeom g = row_geom(p.stride, p.ks, p.pad, stages, TMA);
+            g.rowB = TMA ? rowB : 0;
+            k_conv_row<TMA><<<tiles < slots ? tiles : slots, row_threads<TMA>(), smem, s>>>(p, g, m);
         }
     } // namespace
 
@@ -1015,8 +1104,10 @@ namespace isaacb
             if(conv_row_smem(p, stages, true) <= 227 * 1024)
             {
                 CUtensorMap m{};
-                if(g_rowTma && !p.xUp && encode_row_map(p, row_geom(p.stride, p.ks, p.pad, stages, true), m))
-                    launch_row<true>(p, stages, m, s);
+                RowGeom g = row_geom(p.stride, p.ks, p.pad, stages, true);
+                g.rowB = swizzle_row_bytes(p);
+                if(g_rowTma && !p.xUp && encode_row_map(p, g, m))
+                    launch_row<true>(p, stages, m, s, g.rowB);
                 else
                     launch_row<false>(p, stages, m, s);
                 return true;
