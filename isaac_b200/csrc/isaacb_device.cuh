@@ -650,6 +650,10 @@ namespace isaacb
     // the value is normal, and in both ranges it equals b 2^-133; zero stays zero.  The
     // packed fma (no .ftz) takes subnormal operands as they are; with weights scaled by
     // 2^64 every product and sum is a normal number, each the unscaled one times 2^-69.
+    __device__ __forceinline__ float ubyte_tiny(uint32_t w, int c)
+    {
+        return __int_as_float(int(__byte_perm(w, 0u, 0x4044u + 256u * unsigned(c))));
+    }
     __device__ __forceinline__ f2p ubyte_pair_tiny(uint32_t w, int c)
     {
         const float lo = __int_as_float(int(__byte_perm(w, 0u, 0x4044u + 256u * unsigned(c))));

@@ -184,17 +184,20 @@ namespace isaacb
             return ubyte_f(__ldg(p.isoAQ + slot), 0);
         const uint32_t A = __ldg(p.isoAQ + slot), B = __ldg(p.isoAQ + slot + 64);
         const float fx = cx - (tx - 12582912.0f), fy = cy - (ty - 12582912.0f), fz = cz - (tz - 12582912.0f);
-        const float gx = 1.0f - fx, gy = 1.0f - fy, gz = 1.0f - fz;
+        // bytes as b 2^-133 and z weights times 2^64 (ubyte_pair_tiny): each product and
+        // sum is the unscaled one times 2^-69, and the last multiply undoes it exactly
+        const float fz64 = fz * 0x1p64f;
+        const float gx = 1.0f - fx, gy = 1.0f - fy, gz64 = 0x1p64f - fz64;
         const float w00 = gx * gy, w10 = fx * gy, w01 = gx * fy, w11 = fx * fy;
-        float v = ubyte_f(A, 0) * (w00 * gz);
-        v = fmaf(ubyte_f(A, 1), w10 * gz, v);
-        v = fmaf(ubyte_f(A, 2), w01 * gz, v);
-        v = fmaf(ubyte_f(A, 3), w11 * gz, v);
-        v = fmaf(ubyte_f(B, 0), w00 * fz, v);
-        v = fmaf(ubyte_f(B, 1), w10 * fz, v);
-        v = fmaf(ubyte_f(B, 2), w01 * fz, v);
-        v = fmaf(ubyte_f(B, 3), w11 * fz, v);
-        return v;
+        float v = ubyte_tiny(A, 0) * (w00 * gz64);
+        v = fmaf(ubyte_tiny(A, 1), w10 * gz64, v);
+        v = fmaf(ubyte_tiny(A, 2), w01 * gz64, v);
+        v = fmaf(ubyte_tiny(A, 3), w11 * gz64, v);
+        v = fmaf(ubyte_tiny(B, 0), w00 * fz64, v);
+        v = fmaf(ubyte_tiny(B, 1), w10 * fz64, v);
+        v = fmaf(ubyte_tiny(B, 2), w01 * fz64, v);
+        v = fmaf(ubyte_tiny(B, 3), w11 * fz64, v);
+        return v * 0x1p69f;
     }
 
     // Interpolated alpha byte (0..255 scale) of the iso alpha quads at the reference's
