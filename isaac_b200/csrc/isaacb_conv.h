@@ -33,6 +33,10 @@ namespace isaacb
         // then hold Cg - upC channels; null = off
         const __nv_bfloat16* xUp;
         int upC, upInH, upInW;
+        // host launch hint (row-tile kernel): launch as a programmatic dependent of the
+        // stream's previous kernel, so that its CTAs load their weights while that kernel
+        // drains; the kernel reads its input only after griddepcontrol.wait
+        int pdl;
     };
 
     // bilinear x2 of a half-size RGBA8 frame at full-size pixel (X, Y), aligned with the

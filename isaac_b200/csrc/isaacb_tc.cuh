@@ -43,6 +43,19 @@ namespace isaacb
                 | (uint32_t(M >> 4) << 24);
         }
 
+        // ------------------------------------------------------------ programmatic dependent launch
+        // Wait until the grids this one depends on have completed and their writes are
+        // visible (returns at once for a kernel launched without the programmatic
+        // serialization attribute), and let the stream's next kernel start its launch.
+        __device__ __forceinline__ void grid_dependency_wait()
+        {
+            asm volatile("griddepcontrol.wait;" ::: "memory");
+        }
+        __device__ __forceinline__ void grid_launch_dependents()
+        {
+            asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+        }
+
         // ------------------------------------------------------------ TMEM
         __device__ __forceinline__ void tmem_alloc(uint32_t* dstSmem, uint32_t cols)
         {

@@ -105,6 +105,9 @@ namespace
     // and zeros, 16 channels (the parameters see the first 8; the GEMM wants multiples of 16)
     __global__ void k_input(const uint8_t* __restrict__ low, const int32_t* __restrict__ index, int B, int h, int w, bf16* __restrict__ x)
     {
+        // the first convolution may start loading its weights (it waits for this grid
+        // before reading x)
+        asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
         const size_t n = size_t(B) * h * w;
         for(size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
         {
@@ -289,6 +292,8 @@ namespace
     // the half-size frame plus the pixel-shuffled residual (4 channels per full-size pixel)
     __global__ void k_frame(const uint8_t* __restrict__ low, const float* __restrict__ r, uint8_t* __restrict__ out, int h, int w)
     {
+        // r comes from the output layer, which this kernel follows as a programmatic dependent
+        asm volatile("griddepcontrol.wait;" ::: "memory");
         const size_t n = size_t(h) * w;
         for(size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
         {
@@ -529,7 +534,7 @@ namespace
         return R->act[d.src];
     }
 
-    bool conv_layer(isaacb_recon* R, int L, int B, cudaStream_t s)
+    bool conv_layer(isaacb_recon* R, int L, int B, cudaStream_t s, bool pdl = false)
     {
         const LayerDef& d = kDefs[L];
         const int li = in_level(L), lo = kLevel[L];
@@ -555,6 +560,7 @@ namespace
         p.errorFlag = R->errorFlag;
         p.waitCheckNs = R->waitCheckNs;
         R->waitCheckNs = 0;
+        p.pdl = pdl ? 1 : 0;
         return launch_conv_gemm(p, s);
     }
 
@@ -618,6 +624,7 @@ namespace
                 p.stride = 1;
                 p.relu = d.relu;
                 p.errorFlag = R->errorFlag;
+                p.pdl = 1;
                 if(p.Cg != d.cin || !row_tiles_apply(p) || !launch_conv_gemm(p, s))
                     return false;
                 continue;
@@ -639,12 +646,26 @@ namespace
                 p.stride = 1;
                 p.errorFlag = R->errorFlag;
                 p.yf = R->r;
+                p.pdl = 1;
                 if(!launch_conv_gemm(p, s))
                     return false;
-                k_frame<<<grid_for(size_t(R->lh[0]) * R->lw[0]), 256, 0, s>>>(low, R->r, out, R->lh[0], R->lw[0]);
+                cudaLaunchConfig_t cfg{};
+                cfg.gridDim = dim3(unsigned(grid_for(size_t(R->lh[0]) * R->lw[0])));
+                cfg.blockDim = dim3(256);
+                cfg.stream = s;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                attr[0].val.programmaticStreamSerializationAllowed = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                const uint8_t* lowc = low;
+                const float* rc = R->r;
+                cudaLaunchKernelEx(&cfg, k_frame, lowc, rc, out, R->lh[0], R->lw[0]);
                 continue;
             }
-            if(!conv_layer(R, L, 1, s))
+            // the first layer follows k_input, a plain launch; the others each follow a
+            // row-tile convolution, launched as its programmatic dependent
+            if(!conv_layer(R, L, 1, s, true))
                 return false;
         }
         return true;

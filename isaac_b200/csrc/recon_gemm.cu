@@ -537,6 +537,10 @@ namespace isaacb
             tc::fence_before_sync();
             __syncthreads();
             tc::fence_after_sync();
+            // everything above (weights, bias, barriers, TMEM) is independent of the
+            // previous layer; its output is read only from here on
+            tc::grid_dependency_wait();
+            tc::grid_launch_dependents();
             const uint32_t tmem = sTmem;
             if(p.waitCheckNs != 0)
             {
@@ -1089,7 +1093,17 @@ namespace isaacb
             const int slots = num_sms() * perSm;
             RowGeom g = row_geom(p.stride, p.ks, p.pad, stages, TMA);
             g.rowB = TMA ? rowB : 0;
-            k_conv_row<TMA><<<tiles < slots ? tiles : slots, row_threads<TMA>(), smem, s>>>(p, g, m);
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3(unsigned(tiles < slots ? tiles : slots));
+            cfg.blockDim = dim3(unsigned(row_threads<TMA>()));
+            cfg.dynamicSmemBytes = smem;
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attr[0].val.programmaticStreamSerializationAllowed = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = p.pdl ? 1 : 0;
+            cudaLaunchKernelEx(&cfg, k_conv_row<TMA>, p, g, m);
         }
     } // namespace
 
