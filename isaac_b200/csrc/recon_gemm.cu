@@ -373,6 +373,9 @@ namespace isaacb
             int HWn; // entries a run needs (<= HWp; HWp is padded to 8 for TMA destinations)
             int stages; // halo buffers: 1 or 2
             int rowB; // swizzled staging: bytes per staged pixel (Cg * 2 = 32, 64 or 128); 0 = chunked runs
+            // implicit concatenation by TMA (1x1, xUp): channel chunks of cwc (coarse) and cwf
+            // (fine) channels, each staged as 128 swizzled rows; 0 = off
+            int cwc, cwf;
         };
 
         __host__ __device__ inline RowGeom row_geom(int stride, int ks, int pad, int stages, bool tma = false)
@@ -384,6 +387,7 @@ namespace isaacb
             g.HWp = tma ? (g.HWn + 7) / 8 * 8 : g.HWn;
             g.stages = stages;
             g.rowB = 0;
+            g.cwc = g.cwf = 0;
             return g;
         }
 
@@ -475,7 +479,8 @@ namespace isaacb
 
         template<bool TMA>
         __global__ void __launch_bounds__(row_threads<TMA>(), 1)
-            k_conv_row(const __grid_constant__ ConvGemmParams p, const RowGeom rg, const __grid_constant__ CUtensorMap tmap)
+            k_conv_row(const __grid_constant__ ConvGemmParams p, const RowGeom rg, const __grid_constant__ CUtensorMap tmap,
+                       const __grid_constant__ CUtensorMap tmapUp)
         {
             extern __shared__ unsigned char dsm[];
             __shared__ uint32_t sTmem;
@@ -494,11 +499,12 @@ namespace isaacb
             // swizzled staging: each input row is HWp pixels of rowB bytes, the row buffers
             // and the halo start on multiples of the swizzle pattern's period (8 rows)
             const int rowB = rg.rowB;
-            const uint32_t swSpan = 8u * uint32_t(rowB);
+            const bool cat = TMA && rg.cwc != 0;
+            const uint32_t swSpan = cat ? 1024u : 8u * uint32_t(rowB);
             const uint32_t rowPitch = rowB ? (uint32_t(HWp * rowB) + swSpan - 1u) / swSpan * swSpan : 0u;
             const uint32_t haloBytes = rowB ? uint32_t(ks * S) * rowPitch : uint32_t(ks * nC * S) * runBytes;
             const uint32_t wEnd = sB + uint32_t(p.Npad) * uint32_t(p.Kpad) * 2u;
-            const uint32_t sH = rowB ? (wEnd + swSpan - 1u) / swSpan * swSpan : wEnd;
+            const uint32_t sH = (rowB || cat) ? (wEnd + swSpan - 1u) / swSpan * swSpan : wEnd;
             const uint32_t half = tmem_columns(p.Npad);
             const uint32_t cols = 2 * half;
             if(warp == 0)
@@ -569,7 +575,9 @@ namespace isaacb
                 // 32/64/128-byte swizzle.  Rows and columns outside the image read zeros.
                 if(lane == 0)
                 {
-                    const uint32_t txBytes = rowB ? uint32_t(ks * S * HWp * rowB) : uint32_t(ks * nC * S * rg.HWn) * 16u;
+                    const uint32_t txBytes = cat ? uint32_t(kTileM * p.Cg * 2)
+                        : rowB                   ? uint32_t(ks * S * HWp * rowB)
+                                                 : uint32_t(ks * nC * S * rg.HWn) * 16u;
                     int i = 0;
                     for(int tile = blockIdx.x; tile < nTiles; tile += gridDim.x, ++i)
                     {
@@ -586,6 +594,27 @@ namespace isaacb
                         const int x0 = xt * kTileM;
                         const uint32_t st = sH + uint32_t(s) * haloBytes;
                         tc::mbar_arrive_expect_tx(&sFull[s], txBytes);
+                        if(cat)
+                        {
+                            // tile rows in parity order: row m < 64 is pixel x0 + 2m, row 64 + m
+                            // is pixel x0 + 2m + 1; both halves read coarse pixel x0/2 + m, so
+                            // the coarse chunk is copied to both, the fine chunk by parity
+                            uint32_t dst = st;
+                            for(int c = 0; c < p.upC; c += rg.cwc)
+                            {
+                                for(int h = 0; h < 2; ++h)
+                                    tc::tma_load_4d(dst + uint32_t(h * 64 * rg.cwc * 2), &tmapUp, c, x0 >> 1, y >> 1, b,
+                                                    &sFull[s]);
+                                dst += uint32_t(kTileM * rg.cwc * 2);
+                            }
+                            for(int c = 0; c < p.Cg - p.upC; c += rg.cwf)
+                            {
+                                for(int q = 0; q < 2; ++q)
+                                    tc::tma_load_5d(dst + uint32_t(q * 64 * rg.cwf * 2), &tmap, c, q, x0 >> 1, y, b, &sFull[s]);
+                                dst += uint32_t(kTileM * rg.cwf * 2);
+                            }
+                            continue;
+                        }
                         for(int ty = 0; ty < ks; ++ty)
                         {
                             const int iy = p.transposed ? y + pad - ty : S * y - pad + ty;
@@ -706,7 +735,32 @@ namespace isaacb
                         const uint64_t aBase = tc::smem_desc(st, lboA, 128u);
                         const uint64_t bBase = tc::smem_desc(sB, 128u, sboB);
                         uint32_t acc = 0;
-                        if(rowB)
+                        if(cat)
+                        {
+                            // the chunks in channel order (coarse, then fine), each 128 rows of
+                            // cw * 2 bytes with that width's swizzle
+                            uint32_t region = st, bOff = 0;
+                            for(int part = 0; part < 2; ++part)
+                            {
+                                const int cw = part == 0 ? rg.cwc : rg.cwf;
+                                const int cN = part == 0 ? p.upC : p.Cg - p.upC;
+                                const uint32_t rb = uint32_t(cw * 2);
+                                const uint64_t swDesc = (tc::smem_desc(0, 16u, 8u * rb) & ~uint64_t(0x3FFF))
+                                    | (uint64_t(rb == 32 ? 6 : rb == 64 ? 4 : 2) << 61);
+                                for(int c = 0; c < cN; c += cw)
+                                {
+                                    for(int jp = 0; jp < cw / 16; ++jp)
+                                    {
+                                        const uint32_t addr = region + uint32_t(jp) * 32u;
+                                        tc::mma_bf16(d, swDesc | uint64_t((addr >> 4) & 0x3FFFu), bBase + bOff, idesc, acc);
+                                        acc = 1;
+                                        bOff += 16u;
+                                    }
+                                    region += uint32_t(kTileM) * rb;
+                                }
+                            }
+                        }
+                        else if(rowB)
                         {
                             // K-major A with the rows' own swizzle (layout 6 / 4 / 2 = 32 / 64 /
                             // 128 bytes), 8-row groups swSpan apart; tap (ty, tx) starts idx0 rows
@@ -776,7 +830,9 @@ namespace isaacb
                     tc::fence_after_sync();
                     const int xt = tile % tilesPerRow;
                     const int row = tile / tilesPerRow;
-                    row_epilogue(p, tmem + uint32_t(a) * half + (lane0 << 16), xt, row / p.Ho, row % p.Ho, tid & 127, cBeg,
+                    const int m = tid & 127;
+                    const int px = cat ? (m < 64 ? 2 * m : 2 * (m - 64) + 1) : m; // parity-ordered rows
+                    row_epilogue(p, tmem + uint32_t(a) * half + (lane0 << 16), xt, row / p.Ho, row % p.Ho, px, cBeg,
                                  colsPer, sBias);
                     tc::fence_before_sync();
                     tc::mbar_arrive(&sAccEmpty[a]);
@@ -1080,10 +1136,54 @@ namespace isaacb
             return r == CUDA_SUCCESS;
         }
 
-        template<bool TMA>
-        void launch_row(const ConvGemmParams& p, int stages, const CUtensorMap& m, cudaStream_t s, int rowB = 0)
+        inline int chunk_width(int c)
         {
-            const size_t smem = conv_row_smem(p, stages, TMA);
+            return c % 64 == 0 ? 64 : c % 32 == 0 ? 32 : c % 16 == 0 ? 16 : 0;
+        }
+        inline CUtensorMapSwizzle swizzle_of(int rowBytes)
+        {
+            return rowBytes == 32 ? CU_TENSOR_MAP_SWIZZLE_32B : rowBytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
+        }
+
+        // The two tensor maps of the implicit concatenation by TMA (layout at k_conv_row):
+        // the fine tensor split by column parity, the coarse one plain; false when the layer
+        // does not fit (then the cp.async producer gathers it)
+        bool encode_cat_maps(const ConvGemmParams& p, RowGeom& g, CUtensorMap& fine, CUtensorMap& coarse)
+        {
+            auto enc = tensor_map_encoder();
+            const int cf = p.Cg - p.upC;
+            if(!enc || !p.xUp || p.ks != 1 || p.stride != 1 || p.pad != 0 || p.transposed || p.W % 2 != 0 || p.Wo != p.W
+               || p.Ho != p.H || 2 * p.upInW < p.W || 2 * p.upInH < p.H || p.upC <= 0 || cf <= 0 || !chunk_width(p.upC)
+               || !chunk_width(cf) || (reinterpret_cast<uintptr_t>(p.x) & 15u) != 0
+               || (reinterpret_cast<uintptr_t>(p.xUp) & 15u) != 0)
+                return false;
+            g.cwc = chunk_width(p.upC);
+            g.cwf = chunk_width(cf);
+            cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+            const cuuint64_t C = cuuint64_t(cf), W = cuuint64_t(p.W), H = cuuint64_t(p.H), B = cuuint64_t(p.B);
+            cuuint64_t dims[5] = {C, 2, W / 2, H, B};
+            cuuint64_t strides[4] = {C * 2, 2 * C * 2, W * C * 2, H * W * C * 2};
+            cuuint32_t box[5] = {cuuint32_t(g.cwf), 1, 64, 1, 1};
+            if(enc(&fine, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16*>(p.x), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_of(2 * g.cwf), CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)
+               != CUDA_SUCCESS)
+                return false;
+            const cuuint64_t Cc = cuuint64_t(p.upC), Wc = cuuint64_t(p.upInW), Hc = cuuint64_t(p.upInH);
+            cuuint64_t dimsC[4] = {Cc, Wc, Hc, B};
+            cuuint64_t stridesC[3] = {Cc * 2, Wc * Cc * 2, Hc * Wc * Cc * 2};
+            cuuint32_t boxC[4] = {cuuint32_t(g.cwc), 64, 1, 1};
+            return enc(&coarse, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(p.xUp), dimsC, stridesC, boxC, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle_of(2 * g.cwc), CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)
+                == CUDA_SUCCESS;
+        }
+
+        template<bool TMA>
+        void launch_row(const ConvGemmParams& p, int stages, const CUtensorMap& m, cudaStream_t s, int rowB = 0,
+                        const CUtensorMap* m2 = nullptr, int cwc = 0, int cwf = 0)
+        {
+            const size_t smem = conv_row_smem(p, stages, TMA) + (cwc ? 1024 : 0);
             cudaFuncSetAttribute(k_conv_row<TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
             cudaFuncSetAttribute(k_conv_row<TMA>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
             const int tiles = p.B * p.Ho * ((p.Wo + kTileM - 1) / kTileM);
@@ -1093,6 +1193,8 @@ namespace isaacb
             const int slots = num_sms() * perSm;
             RowGeom g = row_geom(p.stride, p.ks, p.pad, stages, TMA);
             g.rowB = TMA ? rowB : 0;
+            g.cwc = TMA ? cwc : 0;
+            g.cwf = TMA ? cwf : 0;
             cudaLaunchConfig_t cfg{};
             cfg.gridDim = dim3(unsigned(tiles < slots ? tiles : slots));
             cfg.blockDim = dim3(unsigned(row_threads<TMA>()));
@@ -1103,7 +1205,7 @@ namespace isaacb
             attr[0].val.programmaticStreamSerializationAllowed = 1;
             cfg.attrs = attr;
             cfg.numAttrs = p.pdl ? 1 : 0;
-            cudaLaunchKernelEx(&cfg, k_conv_row<TMA>, p, g, m);
+            cudaLaunchKernelEx(&cfg, k_conv_row<TMA>, p, g, m, m2 ? *m2 : m);
         }
     } // namespace
 
@@ -1120,7 +1222,10 @@ namespace isaacb
                 CUtensorMap m{};
                 RowGeom g = row_geom(p.stride, p.ks, p.pad, stages, true);
                 g.rowB = swizzle_row_bytes(p);
-                if(g_rowTma && !p.xUp && encode_row_map(p, g, m))
+                CUtensorMap m2{};
+                if(g_rowTma && p.xUp && conv_row_smem(p, stages, true) + 1024 <= 227 * 1024 && encode_cat_maps(p, g, m, m2))
+                    launch_row<true>(p, stages, m, s, 0, &m2, g.cwc, g.cwf);
+                else if(g_rowTma && !p.xUp && encode_row_map(p, g, m))
                     launch_row<true>(p, stages, m, s, g.rowB);
                 else
                     launch_row<false>(p, stages, m, s);

@@ -92,6 +92,31 @@ def test_inference_matches_oracle():
     assert np.abs(bl - refb).max() <= 1
 
 
+def test_inference_producers_agree():
+    """The decoder's 1x1 layers read their concatenated input [up(coarse), fine] in place:
+    by TMA where the widths allow (the fine tensor split by column parity, the coarse one
+    copied to both halves of the parity-ordered tile rows) and by cp.async gathers
+    otherwise.  Both accumulate every output in the same channel order, so the frames are
+    identical.  At 64 x 128 every level's width is even and the TMA form runs."""
+    from isaac_b200 import _lib
+
+    params = _he_params(4)
+    params[-528:] *= 0.1
+    low, _ = _smooth_pairs(1, 64, 128, 6)
+    net = Reconstructor(1, 64, 128, seed=1)
+    net.set_params(params)
+    lib = _lib.load()
+    outs = []
+    try:
+        for tma in (1, 0):
+            _lib.check(lib.isaacb_conv_set_producer(tma))
+            outs.append(net.infer(torch.from_numpy(low[0]).cuda()).cpu().numpy())
+    finally:
+        _lib.check(lib.isaacb_conv_set_producer(1))
+    assert net.error_flag() == 0
+    assert np.array_equal(outs[0], outs[1])
+
+
 def test_short_training_beats_bilinear():
     low, high = _smooth_pairs(16, 32, 32, 7)
     lt, ht = torch.from_numpy(low).cuda(), torch.from_numpy(high).cuda()
