@@ -600,11 +600,11 @@ namespace isaacb
                             // is pixel x0 + 2m + 1; both halves read coarse pixel x0/2 + m, so
                             // the coarse chunk is copied to both, the fine chunk by parity
                             uint32_t dst = st;
+                            const int yc = min(y >> 1, p.upInH - 1); // the nearest coarse row, clamped
                             for(int c = 0; c < p.upC; c += rg.cwc)
                             {
                                 for(int h = 0; h < 2; ++h)
-                                    tc::tma_load_4d(dst + uint32_t(h * 64 * rg.cwc * 2), &tmapUp, c, x0 >> 1, y >> 1, b,
-                                                    &sFull[s]);
+                                    tc::tma_load_4d(dst + uint32_t(h * 64 * rg.cwc * 2), &tmapUp, c, x0 >> 1, yc, b, &sFull[s]);
                                 dst += uint32_t(kTileM * rg.cwc * 2);
                             }
                             for(int c = 0; c < p.Cg - p.upC; c += rg.cwf)
@@ -1152,8 +1152,10 @@ namespace isaacb
         {
             auto enc = tensor_map_encoder();
             const int cf = p.Cg - p.upC;
+            // columns past the coarse width would read zeros where the gather clamps, so the
+            // coarse width must cover W / 2; rows are clamped in the kernel
             if(!enc || !p.xUp || p.ks != 1 || p.stride != 1 || p.pad != 0 || p.transposed || p.W % 2 != 0 || p.Wo != p.W
-               || p.Ho != p.H || 2 * p.upInW < p.W || 2 * p.upInH < p.H || p.upC <= 0 || cf <= 0 || !chunk_width(p.upC)
+               || p.Ho != p.H || 2 * p.upInW < p.W || p.upInH < 1 || p.upC <= 0 || cf <= 0 || !chunk_width(p.upC)
                || !chunk_width(cf) || (reinterpret_cast<uintptr_t>(p.x) & 15u) != 0
                || (reinterpret_cast<uintptr_t>(p.xUp) & 15u) != 0)
                 return false;

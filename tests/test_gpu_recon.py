@@ -92,18 +92,21 @@ def test_inference_matches_oracle():
     assert np.abs(bl - refb).max() <= 1
 
 
-def test_inference_producers_agree():
+@pytest.mark.parametrize("h,w", [(64, 128), (68, 128)])
+def test_inference_producers_agree(h, w):
     """The decoder's 1x1 layers read their concatenated input [up(coarse), fine] in place:
     by TMA where the widths allow (the fine tensor split by column parity, the coarse one
     copied to both halves of the parity-ordered tile rows) and by cp.async gathers
     otherwise.  Both accumulate every output in the same channel order, so the frames are
-    identical.  At 64 x 128 every level's width is even and the TMA form runs."""
+    identical.  At these sizes every level's width is even and the TMA form runs; at
+    68 rows the 2x2 stride-2 layer leaves 8 coarse rows under 17 fine ones, so the last
+    fine row reads the clamped coarse row."""
     from isaac_b200 import _lib
 
     params = _he_params(4)
     params[-528:] *= 0.1
-    low, _ = _smooth_pairs(1, 64, 128, 6)
-    net = Reconstructor(1, 64, 128, seed=1)
+    low, _ = _smooth_pairs(1, h, w, 6)
+    net = Reconstructor(1, h, w, seed=1)
     net.set_params(params)
     lib = _lib.load()
     outs = []
