@@ -21,7 +21,9 @@ namespace isaacb
     // brick (bx,by,bz) holds the four texels (x0,y0),(x0+1,y0),(x0,y0+1),(x0+1,y0+1)
     // of plane z, with x0 = 8bx-1+lx, y0 = 8by-1+ly, z = 8bz-1+lz, each clamped to
     // the volume.  A trilinear footprint whose base texel is (x0,y0,z0) is the two
-    // slots (lx,ly,lz) and (lx,ly,lz+1) of one brick.
+    // slots (lx,ly,lz) and (lx,ly,lz+1) of one brick.  The combined RGBA8 texture
+    // stores a slot channel-major (quad_channel_major), the iso alpha texture one
+    // byte per texel in the same order.
     constexpr int kSlotsPerBrick = 576;
     constexpr int kApron = 9;
 
@@ -443,45 +445,6 @@ namespace isaacb
         return lin(fx, A, B);
     }
 
-    // Sampler<LINEAR|NEAREST, CLAMP, normalized> on the combined RGBA8 texture
-    // (lib/isaac/isaac_texture.hpp:140-259), exact arithmetic.
-    __device__ __forceinline__ float4 sample_rgba8(const uint4* __restrict__ q, const Geom& g, float3 pos, bool linear)
-    {
-        if(linear)
-        {
-            float cx = pos.x - 0.5f, cy = pos.y - 0.5f, cz = pos.z - 0.5f;
-            float flx = floorf(cx), fly = floorf(cy), flz = floorf(cz);
-            float fx = cx - flx, fy = cy - fly, fz = cz - flz;
-            int ix = iclamp(f2i(flx), -1, g.ls[0] - 1);
-            int iy = iclamp(f2i(fly), -1, g.ls[1] - 1);
-            int iz = iclamp(f2i(flz), -1, g.ls[2] - 1);
-            size_t s = brick_slot(g, ix, iy, iz);
-            uint4 a = __ldg(q + s);
-            uint4 b = __ldg(q + s + 64);
-            float r[4];
-#pragma unroll
-            for(int c = 0; c < 4; ++c)
-                r[c] = tri_q(
-                    fx,
-                    fy,
-                    fz,
-                    byte_f(a.x, c),
-                    byte_f(a.y, c),
-                    byte_f(a.z, c),
-                    byte_f(a.w, c),
-                    byte_f(b.x, c),
-                    byte_f(b.y, c),
-                    byte_f(b.z, c),
-                    byte_f(b.w, c));
-            return make_float4(r[0] / 255.0f, r[1] / 255.0f, r[2] / 255.0f, r[3] / 255.0f);
-        }
-        int ix = iclamp(f2i(pos.x), 0, g.ls[0] - 1);
-        int iy = iclamp(f2i(pos.y), 0, g.ls[1] - 1);
-        int iz = iclamp(f2i(pos.z), 0, g.ls[2] - 1);
-        uint32_t w = reinterpret_cast<const uint32_t*>(q)[brick_slot(g, ix, iy, iz) * 4];
-        return make_float4(byte_f(w, 0) / 255.0f, byte_f(w, 1) / 255.0f, byte_f(w, 2) / 255.0f, byte_f(w, 3) / 255.0f);
-    }
-
     // alpha channel of the combined iso texture (alpha quads, 4 bytes per slot)
     __device__ __forceinline__ float sample_alpha(const uint32_t* __restrict__ q, const Geom& g, float3 pos, bool linear)
     {
@@ -644,21 +607,52 @@ namespace isaacb
     {
         return f2p_fma(a, b, negZero);
     }
-    // bytes (c, c+1) of w as the exact float pair (b_c 2^-133, b_c+1 2^-133): the byte
-    // in bits 16-23 and zeros elsewhere, one byte permute per value and no add.  Below
-    // 128 the value is subnormal, from 128 on bit 23 is the exponent's lowest bit and
-    // the value is normal, and in both ranges it equals b 2^-133; zero stays zero.  The
-    // packed fma (no .ftz) takes subnormal operands as they are; with weights scaled by
-    // 2^64 every product and sum is a normal number, each the unscaled one times 2^-69.
+    // byte c of w as the exact float b_c 2^-133: the byte in bits 16-23 and zeros
+    // elsewhere, one byte permute and no add.  Below 128 the value is subnormal, from 128
+    // on bit 23 is the exponent's lowest bit and the value is normal, and in both ranges
+    // it equals b 2^-133; zero stays zero.  fma (no .ftz) takes subnormal operands as they
+    // are; with weights scaled by 2^64 every product and sum is a normal number, each the
+    // unscaled one times 2^-69.
     __device__ __forceinline__ float ubyte_tiny(uint32_t w, int c)
     {
         return __int_as_float(int(__byte_perm(w, 0u, 0x4044u + 256u * unsigned(c))));
     }
-    __device__ __forceinline__ f2p ubyte_pair_tiny(uint32_t w, int c)
+
+    // ------------------------------------------------------------- channel-major quad slots
+    // A slot of the combined volume texture holds the 2x2 texels (x0,y0), (x0+1,y0),
+    // (x0,y0+1), (x0+1,y0+1) of one z-plane channel by channel: word c of the slot
+    // carries channel c of the four texels in bytes 0-3, in that order.  The march then
+    // weighs a whole word with two integer dot products (dp2a.lo on bytes 0-1, dp2a.hi
+    // on bytes 2-3) and never extracts a byte.
+
+    // the slot of four RGBA8 texels t0..t3 (texel order above): a 4x4 byte transpose
+    __device__ __forceinline__ uint4 quad_channel_major(uint32_t t0, uint32_t t1, uint32_t t2, uint32_t t3)
     {
-        const float lo = __int_as_float(int(__byte_perm(w, 0u, 0x4044u + 256u * unsigned(c))));
-        const float hi = __int_as_float(int(__byte_perm(w, 0u, 0x4044u + 256u * unsigned(c + 1))));
-        return f2p_make(lo, hi);
+        const uint32_t rg01 = __byte_perm(t0, t1, 0x5140u), ba01 = __byte_perm(t0, t1, 0x7362u);
+        const uint32_t rg23 = __byte_perm(t2, t3, 0x5140u), ba23 = __byte_perm(t2, t3, 0x7362u);
+        return make_uint4(__byte_perm(rg01, rg23, 0x5410u), __byte_perm(rg01, rg23, 0x7632u),
+                          __byte_perm(ba01, ba23, 0x5410u), __byte_perm(ba01, ba23, 0x7632u));
+    }
+    // texel k (0..3) of a channel-major slot as an RGBA8 word
+    __device__ __forceinline__ uint32_t quad_texel(uint4 q, int k)
+    {
+        const uint32_t sel = uint32_t(k) | (uint32_t(k) << 4);
+        return __byte_perm(__byte_perm(q.x, q.y, 0x0040u + sel), __byte_perm(q.z, q.w, 0x0040u + sel), 0x5410u);
+    }
+
+    // d = c + a.lo16 * b.byte0 + a.hi16 * b.byte1 (unsigned, exact)
+    __device__ __forceinline__ uint32_t dp2a_lo(uint32_t a, uint32_t b, uint32_t c)
+    {
+        uint32_t d;
+        asm("dp2a.lo.u32.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+        return d;
+    }
+    // d = c + a.lo16 * b.byte2 + a.hi16 * b.byte3 (unsigned, exact)
+    __device__ __forceinline__ uint32_t dp2a_hi(uint32_t a, uint32_t b, uint32_t c)
+    {
+        uint32_t d;
+        asm("dp2a.hi.u32.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+        return d;
     }
 
     // pixel of a thread: a block of 256 threads covers 32x8 pixels and each warp an 8x4 tile

@@ -17,9 +17,13 @@ namespace isaacb
     // Front-to-back march of CombinedVolumeRenderKernel (lib/isaac/isaac_volume_kernel.hpp:61-87)
     // at the reference's sample positions.  Differences from the exact form, all far
     // below one output LSB and covered by the parity tests:
-    //  * pos - 0.5 is one fmaf per axis, the trilinear is evaluated as 8 FP32 weights,
-    //    and the /255 normalisation is folded into the per-ray factor;
-    //  * bytes become floats through a byte permute (no conversion pipe);
+    //  * pos - 0.5 is one fmaf per axis and the /255 normalisation is folded into the
+    //    per-ray factor;
+    //  * the trilinear is an integer dot product: the 8 FP32 weights are rounded to
+    //    16-bit fixed point (w * 65535), and each channel-major slot word (channel c of
+    //    the 2x2 texels of one plane) is weighed whole by dp2a.lo + dp2a.hi.  The sums
+    //    are exact integers below 2^24, so the only error is the weights' rounding,
+    //    at most 8 * 0.5 / 65535 * 255 = 0.016 byte units per sample;
     //  * empty-space skipping: a brick whose texels (apron included) are all zero
     //    yields exactly zero samples, so the samples inside it are counted but not
     //    evaluated -- adding zero leaves the colour unchanged.
@@ -35,15 +39,15 @@ namespace isaacb
     {
         const Geom& g = p.g;
         const float k = factor / 255.0f;
-        // trilinear samples come out scaled by 2^-69 (see the tap loop); 2^69 k is exact
-        const float kS = LINEAR ? k * 0x1p69f : k;
+        // trilinear samples come out scaled by the weights' fixed-point unit 65535
+        constexpr float kUnit = 65535.0f;
+        const float kS = LINEAR ? k / kUnit : k;
         const float off = LINEAR ? 0.5f : 0.0f;
         const float c0x = m.startU.x - off, c0y = m.startU.y - off, c0z = m.startU.z - off;
         const float svx = m.stepVec.x, svy = m.stepVec.y, svz = m.stepVec.z;
         const float lo = LINEAR ? -1.0f : 0.0f;
         const float hx = float(g.ls[0] - 1), hy = float(g.ls[1] - 1), hz = float(g.ls[2] - 1);
         const int nb0 = g.nb[0], nb1 = g.nb[1];
-        const uint32_t* __restrict__ q32 = reinterpret_cast<const uint32_t*>(p.volQ);
         // floor(c) + 1 (the apron-shifted coordinate) straight from the magic-number add
         const int magic = 0x4B400000 - 1;
         float4 color = make_float4(0, 0, 0, 0);
@@ -95,36 +99,35 @@ namespace isaacb
             float r0, r1, r2, r3;
             if(LINEAR)
             {
+                // channel-major slots: A.c / B.c = channel c of the 2x2 texels of planes z0 / z0+1
                 const uint4 A = __ldg(p.volQ + slot);
                 const uint4 B = __ldg(p.volQ + slot + 64);
                 const float fx = cx - (tx - 12582912.0f), fy = cy - (ty - 12582912.0f), fz = cz - (tz - 12582912.0f);
-                // the z weights carry a factor 2^64 (exact: 2^64 - 2^64 fz is 1 - fz
-                // rounded, then scaled), so all eight weights are the unscaled ones times 2^64
-                const float fz64 = fz * 0x1p64f;
-                const float gx = 1.0f - fx, gy = 1.0f - fy, gz64 = 0x1p64f - fz64;
+                const float gx = 1.0f - fx, gy = 1.0f - fy;
+                const float fzU = fz * kUnit, gzU = kUnit - fzU;
                 const float w00 = gx * gy, w10 = fx * gy, w01 = gx * fy, w11 = fx * fy;
-                const float wt[8] = {w00 * gz64, w10 * gz64, w01 * gz64, w11 * gz64,
-                                     w00 * fz64, w10 * fz64, w01 * fz64, w11 * fz64};
-                const uint32_t tap[8] = {A.x, A.y, A.z, A.w, B.x, B.y, B.z, B.w};
-                // (r,g) and (b,a) accumulate as packed FP32 pairs, one FFMA2 each per tap,
-                // over the bytes as b 2^-133 (one byte permute, no bias add): every product
-                // and partial sum is the unscaled one times 2^-69, rounded the same way,
-                // and the 2^69 goes into the compositing factor
-                f2p rg = f2p_make(0.0f, 0.0f), ba = f2p_make(0.0f, 0.0f);
-#pragma unroll
-                for(int k = 0; k < 8; ++k)
-                {
-                    const f2p wk = f2p_make(wt[k], wt[k]);
-                    rg = f2p_fma(ubyte_pair_tiny(tap[k], 0), wk, rg);
-                    ba = f2p_fma(ubyte_pair_tiny(tap[k], 2), wk, ba);
-                }
-                f2p_split(rg, r0, r1);
-                f2p_split(ba, r2, r3);
+                // round(w * 65535) lands in the low bits of 2^23 + w * 65535 (one rounding,
+                // to nearest); <= 65535, so the low 16 bits are the weight
+                auto q = [](float w, float zU) { return __float_as_uint(fmaf(w, zU, 8388608.0f)); };
+                // weight pairs (texel (x0,y) | texel (x0+1,y) << 16) for rows y0 and y0+1 of each plane
+                const uint32_t W0a = __byte_perm(q(w00, gzU), q(w10, gzU), 0x5410u);
+                const uint32_t W1a = __byte_perm(q(w01, gzU), q(w11, gzU), 0x5410u);
+                const uint32_t W0b = __byte_perm(q(w00, fzU), q(w10, fzU), 0x5410u);
+                const uint32_t W1b = __byte_perm(q(w01, fzU), q(w11, fzU), 0x5410u);
+                // Σ weights <= 65535 + 4, so every channel sum is an exact integer below 2^24
+                auto tri = [&](uint32_t a, uint32_t b) {
+                    return __uint2float_rn(dp2a_hi(W1b, b, dp2a_lo(W0b, b, dp2a_hi(W1a, a, dp2a_lo(W0a, a, 0u)))));
+                };
+                r0 = tri(A.x, B.x);
+                r1 = tri(A.y, B.y);
+                r2 = tri(A.z, B.z);
+                r3 = tri(A.w, B.w);
             }
             else
             {
-                const uint32_t w = __ldg(q32 + size_t(slot) * 4);
-                r0 = ubyte_f(w, 0), r1 = ubyte_f(w, 1), r2 = ubyte_f(w, 2), r3 = ubyte_f(w, 3);
+                // texel (x0, y0) of the slot: byte 0 of each channel word
+                const uint4 Q = __ldg(p.volQ + slot);
+                r0 = ubyte_f(Q.x, 0), r1 = ubyte_f(Q.y, 0), r2 = ubyte_f(Q.z, 0), r3 = ubyte_f(Q.w, 0);
             }
             const float s = (1.0f - color.w) * kS;
             color.x = fmaf(s, r0, color.x);

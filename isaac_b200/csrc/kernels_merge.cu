@@ -400,6 +400,8 @@ namespace isaacb
     // reduction per brick gives the flags that drive empty-space skipping.  Then the 4
     // bricks' 576-slot quad blocks, contiguous in memory, go out as 16-byte stores: thread
     // (lx, ly) walks the slot layers lz of all 4 bricks, and slot index = layer * 64 + lxy.
+    // A slot is stored channel-major (quad_channel_major: word c = channel c of its four
+    // texels), the form the march's integer dot products read.
     // Every texel is a copy of a voxel pass 1 computed once.
     constexpr int kPackRow = 4;
     constexpr int kPackPitch = 40; // row pitch in words: 40 = 8 mod 32 keeps the quad reads conflict-free
@@ -520,7 +522,7 @@ namespace isaacb
             const int j = layer / kApron, lz = layer - j * kApron;
             const int t = lz * (kApron * kPackPitch) + base + 8 * j;
             const size_t slot = brick0 * kSlotsPerBrick + size_t(layer) * 64 + lxy;
-            p.volQ[slot] = make_uint4(volS[t], volS[t + 1], volS[t + kPackPitch], volS[t + kPackPitch + 1]);
+            p.volQ[slot] = quad_channel_major(volS[t], volS[t + 1], volS[t + kPackPitch], volS[t + kPackPitch + 1]);
             if(ISO)
                 p.isoAQ[slot] = (isoS[t] >> 24) | ((isoS[t + 1] >> 24) << 8) | ((isoS[t + kPackPitch] >> 24) << 16)
                     | ((isoS[t + kPackPitch + 1] >> 24) << 24);
@@ -1102,7 +1104,7 @@ namespace isaacb
             const int x = int(i % g.ls[0]);
             const int y = int((i / g.ls[0]) % g.ls[1]);
             const int z = int(i / (size_t(g.ls[0]) * g.ls[1]));
-            out[i] = reinterpret_cast<const uint32_t*>(q)[brick_slot(g, x, y, z) * 4];
+            out[i] = quad_texel(__ldg(q + brick_slot(g, x, y, z)), 0);
         }
     }
 
