@@ -260,7 +260,7 @@ typedef struct isaacb_batch_config
 {
     uint32_t tile_w, tile_h; /* tile_w*tile_h == 256, tile_w % 8 == 0, tile_h % 4 == 0 */
     uint32_t blocks_per_sm; /* 0 = as many as fit */
-    int32_t skip_empty; /* 1 check per-brick emptiness, 0 never, -1 per context (default) */
+    int32_t skip_empty; /* 1 check per-brick emptiness, 0 never, -1 when the context's last merge found empty bricks (default) */
 } isaacb_batch_config;
 
 typedef struct isaacb_batch isaacb_batch;

@@ -335,12 +335,9 @@ struct isaacb_ctx
     float* mmResult = nullptr;
     unsigned long long* mmKeys = nullptr;
     int32_t* errorFlag = nullptr;
-    // count of all-zero bricks of the last merge, copied back asynchronously; the
-    // march checks brick emptiness only when the previous count was not zero
+    // count of all-zero bricks of the last merge (device memory); the march reads it and
+    // checks brick emptiness only when it is not zero
     unsigned int* emptyDev = nullptr;
-    unsigned int* emptyPinned = nullptr;
-    cudaEvent_t emptyEvent = nullptr;
-    long long lastEmpty = -1;
     // field-source advection (defaults of lib/isaac.hpp:606-643); the textures start at zero
     bool field[kMaxSources]{};
     uint8_t* adv[kMaxSources]{}; // guarded: (local + 2 * advG) per axis
@@ -814,9 +811,7 @@ extern "C"
         alloc((void**) &c->errorFlag, sizeof(int32_t));
         alloc((void**) &c->emptyDev, sizeof(unsigned int));
         if(e == cudaSuccess)
-            e = cudaMallocHost((void**) &c->emptyPinned, sizeof(unsigned int));
-        if(e == cudaSuccess)
-            e = cudaEventCreateWithFlags(&c->emptyEvent, cudaEventDisableTiming);
+            e = cudaMemset(c->emptyDev, 0, sizeof(unsigned int));
         if(e == cudaSuccess)
             e = cudaMemset(c->errorFlag, 0, sizeof(int32_t));
         if(e == cudaSuccess)
@@ -874,10 +869,6 @@ extern "C"
         cudaFree(c->noise);
         cudaFree(c->noiseTmp);
         cudaFree(c->emptyDev);
-        if(c->emptyPinned)
-            cudaFreeHost(c->emptyPinned);
-        if(c->emptyEvent)
-            cudaEventDestroy(c->emptyEvent);
         for(auto& e : c->ev)
             if(e)
                 cudaEventDestroy(e);
@@ -1278,15 +1269,6 @@ extern "C"
                 PhaseTimer t(c, 0, st);
                 c->updateLaunches += uint32_t(launch_merge(p, st));
             }
-            // the count comes back asynchronously; a later render reads it once the event completed
-            if(cudaEventQuery(c->emptyEvent) != cudaErrorNotReady)
-            {
-                ISAACB_CUDA(
-                    c,
-                    cudaMemcpyAsync(c->emptyPinned, c->emptyDev, sizeof(unsigned int), cudaMemcpyDeviceToHost, st),
-                    "empty brick count");
-                ISAACB_CUDA(c, cudaEventRecord(c->emptyEvent, st), "empty brick event");
-            }
             if(!p.writeIso && c->isoWritten)
             {
                 // the reference's iso texture is all zero when no source has an iso threshold
@@ -1383,10 +1365,7 @@ extern "C"
         p.totalWeightAll = 0.0f;
         for(int s = 0; s < c->nTotal; ++s)
             p.totalWeightAll += c->weight[s];
-        if(cudaEventQuery(c->emptyEvent) == cudaSuccess)
-            c->lastEmpty = (long long) *c->emptyPinned;
-        // either choice renders the same image; skipping only pays when bricks are empty
-        p.skipEmpty = c->lastEmpty != 0 ? 1 : 0;
+        p.emptyCount = c->emptyDev;
         p.lut = c->lutDev;
         p.volQ = c->volQ;
         p.isoAQ = c->isoAQ;
@@ -1748,8 +1727,6 @@ namespace
         for(size_t i = 0; i < b->ctxs.size(); ++i)
         {
             isaacb_ctx* c = b->ctxs[i];
-            if(cudaEventQuery(c->emptyEvent) == cudaSuccess)
-                c->lastEmpty = (long long) *c->emptyPinned;
             BatchCtx& t = b->ctxPinned[i];
             std::memset(&t, 0, sizeof(t));
             t.g = c->g;
@@ -1760,7 +1737,8 @@ namespace
             for(int s = 0; s < c->nTotal; ++s)
                 t.totalWeightAll += c->weight[s];
             t.interpolation = c->interpolation;
-            t.skipEmpty = b->cfg.skip_empty >= 0 ? b->cfg.skip_empty : (c->lastEmpty != 0 ? 1 : 0);
+            t.skipEmpty = b->cfg.skip_empty >= 0 ? (b->cfg.skip_empty != 0 ? 1 : 0) : -1;
+            t.emptyCount = c->emptyDev;
             t.volume = t.totalWeightAll > 0.0f ? 1 : 0;
             t.renderMode = c->renderMode;
             t.aoWeight = c->aoWeight;
@@ -1824,13 +1802,6 @@ namespace
                 if(cudaMemsetAsync(c->emptyDev, 0, sizeof(unsigned int), st) != cudaSuccess)
                     return batch_fail(ISAACB_CUDA_ERROR, "isaacb_batch: empty brick counter");
                 b->launches += uint32_t(launch_merge(p, st));
-                if(!capture && cudaEventQuery(c->emptyEvent) != cudaErrorNotReady)
-                {
-                    if(cudaMemcpyAsync(c->emptyPinned, c->emptyDev, sizeof(unsigned int), cudaMemcpyDeviceToHost, st)
-                           != cudaSuccess
-                       || cudaEventRecord(c->emptyEvent, st) != cudaSuccess)
-                        return batch_fail(ISAACB_CUDA_ERROR, "isaacb_batch: empty brick count");
-                }
             }
         }
         if(cudaMemsetAsync(b->counter, 0, sizeof(int32_t), st) != cudaSuccess)

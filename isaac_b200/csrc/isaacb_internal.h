@@ -184,7 +184,10 @@ namespace isaacb
         int32_t aoSamples;
         int8_t aoOffsets[2 * kMaxAoSamples];
         float totalWeightAll;
-        int32_t skipEmpty; // the volume march checks per-brick emptiness
+        // all-zero bricks counted by the last merge of the combined texture (device memory,
+        // written earlier on the same stream): the volume march skips empty bricks when it
+        // is nonzero, a choice made on the GPU so that it always matches the texture
+        const unsigned int* emptyCount;
         const float4* lut;
         // combined textures
         const uint4* volQ;
@@ -219,7 +222,8 @@ namespace isaacb
         float step;
         float totalWeightAll;
         int32_t interpolation;
-        int32_t skipEmpty;
+        int32_t skipEmpty; // 0 or 1, or -1: skip when *emptyCount (the last merge's all-zero bricks) is nonzero
+        const unsigned int* emptyCount;
         int32_t volume; // totalWeightAll > 0
         int32_t renderMode;
         float aoWeight;

@@ -108,10 +108,12 @@ namespace isaacb
             if(px < sv.W && py < sv.H)
             {
                 uchar4 c;
+                // auto (-1): skip when the context's last merge found empty bricks
+                const bool skip = sc.skipEmpty >= 0 ? sc.skipEmpty != 0 : __ldg(sc.emptyCount) != 0u;
                 if(sc.interpolation)
-                    c = sc.skipEmpty ? batch_pixel<true, true>(sc, sv, px, py, n) : batch_pixel<true, false>(sc, sv, px, py, n);
+                    c = skip ? batch_pixel<true, true>(sc, sv, px, py, n) : batch_pixel<true, false>(sc, sv, px, py, n);
                 else
-                    c = sc.skipEmpty ? batch_pixel<false, true>(sc, sv, px, py, n) : batch_pixel<false, false>(sc, sv, px, py, n);
+                    c = skip ? batch_pixel<false, true>(sc, sv, px, py, n) : batch_pixel<false, false>(sc, sv, px, py, n);
                 bv.out[size_t(py) * sv.W + px] = c;
             }
             __syncthreads();

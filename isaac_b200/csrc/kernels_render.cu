@@ -17,6 +17,7 @@
 #include "isaacb_frame.cuh"
 #include "isaacb_march.cuh"
 
+#include <algorithm>
 #include <cfloat>
 
 namespace isaacb
@@ -396,11 +397,24 @@ namespace isaacb
         k_ssao<<<grid, 256, 0, s>>>(p);
     }
 
-    template<bool VOLUME, bool LINEAR, bool SKIP>
-    __global__ void __launch_bounds__(256) k_shade_volume(const __grid_constant__ FrameParams p)
+    // pixel rows of a k_shade_volume block (32 x kShadeRows pixels, 32 * kShadeRows threads)
+    constexpr int kShadeRows = 4;
+    constexpr int kShadeThreads = 32 * kShadeRows;
+
+    // FULL: registers capped so that a whole SM's threads are resident (16 blocks of 128
+    // threads, 32 registers, a few bytes spilled outside the sample loop).  Launches of
+    // only a few waves take it: more resident rays shorten their tail.  Longer launches
+    // keep the uncapped form (39 registers, 12 blocks), whose loop runs a little faster.
+    template<bool VOLUME, bool LINEAR, bool FULL>
+    __global__ void __launch_bounds__(kShadeThreads, FULL ? 2048 / kShadeThreads : 1) k_shade_volume(const __grid_constant__ FrameParams p)
     {
-        int px, py;
-        thread_pixel(px, py);
+        // empty-space skipping only pays when the texture has empty bricks; the merge that
+        // wrote it counted them (either choice renders the same image)
+        const bool skip = VOLUME && __ldg(p.emptyCount) != 0u;
+        // a block covers 32 x kShadeRows pixels, each warp an 8 x 4 tile
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        const int px = int(blockIdx.x) * 32 + (w & 3) * 8 + (l & 7);
+        const int py = int(blockIdx.y) * kShadeRows + (w >> 2) * 4 + (l >> 3);
         unsigned long long n = 0;
         if(px < p.v.W && py < p.v.H)
         {
@@ -419,9 +433,11 @@ namespace isaacb
                         float4 color;
                         const VolTexRef tex{p.g, p.volQ, p.volFlag};
                         if(LINEAR && march_in_range(p.g, m))
-                            color = march_combined<LINEAR, false, SKIP>(tex, m, factor, n);
+                            color = skip ? march_combined<LINEAR, false, true>(tex, m, factor, n)
+                                         : march_combined<LINEAR, false, false>(tex, m, factor, n);
                         else
-                            color = march_combined<LINEAR, true, SKIP>(tex, m, factor, n);
+                            color = skip ? march_combined<LINEAR, true, true>(tex, m, factor, n)
+                                         : march_combined<LINEAR, true, false>(tex, m, factor, n);
                         const float4 solid = from_byte4(p.color[o]);
                         const float r = 1.0f - color.w;
                         color = make_float4(color.x + r * solid.x, color.y + r * solid.y, color.z + r * solid.z, color.w + r * solid.w);
@@ -434,24 +450,38 @@ namespace isaacb
             count_samples(p.counters, n);
     }
 
+    template<bool FULL>
+    void launch_shade_volume_as(const FrameParams& p, bool volume, dim3 grid, cudaStream_t s)
+    {
+        if(!volume)
+            k_shade_volume<false, false, FULL><<<grid, kShadeThreads, 0, s>>>(p);
+        else if(p.interpolation)
+            k_shade_volume<true, true, FULL><<<grid, kShadeThreads, 0, s>>>(p);
+        else
+            k_shade_volume<true, false, FULL><<<grid, kShadeThreads, 0, s>>>(p);
+    }
+
+    // launches of fewer than this many waves of the uncapped form take the FULL form
+    constexpr int kShadeShortWaves = 4;
+
     void launch_shade_volume(const FrameParams& p, bool volume, cudaStream_t s)
     {
-        dim3 grid((p.v.W + 31) / 32, (p.v.H + 7) / 8);
-        if(!volume)
-            k_shade_volume<false, false, false><<<grid, 256, 0, s>>>(p);
-        else if(p.interpolation)
+        dim3 grid((p.v.W + 31) / 32, (p.v.H + kShadeRows - 1) / kShadeRows);
+        // resident blocks of the uncapped form on the whole device, once per device
+        static int resident[64] = {0};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if(dev >= 0 && dev < 64 && resident[dev] == 0)
         {
-            if(p.skipEmpty)
-                k_shade_volume<true, true, true><<<grid, 256, 0, s>>>(p);
-            else
-                k_shade_volume<true, true, false><<<grid, 256, 0, s>>>(p);
+            int sms = 0, perSm = 0;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_shade_volume<true, true, false>, kShadeThreads, 0);
+            resident[dev] = std::max(1, sms * perSm);
         }
+        const long long waves = (long long) grid.x * grid.y / std::max(1, dev >= 0 && dev < 64 ? resident[dev] : 1);
+        if(volume && waves < kShadeShortWaves)
+            launch_shade_volume_as<true>(p, volume, grid, s);
         else
-        {
-            if(p.skipEmpty)
-                k_shade_volume<true, false, true><<<grid, 256, 0, s>>>(p);
-            else
-                k_shade_volume<true, false, false><<<grid, 256, 0, s>>>(p);
-        }
+            launch_shade_volume_as<false>(p, volume, grid, s);
     }
 } // namespace isaacb

@@ -8,6 +8,7 @@ random 4-8 point transfer functions at full size (step 0.5) and half size
 the full-size crop of 2c x 2c at twice its origin) are the training pairs.
 
     python -m isaac_b200.recon_train --pairs 20000 --timesteps 64 --steps 4000 [--renderer combined]
+    python -m isaac_b200.recon_train --error-budget --eval-views 12 [--renderer combined]
 
 writes the FP32 weights to isaac_b200/data/recon_unet.f32 (per-source renderer)
 or recon_unet_combined.f32 (combined renderer), the defaults the judged renderer
@@ -208,6 +209,54 @@ def evaluate(pr: PairRenderer, net: Reconstructor, views: int, seed: int, timest
     return rec, bil
 
 
+def error_budget(pr: PairRenderer, net: Reconstructor, views: int, seed: int, timesteps: int) -> dict:
+    """Where the learned path's error comes from, per held-out view, as PSNR (dB)
+    against the plain full-size step render:
+
+    * ``reconstruction`` / ``bilinear``: the network and bilinear x2 on the half-size
+      frame at twice the step (the learned path and the method without the network);
+    * ``bilinear_half_step``: bilinear x2 on a half-size frame at the full-size step
+      (the error of the half-size ray grid alone);
+    * ``reconstruction_half_step``: the network on that frame;
+    * ``full_double_step``: the full-size frame at twice the step (the error of the
+      longer step alone).
+
+    Returns the per-view rows and their means."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    W, H = pr.width, pr.height
+    full = torch.empty((H, W, 4), dtype=torch.uint8, device="cuda")
+    full2 = torch.empty_like(full)
+    half = torch.empty((H // 2, W // 2, 4), dtype=torch.uint8, device="cuda")
+    half1 = torch.empty_like(half)
+    out = torch.empty_like(full)
+    rows = []
+    for _ in range(views):
+        t = int(rng.integers(0, timesteps))
+        if pr.timestep != t:
+            pr.set_timestep(t)
+        P, MV = random_camera(W, H, rng)
+        pr.set_view(P, MV, [random_transfer(rng) for _ in SEEDS])
+        pr.render(full, half, update=False)
+        net.infer(half, out)
+        r = {"reconstruction": psnr(out, full), "bilinear": psnr(bilinear2(half, out), full)}
+        pr.low.setStep(pr.step)
+        pr.full.setStep(2 * pr.step)
+        try:
+            pr.render(full2, half1, update=False)
+        finally:
+            pr.low.setStep(2 * pr.step)
+            pr.full.setStep(pr.step)
+        r["bilinear_half_step"] = psnr(bilinear2(half1, out), full)
+        net.infer(half1, out)
+        r["reconstruction_half_step"] = psnr(out, full)
+        r["full_double_step"] = psnr(full2, full)
+        rows.append(r)
+    means = {k: float(np.mean([r[k] for r in rows])) for k in rows[0]}
+    return {"views": rows, "mean": means}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--size", type=int, default=512)
@@ -223,8 +272,18 @@ def main(argv=None):
     ap.add_argument("--eval-views", type=int, default=16)
     ap.add_argument("--renderer", default="per_source", choices=["per_source", "combined"])
     ap.add_argument("--out", default=None, help="weights file (default: the renderer's)")
+    ap.add_argument("--error-budget", action="store_true",
+                    help="no training: split the committed network's held-out error into its sources (error_budget)")
     a = ap.parse_args(argv)
     a.out = a.out or str(weights_for(a.renderer))
+    if a.error_budget:
+        pr = PairRenderer(a.size, a.width, a.height, renderer=a.renderer)
+        net = Reconstructor(1, a.height // 2, a.width // 2, seed=a.seed)
+        net.load(Path(a.out))
+        eb = error_budget(pr, net, a.eval_views, a.seed + 4241, a.timesteps)
+        print(json.dumps({"renderer": a.renderer, "size": a.size, "frame": [a.width, a.height], "views": a.eval_views,
+                          "psnr_db_mean": eb["mean"]}), flush=True)
+        return 0
 
     pr = PairRenderer(a.size, a.width, a.height, renderer=a.renderer)
     low, high = make_pairs(pr, a.pairs, a.timesteps, a.crop, a.seed)
