@@ -14,6 +14,30 @@ namespace isaacb
         const uint8_t* volFlag;
     };
 
+    // the trilinear sample of channel-major slots A (plane z0) and B (plane z0 + 1) at the
+    // fractional position (fx, fy, fz), in units of 1/65535 byte: an exact integer sum of
+    // 16-bit fixed-point weights times bytes
+    __device__ __forceinline__ float4 trilinear_dp2a(uint4 A, uint4 B, float fx, float fy, float fz)
+    {
+        constexpr float kUnit = 65535.0f;
+        const float gx = 1.0f - fx, gy = 1.0f - fy;
+        const float fzU = fz * kUnit, gzU = kUnit - fzU;
+        const float w00 = gx * gy, w10 = fx * gy, w01 = gx * fy, w11 = fx * fy;
+        // round(w * 65535) lands in the low bits of 2^23 + w * 65535 (one rounding, to
+        // nearest); <= 65535, so the low 16 bits are the weight
+        auto q = [](float w, float zU) { return __float_as_uint(fmaf(w, zU, 8388608.0f)); };
+        // weight pairs (texel (x0,y) | texel (x0+1,y) << 16) for rows y0 and y0+1 of each plane
+        const uint32_t W0a = __byte_perm(q(w00, gzU), q(w10, gzU), 0x5410u);
+        const uint32_t W1a = __byte_perm(q(w01, gzU), q(w11, gzU), 0x5410u);
+        const uint32_t W0b = __byte_perm(q(w00, fzU), q(w10, fzU), 0x5410u);
+        const uint32_t W1b = __byte_perm(q(w01, fzU), q(w11, fzU), 0x5410u);
+        // Σ weights <= 65535 + 4, so every channel sum is an exact integer below 2^24
+        auto tri = [&](uint32_t a, uint32_t b) {
+            return __uint2float_rn(dp2a_hi(W1b, b, dp2a_lo(W0b, b, dp2a_hi(W1a, a, dp2a_lo(W0a, a, 0u)))));
+        };
+        return make_float4(tri(A.x, B.x), tri(A.y, B.y), tri(A.z, B.z), tri(A.w, B.w));
+    }
+
     // Front-to-back march of CombinedVolumeRenderKernel (lib/isaac/isaac_volume_kernel.hpp:61-87)
     // at the reference's sample positions.  Differences from the exact form, all far
     // below one output LSB and covered by the parity tests:
@@ -102,26 +126,8 @@ namespace isaacb
                 // channel-major slots: A.c / B.c = channel c of the 2x2 texels of planes z0 / z0+1
                 const uint4 A = __ldg(p.volQ + slot);
                 const uint4 B = __ldg(p.volQ + slot + 64);
-                const float fx = cx - (tx - 12582912.0f), fy = cy - (ty - 12582912.0f), fz = cz - (tz - 12582912.0f);
-                const float gx = 1.0f - fx, gy = 1.0f - fy;
-                const float fzU = fz * kUnit, gzU = kUnit - fzU;
-                const float w00 = gx * gy, w10 = fx * gy, w01 = gx * fy, w11 = fx * fy;
-                // round(w * 65535) lands in the low bits of 2^23 + w * 65535 (one rounding,
-                // to nearest); <= 65535, so the low 16 bits are the weight
-                auto q = [](float w, float zU) { return __float_as_uint(fmaf(w, zU, 8388608.0f)); };
-                // weight pairs (texel (x0,y) | texel (x0+1,y) << 16) for rows y0 and y0+1 of each plane
-                const uint32_t W0a = __byte_perm(q(w00, gzU), q(w10, gzU), 0x5410u);
-                const uint32_t W1a = __byte_perm(q(w01, gzU), q(w11, gzU), 0x5410u);
-                const uint32_t W0b = __byte_perm(q(w00, fzU), q(w10, fzU), 0x5410u);
-                const uint32_t W1b = __byte_perm(q(w01, fzU), q(w11, fzU), 0x5410u);
-                // Σ weights <= 65535 + 4, so every channel sum is an exact integer below 2^24
-                auto tri = [&](uint32_t a, uint32_t b) {
-                    return __uint2float_rn(dp2a_hi(W1b, b, dp2a_lo(W0b, b, dp2a_hi(W1a, a, dp2a_lo(W0a, a, 0u)))));
-                };
-                r0 = tri(A.x, B.x);
-                r1 = tri(A.y, B.y);
-                r2 = tri(A.z, B.z);
-                r3 = tri(A.w, B.w);
+                const float4 r = trilinear_dp2a(A, B, cx - (tx - 12582912.0f), cy - (ty - 12582912.0f), cz - (tz - 12582912.0f));
+                r0 = r.x, r1 = r.y, r2 = r.z, r3 = r.w;
             }
             else
             {
