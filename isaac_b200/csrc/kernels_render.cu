@@ -397,24 +397,35 @@ namespace isaacb
         k_ssao<<<grid, 256, 0, s>>>(p);
     }
 
-    // pixel rows of a k_shade_volume block (32 x kShadeRows pixels, 32 * kShadeRows threads)
-    constexpr int kShadeRows = 4;
-    constexpr int kShadeThreads = 32 * kShadeRows;
+    // A k_shade_volume block is 128 threads, 4 warps of 8 x 4 pixels, covering a tile of
+    // tile_w(FULL) x tile_h(FULL) pixels.
+    constexpr int kShadeThreads = 128;
+    // tile width of the FULL form (the short launches): 16 x 8 pixels keep a block's rays
+    // closer together than 32 x 4 (the 960x540 half-size render: 0.953 -> 0.931 ms)
+    constexpr int kShortTileW = 16;
+    __host__ __device__ constexpr int shade_tile_w(bool full)
+    {
+        return full ? kShortTileW : 32;
+    }
+    __host__ __device__ constexpr int shade_tile_h(bool full)
+    {
+        return kShadeThreads / shade_tile_w(full);
+    }
 
-    // FULL: registers capped so that a whole SM's threads are resident (16 blocks of 128
-    // threads, 32 registers, a few bytes spilled outside the sample loop).  Launches of
-    // only a few waves take it: more resident rays shorten their tail.  Longer launches
-    // keep the uncapped form (39 registers, 12 blocks), whose loop runs a little faster.
+    // FULL: registers capped so that a whole SM's threads are resident (16 blocks, 32
+    // registers, a few bytes spilled).  Launches of only a few waves take it: more
+    // resident rays shorten their tail.  Longer launches keep the uncapped form (46
+    // registers, 10 blocks per SM), whose loop runs faster.
     template<bool VOLUME, bool LINEAR, bool FULL>
     __global__ void __launch_bounds__(kShadeThreads, FULL ? 2048 / kShadeThreads : 1) k_shade_volume(const __grid_constant__ FrameParams p)
     {
         // empty-space skipping only pays when the texture has empty bricks; the merge that
         // wrote it counted them (either choice renders the same image)
         const bool skip = VOLUME && __ldg(p.emptyCount) != 0u;
-        // a block covers 32 x kShadeRows pixels, each warp an 8 x 4 tile
+        constexpr int TW = shade_tile_w(FULL), TH = shade_tile_h(FULL), WX = TW / 8;
         const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-        const int px = int(blockIdx.x) * 32 + (w & 3) * 8 + (l & 7);
-        const int py = int(blockIdx.y) * kShadeRows + (w >> 2) * 4 + (l >> 3);
+        const int px = int(blockIdx.x) * TW + (w % WX) * 8 + (l & 7);
+        const int py = int(blockIdx.y) * TH + (w / WX) * 4 + (l >> 3);
         unsigned long long n = 0;
         if(px < p.v.W && py < p.v.H)
         {
@@ -451,8 +462,9 @@ namespace isaacb
     }
 
     template<bool FULL>
-    void launch_shade_volume_as(const FrameParams& p, bool volume, dim3 grid, cudaStream_t s)
+    void launch_shade_volume_as(const FrameParams& p, bool volume, cudaStream_t s)
     {
+        const dim3 grid((p.v.W + shade_tile_w(FULL) - 1) / shade_tile_w(FULL), (p.v.H + shade_tile_h(FULL) - 1) / shade_tile_h(FULL));
         if(!volume)
             k_shade_volume<false, false, FULL><<<grid, kShadeThreads, 0, s>>>(p);
         else if(p.interpolation)
@@ -466,7 +478,7 @@ namespace isaacb
 
     void launch_shade_volume(const FrameParams& p, bool volume, cudaStream_t s)
     {
-        dim3 grid((p.v.W + 31) / 32, (p.v.H + kShadeRows - 1) / kShadeRows);
+        const long long blocks = (long long) ((p.v.W + 31) / 32) * ((p.v.H + shade_tile_h(false) - 1) / shade_tile_h(false));
         // resident blocks of the uncapped form on the whole device, once per device
         static int resident[64] = {0};
         int dev = 0;
@@ -478,10 +490,10 @@ namespace isaacb
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_shade_volume<true, true, false>, kShadeThreads, 0);
             resident[dev] = std::max(1, sms * perSm);
         }
-        const long long waves = (long long) grid.x * grid.y / std::max(1, dev >= 0 && dev < 64 ? resident[dev] : 1);
+        const long long waves = blocks / std::max(1, dev >= 0 && dev < 64 ? resident[dev] : 1);
         if(volume && waves < kShadeShortWaves)
-            launch_shade_volume_as<true>(p, volume, grid, s);
+            launch_shade_volume_as<true>(p, volume, s);
         else
-            launch_shade_volume_as<false>(p, volume, grid, s);
+            launch_shade_volume_as<false>(p, volume, s);
     }
 } // namespace isaacb

@@ -108,13 +108,12 @@ namespace
         // the first convolution may start loading its weights (it waits for this grid
         // before reading x)
         asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-        const size_t n = size_t(B) * h * w;
-        for(size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        // a batch holds at most 2^26 pixels (isaacb_recon_create), so 32-bit indices suffice
+        const uint32_t n = uint32_t(B) * uint32_t(h) * uint32_t(w), hw = uint32_t(h) * uint32_t(w);
+        for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         {
-            const size_t hw = size_t(h) * w;
-            const int b = int(i / hw);
-            const size_t pp = i - size_t(b) * hw;
-            const int f = index ? __ldg(index + b) : b;
+            const uint32_t b = i / hw, pp = i - b * hw;
+            const int f = index ? __ldg(index + b) : int(b);
             const uchar4 c = __ldg(reinterpret_cast<const uchar4*>(low) + size_t(f) * hw + pp);
             float v[8] = {float(c.x) / 255.0f, float(c.y) / 255.0f, float(c.z) / 255.0f, float(c.w) / 255.0f, 0, 0, 0, 0};
             reinterpret_cast<uint4*>(x)[2 * i] = pack8(v);
@@ -294,10 +293,11 @@ namespace
     {
         // r comes from the output layer, which this kernel follows as a programmatic dependent
         asm volatile("griddepcontrol.wait;" ::: "memory");
-        const size_t n = size_t(h) * w;
-        for(size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        // one thread per half-size pixel (x, y): blockIdx.y is the row
+        const int x = int(blockIdx.x * blockDim.x + threadIdx.x), y = int(blockIdx.y);
+        if(x < w && y < h)
         {
-            const int x = int(i % w), y = int(i / w);
+            const size_t i = size_t(y) * w + x;
             const uchar4* lo = reinterpret_cast<const uchar4*>(low);
             const float4* rp = reinterpret_cast<const float4*>(r + i * 16);
 #pragma unroll
@@ -650,7 +650,7 @@ namespace
                 if(!launch_conv_gemm(p, s))
                     return false;
                 cudaLaunchConfig_t cfg{};
-                cfg.gridDim = dim3(unsigned(grid_for(size_t(R->lh[0]) * R->lw[0])));
+                cfg.gridDim = dim3(unsigned((R->lw[0] + 255) / 256), unsigned(R->lh[0]));
                 cfg.blockDim = dim3(256);
                 cfg.stream = s;
                 cudaLaunchAttribute attr[1];
