@@ -591,6 +591,14 @@ namespace isaacb
         asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
         return r;
     }
+    // a * b rounded once per lane; only for a product that does not feed an add (the
+    // assembler may contract mul.rn.f32x2 + add.rn.f32x2 into one fma, see f2p_mul_exact)
+    __device__ __forceinline__ f2p f2p_mul(f2p a, f2p b)
+    {
+        f2p r;
+        asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+        return r;
+    }
     __device__ __forceinline__ f2p f2p_add(f2p a, f2p b)
     {
         f2p r;

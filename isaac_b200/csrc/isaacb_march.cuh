@@ -22,15 +22,23 @@ namespace isaacb
         constexpr float kUnit = 65535.0f;
         const float gx = 1.0f - fx, gy = 1.0f - fy;
         const float fzU = fz * kUnit, gzU = kUnit - fzU;
-        const float w00 = gx * gy, w10 = fx * gy, w01 = gx * fy, w11 = fx * fy;
-        // round(w * 65535) lands in the low bits of 2^23 + w * 65535 (one rounding, to
-        // nearest); <= 65535, so the low 16 bits are the weight
-        auto q = [](float w, float zU) { return __float_as_uint(fmaf(w, zU, 8388608.0f)); };
+        // the xy weights of a texel row as packed pairs (texel x0, texel x0 + 1):
+        // (w00, w10) = (gx, fx) * gy and (w01, w11) = (gx, fx) * fy
+        const f2p X = f2p_make(gx, fx);
+        const f2p R0 = f2p_mul(X, f2p_make(gy, gy)), R1 = f2p_mul(X, f2p_make(fy, fy));
+        // round(w * 65535) lands in the low bits of 2^23 + w * 65535 (one rounding per lane,
+        // to nearest, as the scalar fmaf); <= 65535, so the low 16 bits are the weight
+        const f2p M = f2p_make(8388608.0f, 8388608.0f), GZ = f2p_make(gzU, gzU), FZ = f2p_make(fzU, fzU);
+        auto pack = [](f2p q) {
+            float lo, hi;
+            f2p_split(q, lo, hi);
+            return __byte_perm(__float_as_uint(lo), __float_as_uint(hi), 0x5410u);
+        };
         // weight pairs (texel (x0,y) | texel (x0+1,y) << 16) for rows y0 and y0+1 of each plane
-        const uint32_t W0a = __byte_perm(q(w00, gzU), q(w10, gzU), 0x5410u);
-        const uint32_t W1a = __byte_perm(q(w01, gzU), q(w11, gzU), 0x5410u);
-        const uint32_t W0b = __byte_perm(q(w00, fzU), q(w10, fzU), 0x5410u);
-        const uint32_t W1b = __byte_perm(q(w01, fzU), q(w11, fzU), 0x5410u);
+        const uint32_t W0a = pack(f2p_fma(R0, GZ, M));
+        const uint32_t W1a = pack(f2p_fma(R1, GZ, M));
+        const uint32_t W0b = pack(f2p_fma(R0, FZ, M));
+        const uint32_t W1b = pack(f2p_fma(R1, FZ, M));
         // Σ weights <= 65535 + 4, so every channel sum is an exact integer below 2^24
         auto tri = [&](uint32_t a, uint32_t b) {
             return __uint2float_rn(dp2a_hi(W1b, b, dp2a_lo(W0b, b, dp2a_hi(W1a, a, dp2a_lo(W0a, a, 0u)))));

@@ -403,9 +403,12 @@ namespace isaacb
     // tile width of the FULL form (the short launches): 16 x 8 pixels keep a block's rays
     // closer together than 32 x 4 (the 960x540 half-size render: 0.953 -> 0.931 ms)
     constexpr int kShortTileW = 16;
+    // tile width and minimum blocks per SM of the uncapped form (the long launches)
+    constexpr int kLongTileW = 32;
+    constexpr int kLongMinBlocks = 1;
     __host__ __device__ constexpr int shade_tile_w(bool full)
     {
-        return full ? kShortTileW : 32;
+        return full ? kShortTileW : kLongTileW;
     }
     __host__ __device__ constexpr int shade_tile_h(bool full)
     {
@@ -417,7 +420,7 @@ namespace isaacb
     // resident rays shorten their tail.  Longer launches keep the uncapped form (46
     // registers, 10 blocks per SM), whose loop runs faster.
     template<bool VOLUME, bool LINEAR, bool FULL>
-    __global__ void __launch_bounds__(kShadeThreads, FULL ? 2048 / kShadeThreads : 1) k_shade_volume(const __grid_constant__ FrameParams p)
+    __global__ void __launch_bounds__(kShadeThreads, FULL ? 2048 / kShadeThreads : kLongMinBlocks) k_shade_volume(const __grid_constant__ FrameParams p)
     {
         // empty-space skipping only pays when the texture has empty bricks; the merge that
         // wrote it counted them (either choice renders the same image)
@@ -478,8 +481,10 @@ namespace isaacb
 
     void launch_shade_volume(const FrameParams& p, bool volume, cudaStream_t s)
     {
-        const long long blocks = (long long) ((p.v.W + 31) / 32) * ((p.v.H + shade_tile_h(false) - 1) / shade_tile_h(false));
-        // resident blocks of the uncapped form on the whole device, once per device
+        const long long blocks = (long long) ((p.v.W + shade_tile_w(false) - 1) / shade_tile_w(false))
+            * ((p.v.H + shade_tile_h(false) - 1) / shade_tile_h(false));
+        // resident blocks of the uncapped form on the whole device, once per device (a
+        // property of the kernel and the device, valid in any context on it)
         static int resident[64] = {0};
         int dev = 0;
         cudaGetDevice(&dev);
