@@ -80,6 +80,10 @@ namespace isaacb
         const float lo = LINEAR ? -1.0f : 0.0f;
         const float hx = float(g.ls[0] - 1), hy = float(g.ls[1] - 1), hz = float(g.ls[2] - 1);
         const int nb0 = g.nb[0], nb1 = g.nb[1];
+        // the slot of apron-shifted coordinates as a sum over the axes: with b = a >> 3 and
+        // l = a & 7 per axis, b * stride + l * step == a * step + b * (stride - 8 * step)
+        const uint32_t sy = uint32_t(nb0) * uint32_t(kSlotsPerBrick) - 64u;
+        const uint32_t sz = uint32_t(nb1) * uint32_t(nb0) * uint32_t(kSlotsPerBrick) - 512u;
         // floor(c) + 1 (the apron-shifted coordinate) straight from the magic-number add
         const int magic = 0x4B400000 - 1;
         float4 color = make_float4(0, 0, 0, 0);
@@ -99,7 +103,7 @@ namespace isaacb
             const float tx = __fadd_rd(cx, 12582912.0f), ty = __fadd_rd(cy, 12582912.0f),
                         tz = __fadd_rd(cz, 12582912.0f);
             const int ax = __float_as_int(tx) - magic, ay = __float_as_int(ty) - magic, az = __float_as_int(tz) - magic;
-            const int brick = ((az >> 3) * nb1 + (ay >> 3)) * nb0 + (ax >> 3);
+            const int brick = SKIP ? ((az >> 3) * nb1 + (ay >> 3)) * nb0 + (ax >> 3) : 0;
             if(SKIP && brick != curBrick)
             {
                 curBrick = brick;
@@ -126,8 +130,8 @@ namespace isaacb
                 fi = last + 1.0f;
                 continue;
             }
-            const uint32_t slot = uint32_t(brick) * uint32_t(kSlotsPerBrick)
-                + uint32_t((ax & 7) | ((ay & 7) << 3) | ((az & 7) << 6));
+            const uint32_t slot = uint32_t(ax) + 568u * uint32_t(ax >> 3) + 8u * uint32_t(ay) + sy * uint32_t(ay >> 3)
+                + 64u * uint32_t(az) + sz * uint32_t(az >> 3);
             float r0, r1, r2, r3;
             if(LINEAR)
             {
