@@ -187,6 +187,9 @@ class JudgedRenderer:
         self.fallback = False
         self.judged = []  # (frame number, PSNR dB)
         self.fallback_frames = 0
+        # a judge frame's plain render does not depend on the half-size render or the
+        # network: it runs on a side stream beside them and fills their idle SMs
+        self._side = torch.cuda.Stream(device=device) if torch.device(device).type == "cuda" else None
 
     def setCamera(self, projection, modelview):
         self.full_viz.setCamera(projection, modelview)
@@ -203,15 +206,26 @@ class JudgedRenderer:
                 self.full_viz.update()
             self.full_viz.render(self.full)
             return self.full
+        torch = _torch()
+        side = self._side if judge else None
+        if side is not None:
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(side):
+                if update:
+                    self.full_viz.update()
+                self.full_viz.render(self.full)
         if update:
             self.low_viz.update()
         self.low_viz.render(self.half)
         self.net.infer(self.half, self.rec)
         if not judge:
             return self.rec
-        if update:
-            self.full_viz.update()
-        self.full_viz.render(self.full)
+        if side is not None:
+            torch.cuda.current_stream().wait_stream(side)
+        else:
+            if update:
+                self.full_viz.update()
+            self.full_viz.render(self.full)
         p = self.measure(self.rec, self.full)
         self.judged.append((k, p))
         self.fallback = p < self.threshold
