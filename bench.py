@@ -855,7 +855,8 @@ def run_sweep(args):
 
     Renders the four spectral sources from an orbit of cameras (``--yaws``) with the
     per-source renderer (BF16 bricks, full size at step 0.5 and half size at step 1.0,
-    as the learned path uses) and with the combined renderer (full size, step 0.5), and
+    as the learned path uses) and with the combined renderer (full size at step 0.5 and
+    half size at step 1.0), and
     prints one JSON line per view: milliseconds per frame (CUDA events, 5 frames after
     2 untimed ones), samples per frame (the kernels' own count) and millions of samples
     per millisecond.  The samples hardly change with the angle, so the rate shows how
@@ -876,10 +877,15 @@ def run_sweep(args):
     fields = scenes.precision_scene(n, device="cuda")
     comb = IsaacVisualization("combined", (W, H), (n, n, n), (n, n, n), (1, 1, 1), (0, 0, 0),
                               [VolumeSource(f"s{i}", f.contiguous(), 1) for i, f in enumerate(fields)])
-    comb.setInterpolation(True)
-    for i in range(4):
-        comb.setTransferPoints(i, tfs[i])
-    comb.update()
+    # the same merged sources at half size and twice the step (the combined learned path)
+    comb_half = IsaacVisualization("combined_half", (W // 2, H // 2), (n, n, n), (n, n, n), (1, 1, 1), (0, 0, 0),
+                                   [VolumeSource(f"s{i}", f.contiguous(), 1) for i, f in enumerate(fields)])
+    for v, st in ((comb, 0.5), (comb_half, 1.0)):
+        v.setInterpolation(True)
+        v.setStep(st)
+        for i in range(4):
+            v.setTransferPoints(i, tfs[i])
+        v.update()
     full = torch.empty((H, W, 4), dtype=torch.uint8, device="cuda")
     half = torch.empty((H // 2, W // 2, 4), dtype=torch.uint8, device="cuda")
     for deg in (float(v) for v in args.yaws.split(",")):
@@ -891,8 +897,11 @@ def run_sweep(args):
         line["per_source_full"] = _sweep_time(pr.full, full)
         comb.setCamera(P, MV)
         line["combined_full"] = _sweep_time(comb, full)
+        comb_half.setCamera(P, MV)
+        line["combined_half"] = _sweep_time(comb_half, half)
         print(json.dumps(json_safe(line)), flush=True)
     comb.close()
+    comb_half.close()
     return 0
 
 
