@@ -160,3 +160,40 @@ def test_trained_weights_beat_bilinear_on_held_out_views(renderer):
     # already within a few dB of the 8-bit truncation floor on these smooth fields
     assert gains.mean() > 0.2, (rec, bil)
     assert (gains > -0.05).all(), (rec, bil)
+
+
+def test_judge_frame_on_side_stream_equals_serial_frames():
+    """On judge frames JudgedRenderer renders the plain frame on a side stream beside the
+    half-size render and the network; the served frame, the plain frame and the measured
+    PSNR must be those of the same steps run one after the other on one stream."""
+    from isaac_b200 import recon, scenes
+    from isaac_b200.recon_train import PairRenderer
+
+    W, H = 320, 180
+    pr = PairRenderer(size=96, width=W, height=H, renderer="combined")
+    pr.set_timestep(0)
+    tfs = [scenes.transfer_4point(0.7 * i) for i in range(4)]
+    P, MV = scenes.orbit_camera(W, H, yaw=0.6, pitch=0.35, distance=2.4)
+    pr.set_view(P, MV, tfs)
+    pr.full.update()
+    pr.low.update()
+    net = Reconstructor(1, H // 2, W // 2, seed=1)
+    net.load(recon.weights_for("combined"))
+    jr = recon.JudgedRenderer(pr.full, pr.low, net, judge_every=1, threshold=10.0)
+    jr.setCamera(P, MV)
+    served = jr.frame().clone()
+    full_side, p_side = jr.full.clone(), jr.judged[-1][1]
+    half = torch.empty((H // 2, W // 2, 4), dtype=torch.uint8, device="cuda")
+    rec = torch.empty((H, W, 4), dtype=torch.uint8, device="cuda")
+    full = torch.empty_like(rec)
+    pr.low.render(half)
+    net.infer(half, rec)
+    pr.full.render(full)
+    torch.cuda.synchronize()
+    assert torch.equal(full_side, full)
+    assert torch.equal(served, rec)
+    assert p_side == psnr(rec, full)
+    assert net.error_flag() == 0
+    net.close()
+    for v in (pr.full, pr.low):
+        v.close()
