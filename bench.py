@@ -895,9 +895,13 @@ def run_sweep(args):
         line["per_source_half"] = _sweep_time(pr.low, half)
         pr.full.setCamera(P, MV)
         line["per_source_full"] = _sweep_time(pr.full, full)
+        # the combined texture is merged for each view (as in-situ rendering merges every
+        # frame), which picks the brick slot order for the camera; the merge is not timed
         comb.setCamera(P, MV)
+        comb.update()
         line["combined_full"] = _sweep_time(comb, full)
         comb_half.setCamera(P, MV)
+        comb_half.update()
         line["combined_half"] = _sweep_time(comb_half, half)
         print(json.dumps(json_safe(line)), flush=True)
     comb.close()

@@ -157,6 +157,11 @@ isaacb_status isaacb_set_dither_mode(isaacb_ctx* ctx, int32_t mode);
 /* Storage type of the per-source renderer's bricks (no reference counterpart;
  * FP32 is the reference behaviour). */
 isaacb_status isaacb_set_storage(isaacb_ctx* ctx, uint32_t src, int32_t dtype);
+/* Slot order inside the combined texture's bricks (no reference counterpart; it
+ * changes speed only, never a texel or a pixel).  -1 (default): chosen by each merge
+ * from its camera for textures larger than 4x the L2 cache, x fastest otherwise;
+ * 0: x fastest; 1: y fastest.  Takes effect at the next update. */
+isaacb_status isaacb_set_slot_order(isaacb_ctx* ctx, int32_t order);
 /* Background colour as handed to the draw callback (lib/isaac.hpp:2245-2249
  * swizzles it to (a,b,g,r) with alpha 0 for the G-buffer clear). */
 isaacb_status isaacb_set_background(isaacb_ctx* ctx, const float rgba[4]);

@@ -145,6 +145,7 @@ SIGNATURES = {
     "isaacb_set_render_mode": (_i32, [_P, _i32]),
     "isaacb_set_dither_mode": (_i32, [_P, _i32]),
     "isaacb_set_storage": (_i32, [_P, _u32, _i32]),
+    "isaacb_set_slot_order": (_i32, [_P, _i32]),
     "isaacb_set_background": (_i32, [_P, _fp]),
     "isaacb_add_clipping": (_i32, [_P, _fp, _fp]),
     "isaacb_edit_clipping": (_i32, [_P, _u32, _fp, _fp]),

@@ -23,7 +23,8 @@ namespace isaacb
     // the volume.  A trilinear footprint whose base texel is (x0,y0,z0) is the two
     // slots (lx,ly,lz) and (lx,ly,lz+1) of one brick.  The combined RGBA8 texture
     // stores a slot channel-major (quad_channel_major), the iso alpha texture one
-    // byte per texel in the same order.
+    // byte per texel in the same order.  Inside a brick the slots are stored x fastest
+    // or y fastest, as the merge chose for its camera (Geom::yfast, slot_in_brick).
     constexpr int kSlotsPerBrick = 576;
     constexpr int kApron = 9;
 
@@ -50,6 +51,9 @@ namespace isaacb
         int32_t gs[3], ls[3], lps[3], pos[3], gss[3], lss[3], posS[3];
         int32_t maxGss;
         int32_t nb[3]; // bricks per axis = (ls >> 3) + 1
+        // slot order of the combined textures' bricks, set by the merge that wrote them:
+        // 0 x fastest (slot lz * 64 + ly * 8 + lx), 1 y fastest (lz * 64 + lx * 8 + ly)
+        int32_t yfast;
     };
 
     __host__ __device__ inline int32_t bricks_per_axis(int32_t l)
@@ -388,12 +392,18 @@ namespace isaacb
     }
 
     // ------------------------------------------------------------- brick addressing
+    // slot of apron-shifted coordinates (ax, ay, az) inside their brick, in the texture's order
+    __device__ __forceinline__ uint32_t slot_in_brick(const Geom& g, int ax, int ay, int az)
+    {
+        const uint32_t xy = g.yfast ? uint32_t((ax & 7) * 8 + (ay & 7)) : uint32_t((ay & 7) * 8 + (ax & 7));
+        return uint32_t(az & 7) * 64u + xy;
+    }
     __device__ __forceinline__ size_t brick_slot(const Geom& g, int x0, int y0, int z0)
     {
         // x0 in [-1, L-1]: base texel of a trilinear footprint
         int ax = x0 + 1, ay = y0 + 1, az = z0 + 1;
         size_t brick = (size_t(az >> 3) * g.nb[1] + size_t(ay >> 3)) * g.nb[0] + size_t(ax >> 3);
-        return brick * kSlotsPerBrick + size_t((az & 7) * 64 + (ay & 7) * 8 + (ax & 7));
+        return brick * kSlotsPerBrick + size_t(slot_in_brick(g, ax, ay, az));
     }
 
     // Per-source bricks order their slots along a Morton curve: slot (lx, ly, lz) of a

@@ -62,7 +62,8 @@ namespace isaacb
     // CLAMP keeps every coordinate inside the volume; a LINEAR ray whose first and
     // last sample lie strictly inside needs no per-sample clamp (positions are affine
     // in the step index, rounding is far below the 1e-3 margin).
-    template<bool LINEAR, bool CLAMP, bool SKIP>
+    // YFAST: the texture's slots are y fastest (Geom::yfast), else x fastest.
+    template<bool LINEAR, bool CLAMP, bool SKIP, bool YFAST = false>
     __device__ __forceinline__ float4 march_combined(
         const VolTexRef& p,
         const March& m,
@@ -81,8 +82,10 @@ namespace isaacb
         const float hx = float(g.ls[0] - 1), hy = float(g.ls[1] - 1), hz = float(g.ls[2] - 1);
         const int nb0 = g.nb[0], nb1 = g.nb[1];
         // the slot of apron-shifted coordinates as a sum over the axes: with b = a >> 3 and
-        // l = a & 7 per axis, b * stride + l * step == a * step + b * (stride - 8 * step)
-        const uint32_t sy = uint32_t(nb0) * uint32_t(kSlotsPerBrick) - 64u;
+        // l = a & 7 per axis, b * stride + l * step == a * step + b * (stride - 8 * step);
+        // the in-brick steps of x and y are (1, 8), or (8, 1) for y-fastest slots
+        constexpr uint32_t stepX = YFAST ? 8u : 1u, stepY = YFAST ? 1u : 8u;
+        const uint32_t sy = uint32_t(nb0) * uint32_t(kSlotsPerBrick) - 8u * stepY;
         const uint32_t sz = uint32_t(nb1) * uint32_t(nb0) * uint32_t(kSlotsPerBrick) - 512u;
         // floor(c) + 1 (the apron-shifted coordinate) straight from the magic-number add
         const int magic = 0x4B400000 - 1;
@@ -130,8 +133,8 @@ namespace isaacb
                 fi = last + 1.0f;
                 continue;
             }
-            const uint32_t slot = uint32_t(ax) + 568u * uint32_t(ax >> 3) + 8u * uint32_t(ay) + sy * uint32_t(ay >> 3)
-                + 64u * uint32_t(az) + sz * uint32_t(az >> 3);
+            const uint32_t slot = stepX * uint32_t(ax) + (576u - 8u * stepX) * uint32_t(ax >> 3) + stepY * uint32_t(ay)
+                + sy * uint32_t(ay >> 3) + 64u * uint32_t(az) + sz * uint32_t(az >> 3);
             float r0, r1, r2, r3;
             if(LINEAR)
             {

@@ -407,10 +407,15 @@ namespace isaacb
     constexpr int kPackPitch = 40; // row pitch in words: 40 = 8 mod 32 keeps the quad reads conflict-free
     constexpr int kPackRows = kApron * kApron; // (ly, lz) rows
     constexpr int kPackWords = kPackRows * kPackPitch;
+    // k_merge_pack's pitch for y-fastest slots: its quad reads then walk y across a warp's
+    // lanes, and 36 = 4 mod 32 puts the 8 rows x 4 columns of a warp on 32 different banks
+    constexpr int kPackPitchY = 36;
 
-    template<bool ISO>
+    template<bool ISO, bool YFAST>
     __global__ void __launch_bounds__(256) k_merge_pack(const __grid_constant__ MergeParams p)
     {
+        // staging pitch: conflict-free quad reads for the slot order
+        constexpr int kPackPitch = YFAST ? kPackPitchY : isaacb::kPackPitch;
         __shared__ uint32_t volS[kPackWords];
         __shared__ uint32_t isoS[ISO ? kPackWords : 1];
         __shared__ int anyS[kPackRow], isoMaxS[kPackRow];
@@ -515,8 +520,10 @@ namespace isaacb
             if(ISO)
                 p.isoFlag[brick0 + j] = uint8_t(isoMaxS[j]);
         }
+        // thread lxy writes slot lxy of each layer: (lx, ly) = (lxy & 7, lxy >> 3) for x-fastest
+        // slots, (lxy >> 3, lxy & 7) for y-fastest ones
         const int lxy = threadIdx.x & 63;
-        const int base = (lxy >> 3) * kPackPitch + (lxy & 7);
+        const int base = YFAST ? (lxy & 7) * kPackPitch + (lxy >> 3) : (lxy >> 3) * kPackPitch + (lxy & 7);
         for(int layer = threadIdx.x >> 6; layer < nRow * kApron; layer += 4)
         {
             const int j = layer / kApron, lz = layer - j * kApron;
@@ -617,7 +624,11 @@ namespace isaacb
         }
         else
             k_merge_voxels<ISO><<<vgrid, 256, 0, s>>>(p);
-        k_merge_pack<ISO><<<dim3((p.g.nb[0] + kPackRow - 1) / kPackRow, p.g.nb[1], p.g.nb[2]), 256, 0, s>>>(p);
+        const dim3 pgrid((p.g.nb[0] + kPackRow - 1) / kPackRow, p.g.nb[1], p.g.nb[2]);
+        if(p.g.yfast)
+            k_merge_pack<ISO, true><<<pgrid, 256, 0, s>>>(p);
+        else
+            k_merge_pack<ISO, false><<<pgrid, 256, 0, s>>>(p);
         return launches;
     }
 

@@ -168,7 +168,14 @@ namespace isaacb
     // ------------------------------------------------------------------ iso
     // interpolated alpha byte (0..255 scale) of the iso alpha quads at c = pos - 0.5,
     // FMA/ALU pipes only; brick index and emptiness (max alpha <= 127) returned
-    template<bool LINEAR>
+    // slot of apron-shifted coordinates inside their brick for a known slot order
+    template<bool YFAST>
+    __device__ __forceinline__ uint32_t slot_in_brick_as(int ax, int ay, int az)
+    {
+        return uint32_t(az & 7) * 64u + (YFAST ? uint32_t((ax & 7) * 8 + (ay & 7)) : uint32_t((ay & 7) * 8 + (ax & 7)));
+    }
+
+    template<bool LINEAR, bool YFAST>
     __device__ __forceinline__ float iso_alpha_fast(const FrameParams& p, float cx, float cy, float cz, int& brick)
     {
         const Geom& g = p.g;
@@ -180,7 +187,7 @@ namespace isaacb
         const float tx = __fadd_rd(cx, 12582912.0f), ty = __fadd_rd(cy, 12582912.0f), tz = __fadd_rd(cz, 12582912.0f);
         const int ax = __float_as_int(tx) - magic, ay = __float_as_int(ty) - magic, az = __float_as_int(tz) - magic;
         brick = ((az >> 3) * g.nb[1] + (ay >> 3)) * g.nb[0] + (ax >> 3);
-        const uint32_t slot = uint32_t(brick) * uint32_t(kSlotsPerBrick) + uint32_t((ax & 7) | ((ay & 7) << 3) | ((az & 7) << 6));
+        const uint32_t slot = uint32_t(brick) * uint32_t(kSlotsPerBrick) + slot_in_brick_as<YFAST>(ax, ay, az);
         if(!LINEAR)
             return ubyte_f(__ldg(p.isoAQ + slot), 0);
         const uint32_t A = __ldg(p.isoAQ + slot), B = __ldg(p.isoAQ + slot + 64);
@@ -206,7 +213,7 @@ namespace isaacb
     // position and c = pos - 0.5 rounded as separate operations, floor/fraction of the
     // unclamped c, CLAMP on the texel indices and the z -> y -> x lerp order of
     // Sampler/trilinear (lib/isaac/isaac_texture.hpp:140-305, isaac_helper.hpp:124-144).
-    template<bool LINEAR>
+    template<bool LINEAR, bool YFAST>
     __device__ __forceinline__ float iso_alpha_exact(const FrameParams& p, const March& m, int i)
     {
         const Geom& g = p.g;
@@ -217,7 +224,7 @@ namespace isaacb
                       az = iclamp(f2i(pos.z), 0, g.ls[2] - 1) + 1;
             const int brick = ((az >> 3) * g.nb[1] + (ay >> 3)) * g.nb[0] + (ax >> 3);
             const uint32_t slot
-                = uint32_t(brick) * uint32_t(kSlotsPerBrick) + uint32_t((ax & 7) | ((ay & 7) << 3) | ((az & 7) << 6));
+                = uint32_t(brick) * uint32_t(kSlotsPerBrick) + slot_in_brick_as<YFAST>(ax, ay, az);
             return byte_f(__ldg(p.isoAQ + slot), 0);
         }
         const float cx = pos.x - 0.5f, cy = pos.y - 0.5f, cz = pos.z - 0.5f;
@@ -229,7 +236,7 @@ namespace isaacb
                   az = iclamp(f2i(flz), -1, g.ls[2] - 1) + 1;
         const int brick = ((az >> 3) * g.nb[1] + (ay >> 3)) * g.nb[0] + (ax >> 3);
         const uint32_t slot
-            = uint32_t(brick) * uint32_t(kSlotsPerBrick) + uint32_t((ax & 7) | ((ay & 7) << 3) | ((az & 7) << 6));
+            = uint32_t(brick) * uint32_t(kSlotsPerBrick) + slot_in_brick_as<YFAST>(ax, ay, az);
         const uint32_t A = __ldg(p.isoAQ + slot), B = __ldg(p.isoAQ + slot + 64);
         return tri_q(fx, fy, fz, byte_f(A, 0), byte_f(A, 1), byte_f(A, 2), byte_f(A, 3), byte_f(B, 0), byte_f(B, 1),
                      byte_f(B, 2), byte_f(B, 3));
@@ -246,7 +253,7 @@ namespace isaacb
     // in the reference.  So hit, depth, colour and normal follow the reference's float
     // operations exactly.
     constexpr float kIsoMargin = 0.125f; // alpha bytes
-    template<bool LINEAR>
+    template<bool LINEAR, bool YFAST>
     __global__ void __launch_bounds__(256) k_iso(const __grid_constant__ FrameParams p)
     {
         int px, py;
@@ -277,7 +284,7 @@ namespace isaacb
                         const float cx = fmaf(m.stepVec.x, fi, c0x), cy = fmaf(m.stepVec.y, fi, c0y),
                                     cz = fmaf(m.stepVec.z, fi, c0z);
                         int brick;
-                        const float a = iso_alpha_fast<LINEAR>(p, cx, cy, cz, brick);
+                        const float a = iso_alpha_fast<LINEAR, YFAST>(p, cx, cy, cz, brick);
                         if(brick != curBrick)
                         {
                             curBrick = brick;
@@ -285,11 +292,11 @@ namespace isaacb
                         }
                         if(skip || a < 127.5f - kIsoMargin)
                             continue;
-                        const float value = iso_alpha_exact<LINEAR>(p, m, i) / 255.0f;
+                        const float value = iso_alpha_exact<LINEAR, YFAST>(p, m, i) / 255.0f;
                         if(value < 0.5f)
                             continue;
                         // the reference's previous value: 0 before the first sample
-                        const float tmp = i == m.startSteps ? 0.0f : iso_alpha_exact<LINEAR>(p, m, i - 1) / 255.0f;
+                        const float tmp = i == m.startSteps ? 0.0f : iso_alpha_exact<LINEAR, YFAST>(p, m, i - 1) / 255.0f;
                         const bool first = ray.isClipped && i == m.startSteps;
                         const float t = fi * m.stepU;
                         if(first)
@@ -338,9 +345,9 @@ namespace isaacb
     {
         dim3 grid((p.v.W + 31) / 32, (p.v.H + 7) / 8);
         if(p.interpolation)
-            k_iso<true><<<grid, 256, 0, s>>>(p);
+            p.g.yfast ? k_iso<true, true><<<grid, 256, 0, s>>>(p) : k_iso<true, false><<<grid, 256, 0, s>>>(p);
         else
-            k_iso<false><<<grid, 256, 0, s>>>(p);
+            p.g.yfast ? k_iso<false, true><<<grid, 256, 0, s>>>(p) : k_iso<false, false><<<grid, 256, 0, s>>>(p);
     }
 
     // ------------------------------------------------------------------ SSAO
@@ -419,16 +426,30 @@ namespace isaacb
     // registers, a few bytes spilled).  Launches of only a few waves take it: more
     // resident rays shorten their tail.  Longer launches keep the uncapped form (46
     // registers, 10 blocks per SM), whose loop runs faster.
-    template<bool VOLUME, bool LINEAR, bool FULL>
+    // tile of a y-fastest texture's blocks (4 warps of 4 x 8 pixels)
+    constexpr int kYTileW = 16;
+    __host__ __device__ constexpr int shade_tile_w(bool full, bool yfast)
+    {
+        return yfast ? kYTileW : shade_tile_w(full);
+    }
+    __host__ __device__ constexpr int shade_tile_h(bool full, bool yfast)
+    {
+        return kShadeThreads / shade_tile_w(full, yfast);
+    }
+
+    // YFAST: the texture's slots are y fastest; each warp then covers 4 x 8 pixels, so that
+    // the image's columns, which views about the y axis keep along y, walk the fastest axis
+    template<bool VOLUME, bool LINEAR, bool FULL, bool YFAST>
     __global__ void __launch_bounds__(kShadeThreads, FULL ? 2048 / kShadeThreads : kLongMinBlocks) k_shade_volume(const __grid_constant__ FrameParams p)
     {
         // empty-space skipping only pays when the texture has empty bricks; the merge that
         // wrote it counted them (either choice renders the same image)
         const bool skip = VOLUME && __ldg(p.emptyCount) != 0u;
-        constexpr int TW = shade_tile_w(FULL), TH = shade_tile_h(FULL), WX = TW / 8;
+        constexpr int TW = shade_tile_w(FULL, YFAST), TH = shade_tile_h(FULL, YFAST);
+        constexpr int WW = YFAST ? 4 : 8, WH = 32 / WW, WX = TW / WW; // warp tile and warps per row
         const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-        const int px = int(blockIdx.x) * TW + (w % WX) * 8 + (l & 7);
-        const int py = int(blockIdx.y) * TH + (w / WX) * 4 + (l >> 3);
+        const int px = int(blockIdx.x) * TW + (w % WX) * WW + (l % WW);
+        const int py = int(blockIdx.y) * TH + (w / WX) * WH + (l / WW);
         unsigned long long n = 0;
         if(px < p.v.W && py < p.v.H)
         {
@@ -447,11 +468,11 @@ namespace isaacb
                         float4 color;
                         const VolTexRef tex{p.g, p.volQ, p.volFlag};
                         if(LINEAR && march_in_range(p.g, m))
-                            color = skip ? march_combined<LINEAR, false, true>(tex, m, factor, n)
-                                         : march_combined<LINEAR, false, false>(tex, m, factor, n);
+                            color = skip ? march_combined<LINEAR, false, true, YFAST>(tex, m, factor, n)
+                                         : march_combined<LINEAR, false, false, YFAST>(tex, m, factor, n);
                         else
-                            color = skip ? march_combined<LINEAR, true, true>(tex, m, factor, n)
-                                         : march_combined<LINEAR, true, false>(tex, m, factor, n);
+                            color = skip ? march_combined<LINEAR, true, true, YFAST>(tex, m, factor, n)
+                                         : march_combined<LINEAR, true, false, YFAST>(tex, m, factor, n);
                         const float4 solid = from_byte4(p.color[o]);
                         const float r = 1.0f - color.w;
                         color = make_float4(color.x + r * solid.x, color.y + r * solid.y, color.z + r * solid.z, color.w + r * solid.w);
@@ -464,16 +485,17 @@ namespace isaacb
             count_samples(p.counters, n);
     }
 
-    template<bool FULL>
+    template<bool FULL, bool YFAST>
     void launch_shade_volume_as(const FrameParams& p, bool volume, cudaStream_t s)
     {
-        const dim3 grid((p.v.W + shade_tile_w(FULL) - 1) / shade_tile_w(FULL), (p.v.H + shade_tile_h(FULL) - 1) / shade_tile_h(FULL));
+        constexpr int TW = shade_tile_w(FULL, YFAST), TH = shade_tile_h(FULL, YFAST);
+        const dim3 grid((p.v.W + TW - 1) / TW, (p.v.H + TH - 1) / TH);
         if(!volume)
-            k_shade_volume<false, false, FULL><<<grid, kShadeThreads, 0, s>>>(p);
+            k_shade_volume<false, false, FULL, YFAST><<<grid, kShadeThreads, 0, s>>>(p);
         else if(p.interpolation)
-            k_shade_volume<true, true, FULL><<<grid, kShadeThreads, 0, s>>>(p);
+            k_shade_volume<true, true, FULL, YFAST><<<grid, kShadeThreads, 0, s>>>(p);
         else
-            k_shade_volume<true, false, FULL><<<grid, kShadeThreads, 0, s>>>(p);
+            k_shade_volume<true, false, FULL, YFAST><<<grid, kShadeThreads, 0, s>>>(p);
     }
 
     // launches of fewer than this many waves of the uncapped form take the FULL form
@@ -492,13 +514,14 @@ namespace isaacb
         {
             int sms = 0, perSm = 0;
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_shade_volume<true, true, false>, kShadeThreads, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_shade_volume<true, true, false, false>, kShadeThreads, 0);
             resident[dev] = std::max(1, sms * perSm);
         }
         const long long waves = blocks / std::max(1, dev >= 0 && dev < 64 ? resident[dev] : 1);
-        if(volume && waves < kShadeShortWaves)
-            launch_shade_volume_as<true>(p, volume, s);
+        const bool full = volume && waves < kShadeShortWaves;
+        if(p.g.yfast)
+            full ? launch_shade_volume_as<true, true>(p, volume, s) : launch_shade_volume_as<false, true>(p, volume, s);
         else
-            launch_shade_volume_as<false>(p, volume, s);
+            full ? launch_shade_volume_as<true, false>(p, volume, s) : launch_shade_volume_as<false, false>(p, volume, s);
     }
 } // namespace isaacb

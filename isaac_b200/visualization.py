@@ -303,6 +303,11 @@ class IsaacVisualization:
         self.interpolation = bool(on)
         check(self.lib.isaacb_set_interpolation(self.ctx, int(on)), self.ctx)
 
+    def setSlotOrder(self, order: int = -1):
+        """Slot order inside the combined texture's bricks: -1 chosen by each merge from its
+        camera (textures beyond 4x L2), 0 x fastest, 1 y fastest.  Speed only."""
+        check(self.lib.isaacb_set_slot_order(self.ctx, int(order)), self.ctx)
+
     def setRenderOptimization(self, on: bool):
         self.renderOptimization = bool(on)
         r = _lib.RENDERER_COMBINED if on else _lib.RENDERER_PER_SOURCE
