@@ -415,7 +415,7 @@ namespace isaacb
     __global__ void __launch_bounds__(256) k_merge_pack(const __grid_constant__ MergeParams p)
     {
         // staging pitch: conflict-free quad reads for the slot order
-        constexpr int kPackPitch = YFAST ? kPackPitchY : isaacb::kPackPitch;
+        constexpr int kPitch = YFAST ? kPackPitchY : kPackPitch;
         __shared__ uint32_t volS[kPackWords];
         __shared__ uint32_t isoS[ISO ? kPackWords : 1];
         __shared__ int anyS[kPackRow], isoMaxS[kPackRow];
@@ -472,20 +472,20 @@ namespace isaacb
             const int r = rr[i];
             if(r >= 0)
             {
-                volS[r * kPackPitch + lane] = v[i];
+                volS[r * kPitch + lane] = v[i];
                 laneAny |= v[i] != 0u;
                 if(ISO)
                 {
-                    isoS[r * kPackPitch + lane] = w[i];
+                    isoS[r * kPitch + lane] = w[i];
                     laneIso = max(laneIso, int(w[i] >> 24));
                 }
                 if(lane == 0)
                 {
-                    volS[r * kPackPitch + 32] = v2[i];
+                    volS[r * kPitch + 32] = v2[i];
                     any32 |= v2[i] != 0u;
                     if(ISO)
                     {
-                        isoS[r * kPackPitch + 32] = w2[i];
+                        isoS[r * kPitch + 32] = w2[i];
                         iso32 = max(iso32, int(w2[i] >> 24));
                     }
                 }
@@ -523,16 +523,16 @@ namespace isaacb
         // thread lxy writes slot lxy of each layer: (lx, ly) = (lxy & 7, lxy >> 3) for x-fastest
         // slots, (lxy >> 3, lxy & 7) for y-fastest ones
         const int lxy = threadIdx.x & 63;
-        const int base = YFAST ? (lxy & 7) * kPackPitch + (lxy >> 3) : (lxy >> 3) * kPackPitch + (lxy & 7);
+        const int base = YFAST ? (lxy & 7) * kPitch + (lxy >> 3) : (lxy >> 3) * kPitch + (lxy & 7);
         for(int layer = threadIdx.x >> 6; layer < nRow * kApron; layer += 4)
         {
             const int j = layer / kApron, lz = layer - j * kApron;
-            const int t = lz * (kApron * kPackPitch) + base + 8 * j;
+            const int t = lz * (kApron * kPitch) + base + 8 * j;
             const size_t slot = brick0 * kSlotsPerBrick + size_t(layer) * 64 + lxy;
-            p.volQ[slot] = quad_channel_major(volS[t], volS[t + 1], volS[t + kPackPitch], volS[t + kPackPitch + 1]);
+            p.volQ[slot] = quad_channel_major(volS[t], volS[t + 1], volS[t + kPitch], volS[t + kPitch + 1]);
             if(ISO)
-                p.isoAQ[slot] = (isoS[t] >> 24) | ((isoS[t + 1] >> 24) << 8) | ((isoS[t + kPackPitch] >> 24) << 16)
-                    | ((isoS[t + kPackPitch + 1] >> 24) << 24);
+                p.isoAQ[slot] = (isoS[t] >> 24) | ((isoS[t + 1] >> 24) << 8) | ((isoS[t + kPitch] >> 24) << 16)
+                    | ((isoS[t + kPitch + 1] >> 24) << 24);
         }
     }
 
